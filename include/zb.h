@@ -1,0 +1,204 @@
+/* zb.h -- C ABI of the B200 DFR residual library (libzefr_b200.so).
+ *
+ * This is the drop-in boundary for ZEFR's residual hot path: the explicit
+ * Direct Flux Reconstruction residual that FRSolver::compute_residual builds
+ * (reference include/solver.hpp:152, src/solver.cpp:1494-1645) and the
+ * explicit RK stepping around it (include/solver.hpp:158-190,
+ * src/solver.cpp:2864-3097).  The reference exposes these as C++ methods
+ * (FRSolver, Zefr, namespace zefr:: in include/zefr_interface.hpp:89-159);
+ * here they are plain C entry points taking pointers, sizes and strides, so a
+ * C++ FRSolver shim, ctypes, cgo or JNI can bind them alike.
+ *
+ * Conventions
+ *  - Every entry point returns zb_status; 0 is success.  No C++ exception
+ *    crosses this boundary.  zb_last_error() describes the last failure on the
+ *    calling thread (the reference throws std::runtime_error with file:line,
+ *    include/macros.hpp:52-54).
+ *  - A zb_plan is host-only set-up (mesh connectivity, operators, metrics);
+ *    building one needs no GPU.  A zb_ctx owns device memory on the device
+ *    current at zb_create time and one CUDA stream.
+ *  - Host buffers passed in are borrowed for the duration of the call.
+ *  - State and residual arrays are addressed with explicit element, variable
+ *    and solution-point strides, the convention of zefr::get_q_spts
+ *    (include/zefr_interface.hpp:126-129, src/zefr.cpp:607-645).
+ *  - One context per host thread (or per stream); calls on one context are
+ *    not thread-safe.
+ */
+#ifndef ZB_H
+#define ZB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int zb_status;
+
+enum {
+  ZB_OK = 0,
+  ZB_ERR_ARG = -1,          /* invalid argument or size */
+  ZB_ERR_CUDA = -2,         /* CUDA runtime error */
+  ZB_ERR_MESH = -3,         /* malformed mesh, unpaired periodic face, negative Jacobian */
+  ZB_ERR_UNSUPPORTED = -4,  /* element type / order / option not built */
+  ZB_ERR_NONFINITE = -5,    /* NaN or Inf found in state or residual */
+  ZB_ERR_NOMEM = -6,        /* device or host allocation failed */
+  ZB_ERR_INTERNAL = -7
+};
+
+/* Boundary conditions: same meaning and numbering as the reference BC_TYPE
+ * enum (include/input.hpp:54-70). */
+enum {
+  ZB_BC_NONE = 0,
+  ZB_BC_PERIODIC = 1,
+  ZB_BC_CHAR = 2,
+  ZB_BC_SUP_IN = 3,
+  ZB_BC_SUP_OUT = 4,
+  ZB_BC_SLIP_WALL = 5,
+  ZB_BC_ISOTHERMAL_NOSLIP = 6,
+  ZB_BC_ADIABATIC_NOSLIP = 7,
+  ZB_BC_ISOTHERMAL_NOSLIP_MOVING = 8,
+  ZB_BC_ADIABATIC_NOSLIP_MOVING = 9,
+  ZB_BC_SYMMETRY = 11
+};
+
+/* Common convective flux (reference FC_TYPE, include/input.hpp:28-31, plus Roe). */
+enum { ZB_FLUX_RUSANOV = 0, ZB_FLUX_ROE = 2 };
+
+/* Arithmetic of the residual.  ZB_FP64: FP64 throughout (the form checked
+ * against the reference).  ZB_MIXED: FP32 state, residual and pointwise flux,
+ * FP64 metrics at set-up only, compensated RK accumulation. */
+enum { ZB_FP64 = 0, ZB_MIXED = 1 };
+
+/* Where a buffer lives. */
+enum { ZB_HOST = 0, ZB_DEVICE = 1 };
+
+typedef struct zb_mesh {
+  int ndims;                 /* 2 or 3 */
+  int gmsh_type;             /* volume element: 2 tri3, 3 quad4, 10 quad9, 5 hex8 */
+  int64_t n_nodes;
+  const double *coords;      /* [n_nodes][3] */
+  int64_t n_eles;
+  int nodes_per_ele;
+  const int64_t *ele2nodes;  /* [n_eles][nodes_per_ele], zero-based, gmsh node order */
+  int64_t n_bnd_faces;
+  int nodes_per_face;        /* nodes listed per boundary face (corner nodes first) */
+  const int64_t *face_nodes; /* [n_bnd_faces][nodes_per_face], zero-based */
+  const int *face_bc;        /* [n_bnd_faces] ZB_BC_* */
+} zb_mesh;
+
+/* Physical and numerical parameters.  Field meanings follow the reference
+ * InputStruct after read_input_file / apply_nondim (src/input.cpp:31-539);
+ * zb_params_from_deck() performs that computation from deck-style inputs. */
+typedef struct zb_params {
+  int order;          /* polynomial order P */
+  int viscous;        /* 0 Euler, 1 Navier-Stokes (LDG) */
+  int fconv;          /* ZB_FLUX_* */
+  int precision;      /* ZB_FP64 or ZB_MIXED */
+  double gamma, prandtl, mu, rt, c_sth;
+  int fix_vis;        /* 1: constant mu; 0: Sutherland */
+  double rus_k, ldg_b, ldg_tau;
+  double rho_fs, V_fs[3], P_fs;
+  double T_wall, R_ref, V_wall[3];
+  double dt;          /* RK time step */
+} zb_params;
+
+/* Deck-style inputs for zb_params_from_deck (reference keys, src/input.cpp). */
+typedef struct zb_deck {
+  int ndims, order, viscous, fconv, precision;
+  int disable_nondim, fix_vis;
+  double gamma, prandtl, R, S, T_gas, rho_fs, P_fs, mach_fs, Re_fs, L_fs, T_fs;
+  double nx_fs, ny_fs, nz_fs;
+  double mach_wall, T_wall, nx_wall, ny_wall, nz_wall;
+  double rus_k, ldg_b, ldg_tau, dt;
+} zb_deck;
+
+typedef struct zb_info {
+  int ndims, nvars, nspts, nfpts, order, etype;  /* etype: 1 tri, 2 quad, 4 hex (reference ELE_TYPE) */
+  int64_t n_eles, n_eles_pad, n_gfpts, n_gfpts_int, n_gfpts_bnd;
+  int nstages;
+  int tile;           /* elements per layout tile */
+  int precision;
+} zb_info;
+
+typedef struct zb_plan zb_plan;
+typedef struct zb_ctx zb_ctx;
+
+/* Error text for the last failing call on this thread. */
+const char *zb_last_error(void);
+
+/* Library version string. */
+const char *zb_version(void);
+
+/* Fill reference-style parameters (reference src/input.cpp:463-539). */
+zb_status zb_params_from_deck(const zb_deck *deck, zb_params *out);
+
+/* Read a gmsh 2.2 ASCII mesh (reference src/geometry.cpp:307-957).
+ * names/bcs map boundary physical names (case-insensitive) to ZB_BC_* like the
+ * deck's mesh_bound lines.  The returned mesh is freed with zb_mesh_free. */
+zb_status zb_mesh_read_gmsh(const char *path, int ndims, int n_map, const char *const *names,
+                            const int *bcs, zb_mesh **out);
+void zb_mesh_free(zb_mesh *mesh);
+
+/* Host-side set-up: connectivity (reference src/geometry.cpp:1159-1744,
+ * src/solver.cpp:312-437), operators (src/elements.cpp:555-810) and metrics
+ * (src/elements.cpp:325-407, 845-996).  No GPU needed. */
+zb_status zb_plan_create(const zb_mesh *mesh, const zb_params *params, zb_plan **out);
+void zb_plan_free(zb_plan *plan);
+zb_status zb_plan_info(const zb_plan *plan, zb_info *out);
+
+/* Copy a named set-up array out in the reference's own layout (for checking
+ * set-up against the reference).  Names: coord_spts, jaco_det_spts,
+ * inv_jaco_spts, oppE, oppD, oppD_fpts, oppDiv, oppDiv_fpts, fpt_partner
+ * (partner element*nfpts+fpt per element fpt, -1-bc on boundaries),
+ * fpt_slot, fpt_norm (left-element normal per element fpt [fpt][dim][ele]),
+ * fpt_dA.  With out == NULL, *n receives the element count. */
+zb_status zb_plan_get(const zb_plan *plan, const char *name, double *out, int64_t *n);
+
+/* Create a device context from a plan on the current device. */
+zb_status zb_create(const zb_plan *plan, zb_ctx **out);
+/* Convenience: mesh + params -> plan -> context. */
+zb_status zb_create_from_mesh(const zb_mesh *mesh, const zb_params *params, zb_ctx **out);
+void zb_destroy(zb_ctx *ctx);
+zb_status zb_info_get(const zb_ctx *ctx, zb_info *out);
+
+/* Use a caller-provided CUDA stream (cudaStream_t) for all later work. */
+zb_status zb_set_stream(zb_ctx *ctx, void *stream);
+zb_status zb_set_dt(zb_ctx *ctx, double dt);
+
+/* State access with get_q_spts strides (in doubles).  where: ZB_HOST/ZB_DEVICE.
+ * zb_set_state copies and converts into the context's layout and precision. */
+zb_status zb_set_state(zb_ctx *ctx, const double *U, int64_t spt_stride, int64_t var_stride,
+                       int64_t ele_stride, int where);
+zb_status zb_get_state(zb_ctx *ctx, double *U, int64_t spt_stride, int64_t var_stride,
+                       int64_t ele_stride, int where);
+
+/* FRSolver::compute_residual(stage): divF_spts(stage) = |J| * div F in
+ * reference form (physical residual is -divF/|J|). */
+zb_status zb_compute_residual(zb_ctx *ctx, unsigned stage);
+zb_status zb_get_residual(zb_ctx *ctx, unsigned stage, double *out, int64_t spt_stride,
+                          int64_t var_stride, int64_t ele_stride, int where);
+
+/* One RK44 stage of FRSolver::step_RK (src/solver.cpp:2864-3097): residual of
+ * stage s, then U = U_ini - a_s dt/|J| divF_s, or on the last stage
+ * U = U_ini - sum_s b_s dt/|J| divF_s.  Stage 0 first saves U_ini. */
+zb_status zb_rk_stage(zb_ctx *ctx, unsigned stage);
+/* n full RK44 steps (FRSolver::update with dt_scheme RK44). */
+zb_status zb_step(zb_ctx *ctx, int n);
+
+/* Residual norms of report_residuals (src/solver.cpp:6990-7137), FP64 device
+ * reduction of divF(stage 0)/|J| per variable: out[3*nvars] = L1, L2, Linf. */
+zb_status zb_residual_norms(zb_ctx *ctx, double *out);
+
+/* Wait for all work queued on the context's stream. */
+zb_status zb_synchronize(zb_ctx *ctx);
+
+/* Number of kernels this library launched on the context since creation. */
+int64_t zb_launch_count(const zb_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZB_H */

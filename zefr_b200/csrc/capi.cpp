@@ -1,0 +1,326 @@
+// extern "C" boundary of libzefr_b200.so (declarations in include/zb.h).
+// Every C++ exception is caught here and turned into a status code plus a
+// thread-local message, the C-ABI analogue of the reference's ThrowException
+// (include/macros.hpp:52-54).
+#include <cstring>
+#include <string>
+
+#include "context.hpp"
+
+namespace zb {
+
+static thread_local std::string g_err;
+
+void set_last_error(const std::string &msg) { g_err = msg; }
+
+}  // namespace zb
+
+#define ZB_GUARD(...)                               \
+  try                                               \
+  {                                                 \
+    __VA_ARGS__;                                    \
+    return ZB_OK;                                   \
+  }                                                 \
+  catch (const zb::Error &e)                        \
+  {                                                 \
+    zb::set_last_error(e.what());                   \
+    return e.code;                                  \
+  }                                                 \
+  catch (const std::bad_alloc &)                    \
+  {                                                 \
+    zb::set_last_error("host allocation failed");   \
+    return ZB_ERR_NOMEM;                            \
+  }                                                 \
+  catch (const std::exception &e)                   \
+  {                                                 \
+    zb::set_last_error(e.what());                   \
+    return ZB_ERR_INTERNAL;                         \
+  }
+
+#define ZB_REQUIRE(cond, msg) \
+  if (!(cond)) ZB_THROW(ZB_ERR_ARG, msg)
+
+extern "C" {
+
+const char *zb_last_error(void) { return zb::g_err.c_str(); }
+
+const char *zb_version(void) { return "zefr_b200 0.1 (sm_100a)"; }
+
+zb_status zb_params_from_deck(const zb_deck *deck, zb_params *out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(deck && out, "null argument");
+    zb::params_from_deck(*deck, *out);
+  })
+}
+
+zb_status zb_mesh_read_gmsh(const char *path, int ndims, int n_map, const char *const *names, const int *bcs,
+                            zb_mesh **out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(path && out, "null argument");
+    ZB_REQUIRE(n_map >= 0 && (n_map == 0 || (names && bcs)), "bad boundary map");
+    std::vector<std::string> nm;
+    std::vector<int> bc;
+    for (int i = 0; i < n_map; i++)
+    {
+      nm.push_back(names[i]);
+      bc.push_back(bcs[i]);
+    }
+    auto *m = new zb::MeshData();
+    try
+    {
+      zb::read_gmsh(path, ndims, nm, bc, *m);
+    }
+    catch (...)
+    {
+      delete m;
+      throw;
+    }
+    // zb_mesh is the first member, so the view pointer doubles as the handle
+    static_assert(offsetof(zb::MeshData, view) == 0, "view must be first");
+    *out = &m->view;
+  })
+}
+
+void zb_mesh_free(zb_mesh *mesh)
+{
+  if (mesh) delete reinterpret_cast<zb::MeshData *>(mesh);
+}
+
+zb_status zb_plan_create(const zb_mesh *mesh, const zb_params *params, zb_plan **out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(mesh && params && out, "null argument");
+    auto *p = new zb_plan();
+    try
+    {
+      zb::build_plan(*mesh, *params, p->plan);
+    }
+    catch (...)
+    {
+      delete p;
+      throw;
+    }
+    *out = p;
+  })
+}
+
+void zb_plan_free(zb_plan *plan) { delete plan; }
+
+zb_status zb_plan_info(const zb_plan *plan, zb_info *out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(plan && out, "null argument");
+    const zb::Plan &p = plan->plan;
+    std::memset(out, 0, sizeof(*out));
+    out->ndims = p.ndims;
+    out->nvars = p.nvars;
+    out->nspts = p.nspts;
+    out->nfpts = p.nfpts;
+    out->order = p.order;
+    out->etype = p.etype;
+    out->n_eles = p.neles;
+    out->n_eles_pad = p.neles_pad;
+    out->n_gfpts_int = p.n_gfpts_int;
+    out->n_gfpts_bnd = p.n_gfpts_bnd;
+    out->n_gfpts = p.n_gfpts_int + p.n_gfpts_bnd;
+    out->nstages = 4;
+    out->tile = p.tile;
+    out->precision = p.params.precision;
+  })
+}
+
+zb_status zb_plan_get(const zb_plan *plan, const char *name, double *out, int64_t *n)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(plan && name && n, "null argument");
+    const zb::Plan &p = plan->plan;
+    std::string nm(name);
+    std::vector<double> tmp;
+    auto put = [&](const std::vector<double> &v) {
+      if (out == nullptr)
+      {
+        *n = (int64_t)v.size();
+        return;
+      }
+      ZB_REQUIRE(*n >= (int64_t)v.size(), "output buffer too small");
+      std::memcpy(out, v.data(), v.size() * sizeof(double));
+      *n = (int64_t)v.size();
+    };
+    if (nm == "coord_spts") put(p.coord_spts);
+    else if (nm == "coord_fpts") put(p.coord_fpts);
+    else if (nm == "jaco_det_spts") put(p.jaco_det_spts);
+    else if (nm == "inv_jaco_spts") put(p.inv_jaco_spts);
+    else if (nm == "fpt_norm") put(p.fnorm);
+    else if (nm == "fpt_dA") put(p.fdA);
+    else if (nm == "weights_spts") put(p.weights_spts);
+    else if (nm == "loc_spts") put(p.loc_spts);
+    else if (nm == "loc_fpts") put(p.loc_fpts);
+    else if (nm == "fpt_partner")
+    {
+      tmp.assign(p.partner.begin(), p.partner.end());
+      put(tmp);
+    }
+    else if (nm == "fpt_slot")
+    {
+      tmp.assign(p.slot.begin(), p.slot.end());
+      put(tmp);
+    }
+    else if (nm == "oppE" || nm == "oppD" || nm == "oppD_fpts" || nm == "oppDiv" || nm == "oppDiv_fpts")
+    {
+      std::vector<double> E, D, Df, Dv, Dvf;
+      p.dense_operators(E, D, Df, Dv, Dvf);
+      if (nm == "oppE") put(E);
+      else if (nm == "oppD") put(D);
+      else if (nm == "oppD_fpts") put(Df);
+      else if (nm == "oppDiv") put(Dv);
+      else put(Dvf);
+    }
+    else
+      ZB_THROW(ZB_ERR_ARG, "unknown plan array " + nm);
+  })
+}
+
+zb_status zb_create(const zb_plan *plan, zb_ctx **out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(plan && out, "null argument");
+    auto *c = new zb_ctx();
+    try
+    {
+      c->impl = zb::ctx_create(plan->plan);
+    }
+    catch (...)
+    {
+      delete c;
+      throw;
+    }
+    *out = c;
+  })
+}
+
+zb_status zb_create_from_mesh(const zb_mesh *mesh, const zb_params *params, zb_ctx **out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(mesh && params && out, "null argument");
+    zb_plan plan;
+    zb::build_plan(*mesh, *params, plan.plan);
+    auto *c = new zb_ctx();
+    try
+    {
+      c->impl = zb::ctx_create(plan.plan);
+    }
+    catch (...)
+    {
+      delete c;
+      throw;
+    }
+    *out = c;
+  })
+}
+
+void zb_destroy(zb_ctx *ctx)
+{
+  if (!ctx) return;
+  try
+  {
+    zb::ctx_destroy(ctx->impl);
+  }
+  catch (...)
+  {
+  }
+  delete ctx;
+}
+
+zb_status zb_info_get(const zb_ctx *ctx, zb_info *out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && out, "null argument");
+    zb::ctx_info(ctx->impl, out);
+  })
+}
+
+zb_status zb_set_stream(zb_ctx *ctx, void *stream)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_set_stream(ctx->impl, stream);
+  })
+}
+
+zb_status zb_set_dt(zb_ctx *ctx, double dt)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_set_dt(ctx->impl, dt);
+  })
+}
+
+zb_status zb_set_state(zb_ctx *ctx, const double *U, int64_t ss, int64_t vs, int64_t es, int where)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_set_state(ctx->impl, U, ss, vs, es, where);
+  })
+}
+
+zb_status zb_get_state(zb_ctx *ctx, double *U, int64_t ss, int64_t vs, int64_t es, int where)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_get_state(ctx->impl, U, ss, vs, es, where);
+  })
+}
+
+zb_status zb_compute_residual(zb_ctx *ctx, unsigned stage)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_compute_residual(ctx->impl, stage);
+  })
+}
+
+zb_status zb_get_residual(zb_ctx *ctx, unsigned stage, double *out, int64_t ss, int64_t vs, int64_t es, int where)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_get_residual(ctx->impl, stage, out, ss, vs, es, where);
+  })
+}
+
+zb_status zb_rk_stage(zb_ctx *ctx, unsigned stage)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_rk_stage(ctx->impl, stage);
+  })
+}
+
+zb_status zb_step(zb_ctx *ctx, int n)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_step(ctx->impl, n);
+  })
+}
+
+zb_status zb_residual_norms(zb_ctx *ctx, double *out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && out, "null argument");
+    zb::ctx_norms(ctx->impl, out);
+  })
+}
+
+zb_status zb_synchronize(zb_ctx *ctx)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_sync(ctx->impl);
+  })
+}
+
+int64_t zb_launch_count(const zb_ctx *ctx) { return ctx ? zb::ctx_launches(ctx->impl) : -1; }
+
+}  // extern "C"

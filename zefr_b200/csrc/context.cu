@@ -1,0 +1,645 @@
+// Device context: buffers in the tile-major layout, layout conversion, kernel
+// dispatch over (dimension, order, precision) and explicit RK44 stepping.
+#include <cstring>
+#include <cmath>
+#include <mutex>
+
+#include "context.hpp"
+#include "dfr_kernels.cuh"
+
+namespace zb {
+
+using dev::Args;
+using dev::LineOpsT;
+using dev::Shape;
+using dev::TW;
+
+#define CK(x)                                                                                  \
+  do                                                                                           \
+  {                                                                                            \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct StageCfg
+{
+  unsigned stage;
+  int rk_mode;      // 0 none, 1 stage update, 2 final combination
+  int save_ini;
+  int extrap_next;
+};
+
+// RK44 tables (src/solver.cpp:722-735)
+static const double kRkAlpha[3] = {0.5, 0.5, 1.0};
+static const double kRkBeta[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+
+struct Ctx
+{
+  Plan plan;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int prec = ZB_FP64;
+  size_t tsz = 8;
+  int D = 0, N = 0, S = 0, Fp = 0, V = 0, nstages = 4;
+  int64_t ntiles = 0;
+  void *U = nullptr, *U_ini = nullptr, *divF[4] = {nullptr, nullptr, nullptr, nullptr};
+  void *divF_vol = nullptr, *Ufp[2] = {nullptr, nullptr}, *Fvn = nullptr, *mets = nullptr, *fgeo = nullptr;
+  void *Ucomp = nullptr;
+  int *nbr = nullptr;
+  double *dtmp = nullptr;
+  size_t dtmp_bytes = 0;
+  double *dred = nullptr;
+  int cur = 0;
+  bool ufp_valid = false;
+  double dt = 0.0;
+  int64_t launches = 0;
+  void (*launch_extrap)(Ctx &) = nullptr;
+  void (*launch_stage)(Ctx &, const StageCfg &) = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// layout conversion kernels
+// ---------------------------------------------------------------------------
+
+// reference-strided FP64 -> tile-major T; padded elements copy element 0
+template <typename T>
+__global__ void k_to_tiles(const double *__restrict__ src, T *__restrict__ dst, T *__restrict__ comp, int64_t neles,
+                           int64_t ntiles, int npts, int nv, int64_t ss, int64_t vs, int64_t es)
+{
+  const int64_t total = ntiles * npts * nv * TW;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int l = (int)(i % TW);
+    const int v = (int)((i / TW) % nv);
+    const int p = (int)((i / ((int64_t)TW * nv)) % npts);
+    const int64_t t = i / ((int64_t)TW * nv * npts);
+    int64_t e = t * TW + l;
+    if (e >= neles) e = 0;
+    dst[i] = (T)src[p * ss + v * vs + e * es];
+    if (comp) comp[i] = T(0);
+  }
+}
+
+template <typename T>
+__global__ void k_from_tiles(const T *__restrict__ srcT, const T *__restrict__ comp, double *__restrict__ dst,
+                             int64_t neles, int npts, int nv, int64_t ss, int64_t vs, int64_t es)
+{
+  const int64_t total = neles * npts * nv;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int64_t e = i % neles;
+    const int v = (int)((i / neles) % nv);
+    const int p = (int)(i / (neles * nv));
+    const int64_t t = e / TW;
+    const int l = (int)(e % TW);
+    const int64_t j = ((t * npts + p) * nv + v) * TW + l;
+    double val = (double)srcT[j];
+    if (comp) val -= (double)comp[j];
+    dst[p * ss + v * vs + e * es] = val;
+  }
+}
+
+// FP64 residual norms of report_residuals: max, sum |r|, sum r^2 with r = divF/|J|
+template <typename T>
+__global__ void k_norms(const T *__restrict__ divF, const T *__restrict__ mets, int64_t neles, int S, int V, int NM,
+                        int DD, double *out)
+{
+  __shared__ double red[3][8][32];
+  double mx[8], l1[8], l2[8];
+  for (int v = 0; v < 8; v++) mx[v] = l1[v] = l2[v] = 0.0;
+  const int64_t npts = neles * S;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int64_t e = i % neles;
+    const int s = (int)(i / neles);
+    const int64_t t = e / TW;
+    const int l = (int)(e % TW);
+    const double det = (double)mets[((t * S + s) * NM + DD) * TW + l];
+    for (int v = 0; v < V; v++)
+    {
+      const double r = (double)divF[((t * S + s) * V + v) * TW + l] / det;
+      const double a = fabs(r);
+      mx[v] = (a > mx[v] || a != a) ? a : mx[v];
+      l1[v] += a;
+      l2[v] += r * r;
+    }
+  }
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  for (int v = 0; v < V; v++)
+  {
+    for (int o = 16; o > 0; o /= 2)
+    {
+      const double m2 = __shfl_down_sync(0xffffffff, mx[v], o);
+      mx[v] = (m2 > mx[v] || m2 != m2) ? m2 : mx[v];
+      l1[v] += __shfl_down_sync(0xffffffff, l1[v], o);
+      l2[v] += __shfl_down_sync(0xffffffff, l2[v], o);
+    }
+    if (lane == 0)
+    {
+      red[0][v][warp] = mx[v];
+      red[1][v][warp] = l1[v];
+      red[2][v][warp] = l2[v];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < V)
+  {
+    const int v = threadIdx.x;
+    double m = 0, s1 = 0, s2 = 0;
+    for (int w = 0; w < (int)(blockDim.x / 32); w++)
+    {
+      m = (red[0][v][w] > m || red[0][v][w] != red[0][v][w]) ? red[0][v][w] : m;
+      s1 += red[1][v][w];
+      s2 += red[2][v][w];
+    }
+    // non-negative doubles order like their bit patterns; NaN (0x7ff8...) wins
+    atomicMax(reinterpret_cast<unsigned long long *>(&out[v]), (unsigned long long)__double_as_longlong(m));
+    atomicAdd(&out[V + v], s1);
+    atomicAdd(&out[2 * V + v], s2);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dispatch
+// ---------------------------------------------------------------------------
+
+template <typename T, int N>
+static LineOpsT<T, N> line_ops(const Plan &p)
+{
+  LineOpsT<T, N> o;
+  for (int i = 0; i < N * N; i++) o.Dm[i] = (T)p.ops.D[i];
+  for (int i = 0; i < N; i++)
+  {
+    o.Em[i] = (T)p.ops.Em[i];
+    o.Ep[i] = (T)p.ops.Ep[i];
+    o.Dbm[i] = (T)p.ops.Dbm[i];
+    o.Dbp[i] = (T)p.ops.Dbp[i];
+  }
+  return o;
+}
+
+template <typename T>
+static dev::Phys<T> phys_of(const zb_params &p)
+{
+  dev::Phys<T> ph;
+  ph.gamma = (T)p.gamma;
+  ph.prandtl = (T)p.prandtl;
+  ph.mu = (T)p.mu;
+  ph.rt = (T)p.rt;
+  ph.c_sth = (T)p.c_sth;
+  ph.rus_k = (T)p.rus_k;
+  ph.ldg_b = (T)p.ldg_b;
+  ph.ldg_tau = (T)p.ldg_tau;
+  ph.rho_fs = (T)p.rho_fs;
+  ph.P_fs = (T)p.P_fs;
+  ph.T_wall = (T)p.T_wall;
+  ph.R_ref = (T)p.R_ref;
+  for (int d = 0; d < 3; d++)
+  {
+    ph.V_fs[d] = (T)p.V_fs[d];
+    ph.V_wall[d] = (T)p.V_wall[d];
+  }
+  ph.fix_vis = p.fix_vis;
+  ph.fconv = p.fconv;
+  return ph;
+}
+
+static int grid_for(int64_t work, int threads)
+{
+  int64_t b = (work + threads - 1) / threads;
+  if (b > 148 * 64) b = 148 * 64;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+template <typename T, int D, int N>
+static void launch_extrap_impl(Ctx &c)
+{
+  using G = Shape<D, N>;
+  const int64_t work = c.ntiles * G::Fp * TW;
+  dev::k_extrap<T, D, N><<<grid_for(work, 256), 256, 0, c.stream>>>((const T *)c.U, (T *)c.Ufp[c.cur], c.ntiles,
+                                                                      line_ops<T, N>(c.plan));
+  c.launches++;
+  CK(cudaGetLastError());
+}
+
+template <typename K>
+static void set_smem(K kernel, size_t bytes)
+{
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+template <typename T, int D, int N>
+static void launch_stage_impl(Ctx &c, const StageCfg &sc)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V, NT = G::NT;
+  Args<T> a;
+  std::memset(&a, 0, sizeof(a));
+  a.U = (const T *)c.U;
+  a.Ufp = (const T *)c.Ufp[c.cur];
+  a.Ufp_next = (T *)c.Ufp[c.cur ^ 1];
+  a.mets = (const T *)c.mets;
+  a.fgeo = (const T *)c.fgeo;
+  a.nbr = c.nbr;
+  a.divF = (T *)c.divF[sc.stage];
+  a.divF_vol = (T *)c.divF_vol;
+  a.Fvn = (T *)c.Fvn;
+  a.rk_mode = sc.rk_mode;
+  a.save_ini = sc.save_ini;
+  a.extrap_next = sc.extrap_next;
+  a.Uout = (T *)c.U;
+  a.U_ini = (T *)c.U_ini;
+  a.Ucomp = nullptr;
+  a.dt = (T)c.dt;
+  a.ntiles = c.ntiles;
+  a.ph = phys_of<T>(c.plan.params);
+  if (sc.rk_mode == 1)
+    a.rk_coef[0] = (T)kRkAlpha[sc.stage];
+  else if (sc.rk_mode == 2)
+  {
+    a.nprev = (int)sc.stage;
+    for (unsigned s = 0; s <= sc.stage; s++) a.rk_coef[s] = (T)kRkBeta[s];
+    for (unsigned s = 0; s < sc.stage; s++) a.divF_prev[s] = (const T *)c.divF[s];
+    if (c.prec == ZB_MIXED) a.Ucomp = (T *)c.Ucomp;
+  }
+  const LineOpsT<T, N> ops = line_ops<T, N>(c.plan);
+  const size_t ops_bytes = sizeof(LineOpsT<T, N>);
+  if (!c.plan.params.viscous)
+  {
+    const size_t smem = (size_t)(S * V + D * S * V + Fp * V) * TW * sizeof(T) + ops_bytes;
+    set_smem(dev::k_euler<T, D, N>, smem);
+    dev::k_euler<T, D, N><<<(unsigned)c.ntiles, NT, smem, c.stream>>>(a, ops);
+    c.launches++;
+    CK(cudaGetLastError());
+  }
+  else
+  {
+    const size_t smem1 = (size_t)(S * V + Fp * V + D * S * V) * TW * sizeof(T) + ops_bytes;
+    set_smem(dev::k_ns_grad<T, D, N>, smem1);
+    dev::k_ns_grad<T, D, N><<<(unsigned)c.ntiles, NT, smem1, c.stream>>>(a, ops);
+    c.launches++;
+    CK(cudaGetLastError());
+    const size_t smem2 = (size_t)(Fp * V + S * V) * TW * sizeof(T) + ops_bytes;
+    set_smem(dev::k_ns_face<T, D, N>, smem2);
+    dev::k_ns_face<T, D, N><<<(unsigned)c.ntiles, NT, smem2, c.stream>>>(a, ops);
+    c.launches++;
+    CK(cudaGetLastError());
+  }
+  if (sc.extrap_next) c.cur ^= 1;
+}
+
+template <typename T, int D, int N>
+static void bind(Ctx &c)
+{
+  c.launch_extrap = &launch_extrap_impl<T, D, N>;
+  c.launch_stage = &launch_stage_impl<T, D, N>;
+}
+
+template <typename T>
+static void bind_t(Ctx &c)
+{
+  const int D = c.D, N = c.N;
+#define ZB_BIND(DD, NN) \
+  if (D == DD && N == NN) { bind<T, DD, NN>(c); return; }
+  ZB_BIND(2, 2) ZB_BIND(2, 3) ZB_BIND(2, 4) ZB_BIND(2, 5) ZB_BIND(2, 6)
+  ZB_BIND(3, 2) ZB_BIND(3, 3) ZB_BIND(3, 4) ZB_BIND(3, 5)
+#undef ZB_BIND
+  ZB_THROW(ZB_ERR_UNSUPPORTED, "no kernels built for ndims=" + std::to_string(D) + " P=" + std::to_string(N - 1));
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+
+static void *dalloc(size_t bytes)
+{
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+  if (e != cudaSuccess)
+  {
+    cudaGetLastError();
+    ZB_THROW(ZB_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  return p;
+}
+
+static void free_all(Ctx *c)
+{
+  void *bufs[] = {c->U, c->U_ini, c->divF[0], c->divF[1], c->divF[2], c->divF[3], c->divF_vol, c->Ufp[0],
+                  c->Ufp[1], c->Fvn, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+}
+
+template <typename T>
+static void upload_static(Ctx &c)
+{
+  const Plan &p = c.plan;
+  const int64_t E = p.neles, nt = c.ntiles;
+  const int S = c.S, Fp = c.Fp, D = c.D, NM = D * D + 1;
+  std::vector<T> mets((size_t)nt * S * NM * TW);
+  std::vector<T> fgeo((size_t)nt * Fp * (D + 1) * TW);
+  std::vector<int> nbr((size_t)nt * Fp * TW);
+  for (int64_t t = 0; t < nt; t++)
+    for (int l = 0; l < TW; l++)
+    {
+      int64_t e = t * TW + l;
+      const bool pad = (e >= E);
+      const int64_t es = pad ? 0 : e;
+      for (int s = 0; s < S; s++)
+      {
+        for (int d1 = 0; d1 < D; d1++)
+          for (int d2 = 0; d2 < D; d2++)
+            mets[((t * S + s) * NM + d1 * D + d2) * TW + l] =
+                (T)p.inv_jaco_spts[(((size_t)d1 * S + s) * D + d2) * E + es];
+        mets[((t * S + s) * NM + D * D) * TW + l] = (T)p.jaco_det_spts[(size_t)s * E + es];
+      }
+      for (int f = 0; f < Fp; f++)
+      {
+        for (int d = 0; d < D; d++)
+          fgeo[((t * Fp + f) * (D + 1) + d) * TW + l] = (T)p.fnorm[((size_t)f * D + d) * E + es];
+        fgeo[((t * Fp + f) * (D + 1) + D) * TW + l] = (T)p.fdA[(size_t)f * E + es];
+        int code;
+        if (pad)
+        {
+          code = 2 * (int)((t * Fp + f) * TW + l);  // pair with itself
+        }
+        else
+        {
+          const int64_t pr = p.partner[(size_t)f * E + e];
+          if (pr < 0)
+            code = (int)pr;
+          else
+          {
+            const int64_t e2 = pr / Fp;
+            const int f2 = (int)(pr % Fp);
+            const int64_t pidx = ((e2 / TW) * Fp + f2) * TW + (e2 % TW);
+            if (pidx >= (int64_t(1) << 30)) ZB_THROW(ZB_ERR_UNSUPPORTED, "mesh too large for 32-bit face index");
+            code = (int)(2 * pidx + p.slot[(size_t)f * E + e]);
+          }
+        }
+        nbr[(t * Fp + f) * TW + l] = code;
+      }
+    }
+  CK(cudaMemcpyAsync(c.mets, mets.data(), mets.size() * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemcpyAsync(c.fgeo, fgeo.data(), fgeo.size() * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemcpyAsync(c.nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+}
+
+Ctx *ctx_create(const Plan &plan)
+{
+  std::unique_ptr<Ctx> c(new Ctx());
+  c->plan = plan;
+  CK(cudaGetDevice(&c->dev));
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  c->own_stream = true;
+  c->prec = plan.params.precision;
+  if (c->prec != ZB_FP64 && c->prec != ZB_MIXED) ZB_THROW(ZB_ERR_ARG, "unknown precision");
+  c->tsz = (c->prec == ZB_FP64) ? sizeof(double) : sizeof(float);
+  c->D = plan.ndims;
+  c->N = plan.N;
+  c->S = plan.nspts;
+  c->Fp = plan.nfpts;
+  c->V = plan.nvars;
+  c->ntiles = plan.ntiles;
+  c->dt = plan.params.dt;
+  if (plan.tile != TW) ZB_THROW(ZB_ERR_INTERNAL, "plan tile width does not match kernels");
+  if (c->prec == ZB_FP64)
+    bind_t<double>(*c);
+  else
+    bind_t<float>(*c);
+  try
+  {
+    const size_t nU = (size_t)c->ntiles * c->S * c->V * TW;
+    const size_t nF = (size_t)c->ntiles * c->Fp * c->V * TW;
+    c->U = dalloc(nU * c->tsz);
+    c->U_ini = dalloc(nU * c->tsz);
+    for (int s = 0; s < c->nstages; s++) c->divF[s] = dalloc(nU * c->tsz);
+    c->Ufp[0] = dalloc(nF * c->tsz);
+    c->Ufp[1] = dalloc(nF * c->tsz);
+    if (plan.params.viscous)
+    {
+      c->divF_vol = dalloc(nU * c->tsz);
+      c->Fvn = dalloc(nF * c->tsz);
+    }
+    if (c->prec == ZB_MIXED) c->Ucomp = dalloc(nU * c->tsz);
+    c->mets = dalloc((size_t)c->ntiles * c->S * (c->D * c->D + 1) * TW * c->tsz);
+    c->fgeo = dalloc((size_t)c->ntiles * c->Fp * (c->D + 1) * TW * c->tsz);
+    c->nbr = (int *)dalloc((size_t)c->ntiles * c->Fp * TW * sizeof(int));
+    c->dred = (double *)dalloc(3 * 8 * sizeof(double));
+    if (c->prec == ZB_FP64)
+      upload_static<double>(*c);
+    else
+      upload_static<float>(*c);
+    // zero the state so a residual before set_state is well defined (all zeros)
+    CK(cudaMemsetAsync(c->U, 0, nU * c->tsz, c->stream));
+    if (c->Ucomp) CK(cudaMemsetAsync(c->Ucomp, 0, nU * c->tsz, c->stream));
+    for (int s = 0; s < c->nstages; s++) CK(cudaMemsetAsync(c->divF[s], 0, nU * c->tsz, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  catch (...)
+  {
+    free_all(c.get());
+    throw;
+  }
+  return c.release();
+}
+
+void ctx_destroy(Ctx *c)
+{
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_all(c);
+  delete c;
+}
+
+void ctx_info(const Ctx *c, zb_info *out)
+{
+  const Plan &p = c->plan;
+  out->ndims = p.ndims;
+  out->nvars = p.nvars;
+  out->nspts = p.nspts;
+  out->nfpts = p.nfpts;
+  out->order = p.order;
+  out->etype = p.etype;
+  out->n_eles = p.neles;
+  out->n_eles_pad = p.neles_pad;
+  out->n_gfpts = p.n_gfpts_int + p.n_gfpts_bnd;
+  out->n_gfpts_int = p.n_gfpts_int;
+  out->n_gfpts_bnd = p.n_gfpts_bnd;
+  out->nstages = c->nstages;
+  out->tile = TW;
+  out->precision = c->prec;
+}
+
+void ctx_set_stream(Ctx *c, void *stream)
+{
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  c->stream = (cudaStream_t)stream;
+  c->own_stream = false;
+}
+
+void ctx_set_dt(Ctx *c, double dt) { c->dt = dt; }
+
+static const double *stage_in(Ctx *c, const double *src, size_t extent_elems, int where)
+{
+  if (where == ZB_DEVICE) return src;
+  const size_t bytes = extent_elems * sizeof(double);
+  if (bytes > c->dtmp_bytes)
+  {
+    if (c->dtmp) cudaFree(c->dtmp);
+    c->dtmp = nullptr;
+    c->dtmp = (double *)dalloc(bytes);
+    c->dtmp_bytes = bytes;
+  }
+  CK(cudaMemcpyAsync(c->dtmp, src, bytes, cudaMemcpyHostToDevice, c->stream));
+  return c->dtmp;
+}
+
+static size_t extent(const Ctx *c, int64_t ss, int64_t vs, int64_t es, int npts)
+{
+  if (ss < 0 || vs < 0 || es < 0) ZB_THROW(ZB_ERR_ARG, "negative strides are not supported");
+  return (size_t)((npts - 1) * ss + (c->V - 1) * vs + (c->plan.neles - 1) * es + 1);
+}
+
+void ctx_set_state(Ctx *c, const double *U, int64_t ss, int64_t vs, int64_t es, int where)
+{
+  if (!U) ZB_THROW(ZB_ERR_ARG, "null state");
+  const size_t ext = extent(c, ss, vs, es, c->S);
+  const double *src = stage_in(c, U, ext, where);
+  const int64_t work = c->ntiles * c->S * c->V * TW;
+  if (c->prec == ZB_FP64)
+    k_to_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>(src, (double *)c->U, nullptr, c->plan.neles,
+                                                                     c->ntiles, c->S, c->V, ss, vs, es);
+  else
+    k_to_tiles<float><<<grid_for(work, 256), 256, 0, c->stream>>>(src, (float *)c->U, (float *)c->Ucomp,
+                                                                    c->plan.neles, c->ntiles, c->S, c->V, ss, vs, es);
+  c->launches++;
+  CK(cudaGetLastError());
+  if (where == ZB_HOST) CK(cudaStreamSynchronize(c->stream));
+  c->ufp_valid = false;
+}
+
+static void from_tiles(Ctx *c, const void *srcT, const void *comp, double *out, int64_t ss, int64_t vs, int64_t es,
+                       int where)
+{
+  const size_t ext = extent(c, ss, vs, es, c->S);
+  double *dst = out;
+  if (where == ZB_HOST)
+  {
+    const size_t bytes = ext * sizeof(double);
+    if (bytes > c->dtmp_bytes)
+    {
+      if (c->dtmp) cudaFree(c->dtmp);
+      c->dtmp = nullptr;
+      c->dtmp = (double *)dalloc(bytes);
+      c->dtmp_bytes = bytes;
+    }
+    dst = c->dtmp;
+    // keep caller's holes intact: start from the caller's buffer
+    CK(cudaMemcpyAsync(dst, out, bytes, cudaMemcpyHostToDevice, c->stream));
+  }
+  const int64_t work = c->plan.neles * c->S * c->V;
+  if (c->prec == ZB_FP64)
+    k_from_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>((const double *)srcT, (const double *)comp, dst,
+                                                                       c->plan.neles, c->S, c->V, ss, vs, es);
+  else
+    k_from_tiles<float><<<grid_for(work, 256), 256, 0, c->stream>>>((const float *)srcT, (const float *)comp, dst,
+                                                                      c->plan.neles, c->S, c->V, ss, vs, es);
+  c->launches++;
+  CK(cudaGetLastError());
+  if (where == ZB_HOST)
+  {
+    CK(cudaMemcpyAsync(out, dst, ext * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+}
+
+void ctx_get_state(Ctx *c, double *U, int64_t ss, int64_t vs, int64_t es, int where)
+{
+  if (!U) ZB_THROW(ZB_ERR_ARG, "null state");
+  from_tiles(c, c->U, c->Ucomp, U, ss, vs, es, where);
+}
+
+static void ensure_ufp(Ctx *c)
+{
+  if (!c->ufp_valid)
+  {
+    c->launch_extrap(*c);
+    c->ufp_valid = true;
+  }
+}
+
+void ctx_compute_residual(Ctx *c, unsigned stage)
+{
+  if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  ensure_ufp(c);
+  StageCfg sc{stage, 0, 0, 0};
+  c->launch_stage(*c, sc);
+}
+
+void ctx_get_residual(Ctx *c, unsigned stage, double *out, int64_t ss, int64_t vs, int64_t es, int where)
+{
+  if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  if (!out) ZB_THROW(ZB_ERR_ARG, "null output");
+  from_tiles(c, c->divF[stage], nullptr, out, ss, vs, es, where);
+}
+
+void ctx_rk_stage(Ctx *c, unsigned stage)
+{
+  if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  ensure_ufp(c);
+  StageCfg sc;
+  sc.stage = stage;
+  sc.rk_mode = (stage + 1 < (unsigned)c->nstages) ? 1 : 2;
+  sc.save_ini = (stage == 0);
+  sc.extrap_next = 1;
+  c->launch_stage(*c, sc);
+}
+
+void ctx_step(Ctx *c, int n)
+{
+  if (n < 0) ZB_THROW(ZB_ERR_ARG, "negative step count");
+  for (int i = 0; i < n; i++)
+    for (int s = 0; s < c->nstages; s++) ctx_rk_stage(c, (unsigned)s);
+}
+
+void ctx_norms(Ctx *c, double *out)
+{
+  const int V = c->V;
+  CK(cudaMemsetAsync(c->dred, 0, 3 * 8 * sizeof(double), c->stream));
+  const int64_t work = c->plan.neles * c->S;
+  const int blocks = grid_for(work, 256);
+  if (c->prec == ZB_FP64)
+    k_norms<double><<<blocks, 256, 0, c->stream>>>((const double *)c->divF[0], (const double *)c->mets, c->plan.neles,
+                                                   c->S, V, c->D * c->D + 1, c->D * c->D, c->dred);
+  else
+    k_norms<float><<<blocks, 256, 0, c->stream>>>((const float *)c->divF[0], (const float *)c->mets, c->plan.neles,
+                                                  c->S, V, c->D * c->D + 1, c->D * c->D, c->dred);
+  c->launches++;
+  CK(cudaGetLastError());
+  double h[24];
+  CK(cudaMemcpyAsync(h, c->dred, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const double ndof = (double)c->plan.neles * c->S;
+  bool bad = false;
+  for (int v = 0; v < V; v++)
+  {
+    out[v] = h[v] / ndof;
+    out[V + v] = h[V + v] / ndof;
+    out[2 * V + v] = std::sqrt(h[2 * V + v]) / ndof;
+    if (!std::isfinite(h[v]) || !std::isfinite(h[V + v]) || !std::isfinite(h[2 * V + v])) bad = true;
+  }
+  if (bad) ZB_THROW(ZB_ERR_NONFINITE, "NaN in residual");
+}
+
+void ctx_sync(Ctx *c) { CK(cudaStreamSynchronize(c->stream)); }
+
+int64_t ctx_launches(const Ctx *c) { return c->launches; }
+
+}  // namespace zb

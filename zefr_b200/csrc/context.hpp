@@ -1,0 +1,39 @@
+// Device context of the DFR residual (opaque zb_ctx of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+
+#include "zb_internal.hpp"
+
+struct zb_plan
+{
+  zb::Plan plan;
+};
+
+namespace zb {
+
+struct Ctx;
+
+Ctx *ctx_create(const Plan &plan);
+void ctx_destroy(Ctx *c);
+void ctx_info(const Ctx *c, zb_info *out);
+void ctx_set_stream(Ctx *c, void *stream);
+void ctx_set_dt(Ctx *c, double dt);
+void ctx_set_state(Ctx *c, const double *U, int64_t ss, int64_t vs, int64_t es, int where);
+void ctx_get_state(Ctx *c, double *U, int64_t ss, int64_t vs, int64_t es, int where);
+void ctx_compute_residual(Ctx *c, unsigned stage);
+void ctx_get_residual(Ctx *c, unsigned stage, double *out, int64_t ss, int64_t vs, int64_t es, int where);
+void ctx_rk_stage(Ctx *c, unsigned stage);
+void ctx_step(Ctx *c, int n);
+void ctx_norms(Ctx *c, double *out);
+void ctx_sync(Ctx *c);
+int64_t ctx_launches(const Ctx *c);
+
+}  // namespace zb
+
+struct zb_ctx
+{
+  zb::Ctx *impl;
+};

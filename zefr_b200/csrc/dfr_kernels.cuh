@@ -1,0 +1,759 @@
+// Tensor-product DFR residual kernels for quadrilaterals (D = 2) and
+// hexahedra (D = 3) of order P = N - 1, templated on the arithmetic type.
+//
+// Data layout in HBM is tile-major structure-of-arrays: TW consecutive
+// elements form a tile and every per-element array is stored as
+//   [tile][point][component][TW]
+// so one CTA reads its whole tile as one contiguous chunk and, inside it, the
+// TW elements of a (point, component) pair sit in one 32- or 64-byte run.
+//
+// Reference: the residual is FRSolver::compute_residual (src/solver.cpp:1494-
+// 1645).  Its dense operator products (src/elements.cpp:1337-1501) are applied
+// here as line operators: every nonzero of oppE, oppD, oppD_fpts, oppDiv and
+// oppDiv_fpts for quads and hexes lies on the line of points through a
+// solution point (src/elements.cpp:592-655), and the nonzeros are summed in the
+// same order as the reference's row-major products.
+#pragma once
+
+#include <cstdint>
+
+#include "physics.cuh"
+
+namespace zb {
+namespace dev {
+
+constexpr int TW = 8;  // elements per tile
+
+template <int D, int N>
+struct Shape
+{
+  static constexpr int S = (D == 2) ? N * N : N * N * N;
+  static constexpr int NF = (D == 2) ? N : N * N;  // flux points per face
+  static constexpr int Fp = 2 * D * NF;
+  static constexpr int V = D + 2;
+  static constexpr int NM = D * D + 1;  // adjugate entries + |J|
+  static constexpr int NT = (D == 2) ? ((S * TW <= 128) ? 128 : 256) : 256;
+};
+
+template <typename T, int N>
+struct LineOpsT
+{
+  T Dm[N * N];  // Dm[i*N+m] = l'_{m+1}(x_i) on [-1, x, 1]
+  T Em[N], Ep[N], Dbm[N], Dbp[N];
+};
+
+template <typename T>
+struct Args
+{
+  const T *U;        // [tile][S][V][TW]
+  const T *Ufp;      // [tile][Fp][V][TW] extrapolated state (this stage)
+  T *Ufp_next;       // extrapolation of the updated state (next stage)
+  const T *mets;     // [tile][S][NM][TW]: adj[d1][d2] (reference inv_jaco), |J|
+  const T *fgeo;     // [tile][Fp][D+1][TW]: face unit normal (left side), own dA
+  const int *nbr;    // [tile][Fp][TW]: 2*partner+slot, or -1-bc
+  T *divF;           // [tile][S][V][TW] residual of this stage
+  T *divF_vol;       // NS: volume part of the residual
+  T *Fvn;            // NS: viscous normal flux at own flux points
+  // RK update fused into the last kernel of a stage
+  int rk_mode;       // 0: none; 1: U = U_ini - a dt/|J| divF; 2: final combination
+  int save_ini;      // stage 0: write U_ini = U before updating
+  int extrap_next;   // write Ufp_next from the updated state
+  int nprev;         // final stage: number of earlier divF registers
+  T *Uout;           // updated state (may alias U)
+  T *U_ini;          // RK start state
+  T *Ucomp;          // compensated-summation remainder (final stage, nullptr = off)
+  const T *divF_prev[6];
+  T rk_coef[6];      // a_s (mode 1: [0]) or b_s (mode 2)
+  T dt;
+  int64_t ntiles;
+  Phys<T> ph;
+};
+
+// Flux point f -> normal dimension, side (-1/+1), first spt of its line and
+// stride along the line (orderings of src/quads.cpp:108-148, src/hexas.cpp:148-205).
+template <int D, int N>
+__device__ __forceinline__ void fpt_line(int f, int &dim, int &side, int &base, int &stride)
+{
+  if (D == 2)
+  {
+    const int face = f / N, j = f % N;
+    switch (face)
+    {
+      case 0: dim = 1; side = -1; base = j; stride = N; break;
+      case 1: dim = 0; side = 1; base = N * j; stride = 1; break;
+      case 2: dim = 1; side = 1; base = N - 1 - j; stride = N; break;
+      default: dim = 0; side = -1; base = N * (N - 1 - j); stride = 1; break;
+    }
+  }
+  else
+  {
+    constexpr int N2 = N * N;
+    const int face = f / N2, r = f % N2, j = r / N, k = r % N;
+    switch (face)
+    {
+      case 0: dim = 2; side = -1; base = k + N * j; stride = N2; break;
+      case 1: dim = 2; side = 1; base = (N - 1 - k) + N * j; stride = N2; break;
+      case 2: dim = 0; side = -1; base = N * k + N2 * j; stride = 1; break;
+      case 3: dim = 0; side = 1; base = N * (N - 1 - k) + N2 * j; stride = 1; break;
+      case 4: dim = 1; side = -1; base = (N - 1 - k) + N2 * j; stride = N; break;
+      default: dim = 1; side = 1; base = k + N2 * j; stride = N; break;
+    }
+  }
+}
+
+// Solution point s: line coordinate along dimension d and the flux points at
+// the -/+ ends of that line.
+template <int D, int N>
+__device__ __forceinline__ void spt_ends(int s, int d, int &i, int &fm, int &fp)
+{
+  if (D == 2)
+  {
+    const int ix = s % N, iy = s / N;
+    if (d == 0) { i = ix; fm = 3 * N + (N - 1 - iy); fp = N + iy; }
+    else { i = iy; fm = ix; fp = 2 * N + (N - 1 - ix); }
+  }
+  else
+  {
+    constexpr int N2 = N * N;
+    const int ix = s % N, iy = (s / N) % N, iz = s / N2;
+    if (d == 0) { i = ix; fm = 2 * N2 + iz * N + iy; fp = 3 * N2 + iz * N + (N - 1 - iy); }
+    else if (d == 1) { i = iy; fm = 4 * N2 + iz * N + (N - 1 - ix); fp = 5 * N2 + iz * N + ix; }
+    else { i = iz; fm = iy * N + ix; fp = N2 + iy * N + (N - 1 - ix); }
+  }
+}
+
+template <int N>
+__device__ __forceinline__ constexpr int pow_n(int d)
+{
+  return d == 0 ? 1 : (d == 1 ? N : N * N);
+}
+
+// Face id -> (dimension, side) for summing surface terms in flux point order.
+template <int D>
+__device__ __forceinline__ void face_dim_side(int face, int &dim, int &side)
+{
+  if (D == 2)
+  {
+    dim = (face == 0 || face == 2) ? 1 : 0;
+    side = (face == 1 || face == 2) ? 1 : -1;
+  }
+  else
+  {
+    dim = (face < 2) ? 2 : (face < 4 ? 0 : 1);
+    side = (face % 2 == 0) ? -1 : 1;
+  }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void load_ops(T *sops, const LineOpsT<T, N> &ops)
+{
+  const T *src = reinterpret_cast<const T *>(&ops);
+  constexpr int n = N * N + 4 * N;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sops[i] = src[i];
+}
+
+// Shared-memory views of the line operators
+template <typename T, int N>
+struct SOps
+{
+  const T *Dm, *Em, *Ep, *Dbm, *Dbp;
+  __device__ SOps(const T *p) : Dm(p), Em(p + N * N), Ep(p + N * N + N), Dbm(p + N * N + 2 * N), Dbp(p + N * N + 3 * N) {}
+};
+
+// extrapolate component v of the tile state in smem (layout [S][V][TW]) to flux point f
+template <typename T, int D, int N>
+__device__ __forceinline__ T extrap_smem(const T *sX, const SOps<T, N> &o, int f, int v, int l, int nv)
+{
+  int dim, side, base, stride;
+  fpt_line<D, N>(f, dim, side, base, stride);
+  const T *E = side < 0 ? o.Em : o.Ep;
+  T acc = E[0] * sX[((base)*nv + v) * TW + l];
+#pragma unroll
+  for (int m = 1; m < N; m++) acc += E[m] * sX[((base + m * stride) * nv + v) * TW + l];
+  return acc;
+}
+
+// read the neighbour's copy of a [tile][Fp][V][TW] array
+template <typename T, int V>
+__device__ __forceinline__ void gather_fpt(const T *A, int pidx, T out[V])
+{
+  const int64_t row = (int64_t)(pidx / TW) * V;
+  const int lane = pidx % TW;
+#pragma unroll
+  for (int v = 0; v < V; v++) out[v] = A[(row + v) * TW + lane];
+}
+
+// ---------------------------------------------------------------------------
+// Extrapolate the state to flux points: U_fpts = oppE U_spts (src/elements.cpp:1337-1360)
+// ---------------------------------------------------------------------------
+template <typename T, int D, int N>
+__global__ void __launch_bounds__(256) k_extrap(const T *__restrict__ U, T *__restrict__ Ufp, int64_t ntiles,
+                                                LineOpsT<T, N> ops)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V;
+  const int64_t total = ntiles * Fp * TW;
+  for (int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gid < total; gid += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int l = (int)(gid % TW);
+    const int f = (int)((gid / TW) % Fp);
+    const int64_t tile = gid / ((int64_t)TW * Fp);
+    int dim, side, base, stride;
+    fpt_line<D, N>(f, dim, side, base, stride);
+    const T *Ut = U + tile * (int64_t)S * V * TW;
+    T *out = Ufp + (tile * Fp + f) * (int64_t)V * TW;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      T acc = (side < 0 ? ops.Em[0] : ops.Ep[0]) * Ut[((base)*V + v) * TW + l];
+#pragma unroll
+      for (int m = 1; m < N; m++) acc += (side < 0 ? ops.Em[m] : ops.Ep[m]) * Ut[((base + m * stride) * V + v) * TW + l];
+      out[v * TW + l] = acc;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Common convective flux at one own flux point (Rusanov or Roe) plus ghost
+// states on boundaries; returns the outward, dA-scaled own-side value in Fc
+// (src/faces.cpp:1243-1364, 1616-1640).  For viscous runs the LDG part is
+// added by the caller.
+// ---------------------------------------------------------------------------
+template <typename T, int D>
+__device__ __forceinline__ void conv_common(const Args<T> &a, const T Uo[D + 2], const T Un[D + 2], int code,
+                                            const T n[D], T UL[D + 2], T UR[D + 2], T UB[D + 2], T F[D + 2])
+{
+  if (code >= 0)
+  {
+    const int slot = code & 1;
+#pragma unroll
+    for (int v = 0; v < D + 2; v++)
+    {
+      UL[v] = slot ? Un[v] : Uo[v];
+      UR[v] = slot ? Uo[v] : Un[v];
+      UB[v] = UR[v];
+    }
+  }
+  else
+  {
+#pragma unroll
+    for (int v = 0; v < D + 2; v++) UL[v] = Uo[v];
+    ghost_state<T, D>(-code - 1, UL, n, UR, UB, a.ph);
+  }
+  if (a.ph.fconv == 2)
+    roe<T, D>(UL, UR, n, F, a.ph);
+  else
+    rusanov<T, D>(UL, UR, n, F, a.ph);
+}
+
+// ---------------------------------------------------------------------------
+// Final per-point residual: volume part + surface correction, then optional
+// RK update (src/solver.cpp:2916-2937, 3040-3094).
+// ---------------------------------------------------------------------------
+template <typename T, int D, int N>
+__device__ __forceinline__ void finish_point(const Args<T> &a, int64_t tile, int s, int l, const T vol[D + 2],
+                                             const T *sFc, const SOps<T, N> &o, T *sUnew)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, V = G::V, NM = G::NM;
+  T surf[V];
+#pragma unroll
+  for (int v = 0; v < V; v++) surf[v] = T(0);
+  // surface terms in ascending flux point order = ascending face order
+#pragma unroll
+  for (int face = 0; face < 2 * D; face++)
+  {
+    int dim, side;
+    face_dim_side<D>(face, dim, side);
+    int i, fm, fp;
+    spt_ends<D, N>(s, dim, i, fm, fp);
+    const int f = side < 0 ? fm : fp;
+    const T c = side < 0 ? -o.Dbm[i] : o.Dbp[i];
+#pragma unroll
+    for (int v = 0; v < V; v++) surf[v] += c * sFc[(f * V + v) * TW + l];
+  }
+  const int64_t base = (tile * S + s) * (int64_t)V * TW;
+  T res[V];
+#pragma unroll
+  for (int v = 0; v < V; v++)
+  {
+    res[v] = vol[v] + surf[v];
+    a.divF[base + v * TW + l] = res[v];
+  }
+  if (a.rk_mode == 0) return;
+  const T detJ = a.mets[((tile * S + s) * NM + D * D) * TW + l];
+#pragma unroll
+  for (int v = 0; v < V; v++)
+  {
+    const int64_t idx = base + v * TW + l;
+    T u_ini;
+    if (a.save_ini)
+    {
+      u_ini = a.U[idx];
+      a.U_ini[idx] = u_ini;
+    }
+    else
+      u_ini = a.U_ini[idx];
+    T unew;
+    if (a.rk_mode == 1)
+      unew = u_ini - a.rk_coef[0] * a.dt / detJ * res[v];
+    else
+    {
+      T delta = T(0);
+      // sum of stage increments in stage order
+      for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * a.dt / detJ * a.divF_prev[st][idx];
+      delta -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
+      if (a.Ucomp)
+      {
+        // Kahan-compensated accumulation of the step increment
+        const T c = a.Ucomp[idx];
+        const T y = delta - c;
+        unew = u_ini + y;
+        a.Ucomp[idx] = (unew - u_ini) - y;
+      }
+      else
+      {
+        // reference order: U = U_ini; U -= b_s dt/|J| divF_s for s = 0..
+        unew = u_ini;
+        for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * a.dt / detJ * a.divF_prev[st][idx];
+        unew -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
+      }
+    }
+    a.Uout[idx] = unew;
+    if (sUnew) sUnew[(s * V + v) * TW + l] = unew;
+  }
+}
+
+template <typename T, int D, int N>
+__device__ __forceinline__ void extrap_next_tile(const Args<T> &a, int64_t tile, const T *sUnew, const SOps<T, N> &o)
+{
+  using G = Shape<D, N>;
+  constexpr int Fp = G::Fp, V = G::V;
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    T *out = a.Ufp_next + (tile * Fp + f) * (int64_t)V * TW;
+#pragma unroll
+    for (int v = 0; v < V; v++) out[v * TW + l] = extrap_smem<T, D, N>(sUnew, o, f, v, l, V);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Euler: volume flux, common flux and divergence of one tile in one kernel.
+// ---------------------------------------------------------------------------
+template <typename T, int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(Args<T> a, LineOpsT<T, N> ops)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V, NM = G::NM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sU = reinterpret_cast<T *>(smem_raw);
+  T *sF = sU + S * V * TW;
+  T *sFc = sF + D * S * V * TW;
+  T *sops = sFc + Fp * V * TW;
+  load_ops<T, N>(sops, ops);
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  {
+    const T *src = a.U + tile * (int64_t)S * V * TW;
+    for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
+  }
+  __syncthreads();
+  SOps<T, N> o(sops);
+  // transformed volume flux F~ = adj F (src/elements.cpp:1588-1699)
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    T U[V], F[V][D], P;
+#pragma unroll
+    for (int v = 0; v < V; v++) U[v] = sU[(s * V + v) * TW + l];
+    flux_conv<T, D>(U, F, P, a.ph.gamma);
+    const T *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
+    T adj[D][D];
+#pragma unroll
+    for (int d1 = 0; d1 < D; d1++)
+#pragma unroll
+      for (int d2 = 0; d2 < D; d2++) adj[d1][d2] = m[(d1 * D + d2) * TW];
+#pragma unroll
+    for (int v = 0; v < V; v++)
+#pragma unroll
+      for (int d1 = 0; d1 < D; d1++)
+      {
+        T t = F[v][0] * adj[d1][0];
+#pragma unroll
+        for (int d2 = 1; d2 < D; d2++) t += F[v][d2] * adj[d1][d2];
+        sF[((d1 * S + s) * V + v) * TW + l] = t;
+      }
+  }
+  // common flux at the tile's flux points
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    const int64_t fi = (tile * Fp + f) * (int64_t)TW + l;
+    const int code = a.nbr[fi];
+    T n[D], dA;
+    const T *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+    for (int d = 0; d < D; d++) n[d] = g[d * TW];
+    dA = g[D * TW];
+    T Uo[V], Un[V], UL[V], UR[V], UB[V], Fc[V];
+    const T *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
+    if (code >= 0) gather_fpt<T, V>(a.Ufp, code >> 1, Un);
+    conv_common<T, D>(a, Uo, Un, code, n, UL, UR, UB, Fc);
+    const bool right = (code >= 0) && (code & 1);
+#pragma unroll
+    for (int v = 0; v < V; v++) sFc[(f * V + v) * TW + l] = right ? -Fc[v] * dA : Fc[v] * dA;
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    T vol[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) vol[v] = T(0);
+#pragma unroll
+    for (int d = 0; d < D; d++)
+    {
+      int i, fm, fp;
+      spt_ends<D, N>(s, d, i, fm, fp);
+      const int st = pow_n<N>(d);
+      const int b = s - i * st;
+#pragma unroll
+      for (int m = 0; m < N; m++)
+      {
+        const T c = o.Dm[i * N + m];
+#pragma unroll
+        for (int v = 0; v < V; v++) vol[v] += c * sF[((d * S + b + m * st) * V + v) * TW + l];
+      }
+    }
+    finish_point<T, D, N>(a, tile, s, l, vol, sFc, o, a.extrap_next ? sU : nullptr);
+  }
+  if (a.extrap_next)
+  {
+    __syncthreads();
+    extrap_next_tile<T, D, N>(a, tile, sU, o);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Navier-Stokes kernel 1: common solution, corrected gradient, viscous normal
+// flux at own flux points, volume flux and its divergence
+// (src/solver.cpp:1540-1600; src/elements.cpp:1393-1447, 1588-1699;
+//  src/faces.cpp:1366-1474, 508-710).
+// ---------------------------------------------------------------------------
+template <typename T, int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(Args<T> a, LineOpsT<T, N> ops)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V, NM = G::NM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sU = reinterpret_cast<T *>(smem_raw);
+  T *sUC = sU + S * V * TW;
+  T *sdU = sUC + Fp * V * TW;  // [D][S][V][TW]: physical gradient, then F~
+  T *sops = sdU + D * S * V * TW;
+  load_ops<T, N>(sops, ops);
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  {
+    const T *src = a.U + tile * (int64_t)S * V * TW;
+    for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
+  }
+  __syncthreads();
+  SOps<T, N> o(sops);
+  const T beta = a.ph.ldg_b;
+  // common solution at own flux points (LDG, flip_beta = 1)
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    const int64_t fi = (tile * Fp + f) * (int64_t)TW + l;
+    const int code = a.nbr[fi];
+    T Uo[V], UC[V];
+    const T *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
+    if (code >= 0)
+    {
+      T Un[V];
+      gather_fpt<T, V>(a.Ufp, code >> 1, Un);
+      const int slot = code & 1;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+      {
+        const T ul = slot ? Un[v] : Uo[v];
+        const T ur = slot ? Uo[v] : Un[v];
+        if (beta == T(0.5))
+          UC[v] = ur;
+        else if (beta == T(-0.5))
+          UC[v] = ul;
+        else
+          UC[v] = T(0.5) * (ul + ur) - beta * (ul - ur);
+      }
+    }
+    else
+    {
+      T n[D], UR[V];
+      const T *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+      for (int d = 0; d < D; d++) n[d] = g[d * TW];
+      ghost_state<T, D>(-code - 1, Uo, n, UR, UC, a.ph);
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) sUC[(f * V + v) * TW + l] = UC[v];
+  }
+  __syncthreads();
+  // corrected reference gradient, transformed to physical space
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    T tdU[V][D];
+#pragma unroll
+    for (int d = 0; d < D; d++)
+    {
+      int i, fm, fp;
+      spt_ends<D, N>(s, d, i, fm, fp);
+      const int st = pow_n<N>(d);
+      const int b = s - i * st;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+      {
+        T acc = T(0);
+#pragma unroll
+        for (int m = 0; m < N; m++) acc += o.Dm[i * N + m] * sU[((b + m * st) * V + v) * TW + l];
+        const T cm = o.Dbm[i] * sUC[(fm * V + v) * TW + l];
+        const T cp = o.Dbp[i] * sUC[(fp * V + v) * TW + l];
+        tdU[v][d] = acc + ((fm < fp) ? (cm + cp) : (cp + cm));
+      }
+    }
+    const T *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
+    T adj[D][D];
+#pragma unroll
+    for (int d1 = 0; d1 < D; d1++)
+#pragma unroll
+      for (int d2 = 0; d2 < D; d2++) adj[d1][d2] = m[(d1 * D + d2) * TW];
+    const T inv_det = T(1) / m[D * D * TW];
+#pragma unroll
+    for (int v = 0; v < V; v++)
+#pragma unroll
+      for (int d1 = 0; d1 < D; d1++)
+      {
+        T g = tdU[v][0] * adj[0][d1];
+#pragma unroll
+        for (int d2 = 1; d2 < D; d2++) g += tdU[v][d2] * adj[d2][d1];
+        sdU[((d1 * S + s) * V + v) * TW + l] = g * inv_det;
+      }
+  }
+  __syncthreads();
+  // viscous normal flux at own flux points (own side; boundaries: prescribed side)
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    const int64_t fi = (tile * Fp + f) * (int64_t)TW + l;
+    const int code = a.nbr[fi];
+    if (code >= 0 && ((beta == T(0.5) && (code & 1)) || (beta == T(-0.5) && !(code & 1)))) continue;
+    T n[D];
+    const T *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+    for (int d = 0; d < D; d++) n[d] = g[d * TW];
+    T Uf[V], dUf[V][D], Fn[V];
+    const T *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      Uf[v] = uo[v * TW];
+#pragma unroll
+      for (int d = 0; d < D; d++) dUf[v][d] = extrap_smem<T, D, N>(sdU + d * S * V * TW, o, f, v, l, V);
+    }
+    if (code >= 0)
+      visc_normal<T, D>(Uf, dUf, n, Fn, a.ph);
+    else
+    {
+      T UR[V], UB[V], dUB[V][D];
+      ghost_state<T, D>(-code - 1, Uf, n, UR, UB, a.ph);
+      ghost_grad<T, D>(-code - 1, Uf, dUf, n, dUB);
+      visc_normal<T, D>(UB, dUB, n, Fn, a.ph);
+    }
+    T *out = a.Fvn + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) out[v * TW] = Fn[v];
+  }
+  __syncthreads();
+  // flux at solution points, transformed: F~ = adj (F_conv + F_visc)
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    T U[V], dU[V][D], F[V][D], P;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      U[v] = sU[(s * V + v) * TW + l];
+#pragma unroll
+      for (int d = 0; d < D; d++) dU[v][d] = sdU[((d * S + s) * V + v) * TW + l];
+    }
+    flux_conv<T, D>(U, F, P, a.ph.gamma);
+    flux_visc_add<T, D>(U, dU, F, a.ph);
+    const T *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
+    T adj[D][D];
+#pragma unroll
+    for (int d1 = 0; d1 < D; d1++)
+#pragma unroll
+      for (int d2 = 0; d2 < D; d2++) adj[d1][d2] = m[(d1 * D + d2) * TW];
+#pragma unroll
+    for (int v = 0; v < V; v++)
+#pragma unroll
+      for (int d1 = 0; d1 < D; d1++)
+      {
+        T t = F[v][0] * adj[d1][0];
+#pragma unroll
+        for (int d2 = 1; d2 < D; d2++) t += F[v][d2] * adj[d1][d2];
+        sdU[((d1 * S + s) * V + v) * TW + l] = t;
+      }
+  }
+  __syncthreads();
+  // volume divergence
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    T vol[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) vol[v] = T(0);
+#pragma unroll
+    for (int d = 0; d < D; d++)
+    {
+      int i, fm, fp;
+      spt_ends<D, N>(s, d, i, fm, fp);
+      const int st = pow_n<N>(d);
+      const int b = s - i * st;
+#pragma unroll
+      for (int m = 0; m < N; m++)
+      {
+        const T c = o.Dm[i * N + m];
+#pragma unroll
+        for (int v = 0; v < V; v++) vol[v] += c * sdU[((d * S + b + m * st) * V + v) * TW + l];
+      }
+    }
+    T *out = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) out[v * TW] = vol[v];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Navier-Stokes kernel 2: convective + LDG common flux, surface correction,
+// optional RK update (src/faces.cpp:1476-1614; src/elements.cpp:1476-1501).
+// ---------------------------------------------------------------------------
+template <typename T, int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT) k_ns_face(Args<T> a, LineOpsT<T, N> ops)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sFc = reinterpret_cast<T *>(smem_raw);
+  T *sUnew = sFc + Fp * V * TW;
+  T *sops = sUnew + S * V * TW;
+  load_ops<T, N>(sops, ops);
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  __syncthreads();
+  SOps<T, N> o(sops);
+  const T beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    const int64_t fi = (tile * Fp + f) * (int64_t)TW + l;
+    const int code = a.nbr[fi];
+    T n[D], dA;
+    const T *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+    for (int d = 0; d < D; d++) n[d] = g[d * TW];
+    dA = g[D * TW];
+    T Uo[V], Un[V], UL[V], UR[V], UB[V], Fc[V], Fv[V];
+    const T *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
+    if (code >= 0) gather_fpt<T, V>(a.Ufp, code >> 1, Un);
+    conv_common<T, D>(a, Uo, Un, code, n, UL, UR, UB, Fc);
+    const T *fvo = a.Fvn + (tile * Fp + f) * (int64_t)V * TW + l;
+    if (code >= 0)
+    {
+      const int slot = code & 1;
+      T FnL[V], FnR[V];
+      // own side is left when slot == 0
+      if (beta == T(0.5))
+      {
+        if (slot == 0)
+        {
+#pragma unroll
+          for (int v = 0; v < V; v++) FnL[v] = fvo[v * TW];
+        }
+        else
+          gather_fpt<T, V>(a.Fvn, code >> 1, FnL);
+#pragma unroll
+        for (int v = 0; v < V; v++) FnR[v] = T(0);
+      }
+      else if (beta == T(-0.5))
+      {
+        if (slot == 1)
+        {
+#pragma unroll
+          for (int v = 0; v < V; v++) FnR[v] = fvo[v * TW];
+        }
+        else
+          gather_fpt<T, V>(a.Fvn, code >> 1, FnR);
+#pragma unroll
+        for (int v = 0; v < V; v++) FnL[v] = T(0);
+      }
+      else
+      {
+        T Fo[V], Fx[V];
+#pragma unroll
+        for (int v = 0; v < V; v++) Fo[v] = fvo[v * TW];
+        gather_fpt<T, V>(a.Fvn, code >> 1, Fx);
+#pragma unroll
+        for (int v = 0; v < V; v++)
+        {
+          FnL[v] = slot ? Fx[v] : Fo[v];
+          FnR[v] = slot ? Fo[v] : Fx[v];
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < V; v++)
+        Fv[v] = T(0.5) * (FnL[v] + FnR[v]) + tau * (UL[v] - UR[v]) + beta * (FnL[v] - FnR[v]);
+    }
+    else
+    {
+#pragma unroll
+      for (int v = 0; v < V; v++) Fv[v] = fvo[v * TW] + tau * (UL[v] - UB[v]);
+    }
+    const bool right = (code >= 0) && (code & 1);
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      T acc = right ? -Fc[v] * dA : Fc[v] * dA;
+      if (right)
+        acc -= Fv[v] * dA;
+      else
+        acc += Fv[v] * dA;
+      sFc[(f * V + v) * TW + l] = acc;
+    }
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    T vol[V];
+    const T *dv = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) vol[v] = dv[v * TW];
+    finish_point<T, D, N>(a, tile, s, l, vol, sFc, o, a.extrap_next ? sUnew : nullptr);
+  }
+  if (a.extrap_next)
+  {
+    __syncthreads();
+    extrap_next_tile<T, D, N>(a, tile, sUnew, o);
+  }
+}
+
+}  // namespace dev
+}  // namespace zb

@@ -1,0 +1,245 @@
+"""Host-side mirror of ZEFR's FRSolver for the DFR residual path.
+
+Method names follow the reference ``FRSolver`` (include/solver.hpp:140-190):
+``compute_residual(stage)`` fills the stage's ``divF_spts`` register,
+``update()`` advances one explicit RK44 step, ``step_RK_stage(stage)`` does one
+stage, and the state is read and written in the reference layout
+``U_spts[spt][var][ele]`` (``get_q_spts`` strides, src/zefr.cpp:607-645).
+Everything runs in ``libzefr_b200.so`` on the GPU through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, Optional, Union
+
+import numpy as np
+
+from . import _lib
+from ._lib import ZbInfo, ZbMesh, ZbParams, check, lib
+from .meshgen import Mesh, read_gmsh
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+def make_params(order: int, viscous: bool = False, *, gamma: float = 1.4, prandtl: float = 0.72, mu: float = 0.0,
+                rt: float = 0.0, c_sth: float = 0.0, fix_vis: bool = True, rus_k: float = 0.0,
+                ldg_b: float = 0.5, ldg_tau: float = 1.0, rho_fs: float = 1.0, V_fs=(0.0, 0.0, 0.0),
+                P_fs: float = 1.0, T_wall: float = 0.0, R_ref: float = 0.0, V_wall=(0.0, 0.0, 0.0),
+                dt: float = 1e-3, fconv: str = "rusanov", precision: str = "fp64") -> ZbParams:
+    """Solver parameters with the meaning of the reference InputStruct fields."""
+    p = ZbParams()
+    p.order = order
+    p.viscous = int(bool(viscous))
+    p.fconv = {"rusanov": _lib.ZB_FLUX_RUSANOV, "roe": _lib.ZB_FLUX_ROE}[fconv.lower()]
+    p.precision = {"fp64": _lib.ZB_FP64, "mixed": _lib.ZB_MIXED}[precision.lower()]
+    p.gamma, p.prandtl, p.mu, p.rt, p.c_sth = gamma, prandtl, mu, rt, c_sth
+    p.fix_vis = int(bool(fix_vis))
+    p.rus_k, p.ldg_b, p.ldg_tau = rus_k, ldg_b, ldg_tau
+    p.rho_fs, p.P_fs, p.T_wall, p.R_ref, p.dt = rho_fs, P_fs, T_wall, R_ref, dt
+    for d in range(3):
+        p.V_fs[d] = float(V_fs[d]) if d < len(V_fs) else 0.0
+        p.V_wall[d] = float(V_wall[d]) if d < len(V_wall) else 0.0
+    return p
+
+
+def params_from_reference(ref_params: Dict[str, float], order: int, **overrides) -> ZbParams:
+    """Build parameters from the reference's InputStruct values (as the oracle reports them)."""
+    rp = ref_params
+    kw = dict(gamma=rp["gamma"], prandtl=rp["prandtl"], mu=rp["mu"], rt=rp["rt"], c_sth=rp["c_sth"],
+              fix_vis=bool(rp["fix_vis"]), rus_k=rp["rus_k"], ldg_b=rp["ldg_b"], ldg_tau=rp["ldg_tau"],
+              rho_fs=rp["rho_fs"], V_fs=(rp["V_fs0"], rp["V_fs1"], rp["V_fs2"]), P_fs=rp["P_fs"],
+              T_wall=rp["T_wall"], R_ref=rp["R_ref"], V_wall=(rp["V_wall0"], rp["V_wall1"], rp["V_wall2"]),
+              dt=rp["dt"])
+    kw.update(overrides)
+    return make_params(order, bool(rp["viscous"]), **kw)
+
+
+def params_from_deck(**deck) -> ZbParams:
+    """Reference deck keys -> parameters (non-dimensionalisation of src/input.cpp:463-539)."""
+    d = _lib.ZbDeck()
+    defaults = dict(ndims=2, order=3, viscous=0, fconv=0, precision=0, disable_nondim=0, fix_vis=0, gamma=1.4,
+                    prandtl=0.72, R=286.9, S=120.0, T_gas=291.15, rho_fs=1.4, P_fs=1.0, mach_fs=0.2, Re_fs=200.0,
+                    L_fs=1.0, T_fs=300.0, nx_fs=1.0, ny_fs=0.0, nz_fs=0.0, mach_wall=0.0, T_wall=300.0,
+                    nx_wall=1.0, ny_wall=0.0, nz_wall=0.0, rus_k=0.0, ldg_b=0.5, ldg_tau=1.0, dt=1e-3)
+    defaults.update(deck)
+    for k, v in defaults.items():
+        setattr(d, k, v)
+    p = ZbParams()
+    check(lib().zb_params_from_deck(ctypes.byref(d), ctypes.byref(p)))
+    return p
+
+
+class _MeshArrays:
+    """Keeps numpy buffers alive behind a ZbMesh view."""
+
+    def __init__(self, mesh: Mesh, bounds: Dict[str, str]):
+        self.coords = np.ascontiguousarray(mesh.nodes, dtype=np.float64)
+        self.ele2nodes = np.ascontiguousarray(mesh.elements, dtype=np.int64)
+        npf = max((len(f[1]) for f in mesh.bnd_faces), default=1)
+        fn = np.full((max(len(mesh.bnd_faces), 1), npf), -1, dtype=np.int64)
+        bc = np.zeros(max(len(mesh.bnd_faces), 1), dtype=np.int32)
+        lower = {k.lower(): v.lower() for k, v in bounds.items()}
+        for i, (_, nodes, name) in enumerate(mesh.bnd_faces):
+            fn[i, :len(nodes)] = nodes
+            key = name.lower()
+            if key not in lower:
+                raise ValueError(f'Unrecognized mesh boundary: "{key}"')
+            bc[i] = _lib.BC_CODES[lower[key]]
+        self.face_nodes, self.face_bc = fn, bc
+        m = ZbMesh()
+        m.ndims = mesh.ndims
+        m.gmsh_type = mesh.gmsh_type
+        m.n_nodes = self.coords.shape[0]
+        m.coords = self.coords.ctypes.data_as(_DP)
+        m.n_eles = self.ele2nodes.shape[0]
+        m.nodes_per_ele = self.ele2nodes.shape[1]
+        m.ele2nodes = self.ele2nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        m.n_bnd_faces = len(mesh.bnd_faces)
+        m.nodes_per_face = npf
+        m.face_nodes = self.face_nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        m.face_bc = self.face_bc.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        self.view = m
+
+
+def _as_mesh(mesh: Union[Mesh, str]) -> Mesh:
+    return read_gmsh(mesh) if isinstance(mesh, str) else mesh
+
+
+class Plan:
+    """Host-only set-up (connectivity, operators, metrics); needs no GPU."""
+
+    def __init__(self, mesh: Union[Mesh, str], params: ZbParams, bounds: Dict[str, str]):
+        mesh = _as_mesh(mesh)
+        self._arrays = _MeshArrays(mesh, bounds)
+        self._params = params
+        h = ctypes.c_void_p()
+        check(lib().zb_plan_create(ctypes.byref(self._arrays.view), ctypes.byref(params), ctypes.byref(h)))
+        self.h = h
+        self.info = ZbInfo()
+        check(lib().zb_plan_info(self.h, ctypes.byref(self.info)))
+
+    def get(self, name: str) -> np.ndarray:
+        n = ctypes.c_int64(0)
+        check(lib().zb_plan_get(self.h, name.encode(), None, ctypes.byref(n)))
+        out = np.empty(n.value)
+        check(lib().zb_plan_get(self.h, name.encode(), out.ctypes.data_as(_DP), ctypes.byref(n)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().zb_plan_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FRSolver:
+    """DFR residual and RK44 stepping on the GPU, FRSolver-style.
+
+    ``mesh`` is a :class:`zefr_b200.meshgen.Mesh` or a gmsh 2.2 file path;
+    ``bounds`` maps the mesh's boundary names to deck condition names
+    (the deck's ``mesh_bound`` lines, e.g. ``{"PERIODIC": "periodic"}``).
+    """
+
+    def __init__(self, mesh: Union[Mesh, str], params: ZbParams, bounds: Dict[str, str]):
+        self.plan = Plan(mesh, params, bounds)
+        h = ctypes.c_void_p()
+        check(lib().zb_create(self.plan.h, ctypes.byref(h)))
+        self.h = h
+        self.info = ZbInfo()
+        check(lib().zb_info_get(self.h, ctypes.byref(self.info)))
+        self.nspts, self.nvars, self.neles = self.info.nspts, self.info.nvars, int(self.info.n_eles)
+        self.ndims, self.nstages = self.info.ndims, self.info.nstages
+
+    # -- lifetime --
+    def close(self):
+        if getattr(self, "h", None):
+            lib().zb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def state_shape(self):
+        return (self.nspts, self.nvars, self.neles)
+
+    def _strides(self):
+        E = self.neles
+        return (self.nvars * E, E, 1)
+
+    # -- state --
+    def set_state(self, U) -> None:
+        if hasattr(U, "is_cuda") and U.is_cuda:
+            import torch
+            U = U.to(torch.float64).contiguous()
+            assert tuple(U.shape) == self.state_shape
+            check(lib().zb_set_state(self.h, ctypes.cast(U.data_ptr(), _DP), *self._strides(), _lib.ZB_DEVICE))
+            self._keep = U
+            return
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.shape != self.state_shape:
+            raise ValueError(f"state shape {U.shape} != {self.state_shape}")
+        check(lib().zb_set_state(self.h, U.ctypes.data_as(_DP), *self._strides(), _lib.ZB_HOST))
+
+    def get_state(self) -> np.ndarray:
+        out = np.zeros(self.state_shape)
+        check(lib().zb_get_state(self.h, out.ctypes.data_as(_DP), *self._strides(), _lib.ZB_HOST))
+        return out
+
+    def get_state_device(self, out) -> None:
+        """Copy the state into a contiguous float64 CUDA tensor of state_shape."""
+        check(lib().zb_get_state(self.h, ctypes.cast(out.data_ptr(), _DP), *self._strides(), _lib.ZB_DEVICE))
+
+    # -- residual --
+    def compute_residual(self, stage: int = 0) -> None:
+        check(lib().zb_compute_residual(self.h, stage))
+
+    def get_residual(self, stage: int = 0) -> np.ndarray:
+        out = np.zeros(self.state_shape)
+        check(lib().zb_get_residual(self.h, stage, out.ctypes.data_as(_DP), *self._strides(), _lib.ZB_HOST))
+        return out
+
+    def get_residual_device(self, out, stage: int = 0) -> None:
+        check(lib().zb_get_residual(self.h, stage, ctypes.cast(out.data_ptr(), _DP), *self._strides(),
+                                    _lib.ZB_DEVICE))
+
+    def residual(self, U, stage: int = 0) -> np.ndarray:
+        self.set_state(U)
+        self.compute_residual(stage)
+        return self.get_residual(stage)
+
+    # -- time stepping --
+    def step_RK_stage(self, stage: int) -> None:
+        check(lib().zb_rk_stage(self.h, stage))
+
+    def update(self) -> None:
+        check(lib().zb_step(self.h, 1))
+
+    def step(self, n: int) -> None:
+        check(lib().zb_step(self.h, n))
+
+    def set_dt(self, dt: float) -> None:
+        check(lib().zb_set_dt(self.h, dt))
+
+    def residual_norms(self) -> Dict[str, np.ndarray]:
+        out = np.zeros(3 * self.nvars)
+        check(lib().zb_residual_norms(self.h, out.ctypes.data_as(_DP)))
+        V = self.nvars
+        return {"linf": out[:V], "l1": out[V:2 * V], "l2": out[2 * V:]}
+
+    def set_stream(self, stream_ptr: int) -> None:
+        check(lib().zb_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+
+    def synchronize(self) -> None:
+        check(lib().zb_synchronize(self.h))
+
+    def launch_count(self) -> int:
+        return int(lib().zb_launch_count(self.h))
