@@ -1,0 +1,380 @@
+"""CPU restatement of the reference DFR residual in numpy (test infrastructure).
+
+This is the oracle the CUDA path is checked against.  It restates
+``FRSolver::compute_residual`` (reference src/solver.cpp:1494-1645) step by
+step on reference-layout arrays (row-major, last index fastest,
+include/mdvector.hpp:189-260):
+
+  1. U_fpts = oppE U_spts                        src/elements.cpp:1337-1360
+  2. boundary ghost states                       src/faces.cpp:123-506
+  3. dU_spts = oppD U_spts                       src/elements.cpp:1393-1419
+     common solution (LDG)                       src/faces.cpp:1366-1474
+     dU_spts += oppD_fpts Ucomm                  src/elements.cpp:1421-1447
+  4. physical gradient, flux, transformed flux   src/elements.cpp:1588-1699, include/flux.hpp:1-202
+  5. dU_fpts = oppE dU_spts, boundary gradient   src/elements.cpp:1362-1391, src/faces.cpp:508-710
+  6. divF = oppDiv F                             src/elements.cpp:1449-1474
+  7. Rusanov + LDG common flux, +-F dA           src/faces.cpp:1243-1364, 1476-1614
+  8. divF += oppDiv_fpts Fcomm                   src/elements.cpp:1476-1501
+
+The face data are organised per element flux point with the reference's
+left/right roles (slot), so each face flux is evaluated identically from both
+sides.  Set-up arrays come from the reference itself (golden fixtures) or from
+any set-up shown equal to it.  Only tests, fixture scripts, smoke() and the
+benchmark's CPU leg import this module.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Dict, Optional
+
+import numpy as np
+
+# reference BC_TYPE codes (include/input.hpp:54-70)
+BC_CHAR, BC_SUP_IN, BC_SUP_OUT, BC_SLIP, BC_ISO, BC_ADI, BC_ISO_MOVE, BC_ADI_MOVE, BC_SYM = 2, 3, 4, 5, 6, 7, 8, 9, 11
+
+
+@dataclass
+class Setup:
+    """Reference-layout set-up arrays of one element type."""
+
+    ndims: int
+    oppE: np.ndarray         # [Fp, S]
+    oppD: np.ndarray         # [D, S, S]
+    oppD_fpts: np.ndarray    # [D, S, Fp]
+    oppDiv: np.ndarray       # [S, D, S]
+    oppDiv_fpts: np.ndarray  # [S, Fp]
+    inv_jaco: np.ndarray     # [D, S, D, E]
+    jaco_det: np.ndarray     # [S, E]
+    partner: np.ndarray      # [Fp, E] int: e'*Fp + f' or -1-bc
+    slot: np.ndarray         # [Fp, E] 0 left / 1 right
+    norm: np.ndarray         # [Fp, D, E] left unit normal
+    dA: np.ndarray           # [Fp, E] own dA
+
+    @staticmethod
+    def from_arrays(ndims: int, nspts: int, nfpts: int, neles: int, get) -> "Setup":
+        D, S, Fp, E = ndims, nspts, nfpts, neles
+        return Setup(
+            ndims=D,
+            oppE=get("oppE").reshape(Fp, S), oppD=get("oppD").reshape(D, S, S),
+            oppD_fpts=get("oppD_fpts").reshape(D, S, Fp), oppDiv=get("oppDiv").reshape(S, D, S),
+            oppDiv_fpts=get("oppDiv_fpts").reshape(S, Fp),
+            inv_jaco=get("inv_jaco_spts").reshape(D, S, D, E), jaco_det=get("jaco_det_spts").reshape(S, E),
+            partner=get("fpt_partner").astype(np.int64).reshape(Fp, E), slot=get("fpt_slot").astype(np.int64).reshape(Fp, E),
+            norm=get("fpt_norm").reshape(Fp, D, E), dA=get("fpt_dA").reshape(Fp, E))
+
+
+def _flux_conv(U: np.ndarray, gamma: float):
+    """U [V, ...] -> F [V, D, ...], P (include/flux.hpp:11-63, zero grid velocity)."""
+    V = U.shape[0]
+    D = V - 2
+    invrho = 1.0 / U[0]
+    momF = U[1] * U[1]
+    for d in range(1, D):
+        momF = momF + U[d + 1] * U[d + 1]
+    momF = momF * invrho
+    P = (gamma - 1.0) * (U[D + 1] - 0.5 * momF)
+    H = (U[D + 1] + P) * invrho
+    F = np.zeros((V, D) + U.shape[1:])
+    for d in range(D):
+        F[0, d] = U[d + 1]
+        for k in range(D):
+            F[k + 1, d] = U[d + 1] * U[k + 1] * invrho + (P if k == d else 0.0)
+        F[D + 1, d] = U[d + 1] * H
+    return F, P
+
+
+def _flux_visc_add(U: np.ndarray, dU: np.ndarray, F: np.ndarray, p: Dict[str, float]) -> None:
+    """F[V, D, ...] -= viscous flux (include/flux.hpp:71-202); dU [V, D, ...]."""
+    V = U.shape[0]
+    D = V - 2
+    gamma = p["gamma"]
+    invrho = 1.0 / U[0]
+    vel = [U[d + 1] * invrho for d in range(D)]
+    vsq = vel[0] * vel[0]
+    for d in range(1, D):
+        vsq = vsq + vel[d] * vel[d]
+    e_int = U[D + 1] * invrho - 0.5 * vsq
+    if p["fix_vis"]:
+        mu = p["mu"] + 0.0 * e_int
+    else:
+        rt_ratio = (gamma - 1.0) * e_int / p["rt"]
+        mu = p["mu"] * np.power(rt_ratio, 1.5) * (1.0 + p["c_sth"]) / (rt_ratio + p["c_sth"])
+    dvel = [[(dU[i + 1, j] - dU[0, j] * vel[i]) * invrho for j in range(D)] for i in range(D)]
+    de = []
+    for j in range(D):
+        s = vel[0] * dvel[0][j]
+        for i in range(1, D):
+            s = s + vel[i] * dvel[i][j]
+        dke = 0.5 * vsq * dU[0, j] + U[0] * s
+        de.append((dU[D + 1, j] - dke - dU[0, j] * e_int) * invrho)
+    div = dvel[0][0]
+    for d in range(1, D):
+        div = div + dvel[d][d]
+    diag = div / 3.0
+    kappa = (mu / p["prandtl"]) * gamma
+    for j in range(D):
+        w = 0.0
+        for i in range(D):
+            tau = 2.0 * mu * (dvel[i][i] - diag) if i == j else mu * (dvel[i][j] + dvel[j][i])
+            F[i + 1, j] -= tau
+            w = w + vel[i] * tau
+        F[D + 1, j] -= (w + kappa * de[j])
+
+
+def _ghost(bc: np.ndarray, UL: np.ndarray, n: np.ndarray, p: Dict[str, float]):
+    """Ghost (Rusanov) and prescribed (LDG) right states (src/faces.cpp:123-506).
+
+    UL [V, M], n [D, M], bc [M] -> UR, UB [V, M]."""
+    V, M = UL.shape
+    D = V - 2
+    g = p["gamma"]
+    UR = UL.copy()
+    UB = UL.copy()
+    V_fs = np.array([p["V_fs0"], p["V_fs1"], p["V_fs2"]])[:D]
+    V_wall = np.array([p["V_wall0"], p["V_wall1"], p["V_wall2"]])[:D]
+    m = bc == BC_SUP_IN
+    if m.any():
+        UR[0, m] = p["rho_fs"]
+        vsq = 0.0
+        for d in range(D):
+            UR[d + 1, m] = p["rho_fs"] * V_fs[d]
+            vsq += V_fs[d] * V_fs[d]
+        UR[D + 1, m] = p["P_fs"] / (g - 1.0) + 0.5 * p["rho_fs"] * vsq
+        UB[:, m] = UR[:, m]
+    m = bc == BC_CHAR
+    if m.any():
+        u = UL[:, m]
+        nn = n[:, m]
+        VnL = sum(u[d + 1] / u[0] * nn[d] for d in range(D))
+        VnR = sum(V_fs[d] * nn[d] for d in range(D))
+        momF = sum(u[d + 1] * u[d + 1] for d in range(D)) / u[0]
+        PL = (g - 1.0) * (u[D + 1] - 0.5 * momF)
+        PR = p["P_fs"]
+        cL = np.sqrt(g * PL / u[0])
+        cR = np.sqrt(g * PR / p["rho_fs"])
+        sup = np.abs(VnR) >= cR
+        RL = np.where(sup & (VnL >= 0), VnR + 2.0 / (g - 1) * cR, VnL + 2.0 / (g - 1) * cL)
+        RB = np.where(sup & (VnL < 0), VnL - 2.0 / (g - 1) * cL, VnR - 2.0 / (g - 1) * cR)
+        cstar = 0.25 * (g - 1) * (RL - RB)
+        ustarn = 0.5 * (RL + RB)
+        rhoR = cstar * cstar / g
+        inflow = VnL < 0.0
+        rhoR = rhoR * np.where(inflow, p["rho_fs"] ** g / PR, np.power(u[0], g) / PL)
+        VR = [np.where(inflow, V_fs[d] + (ustarn - VnR) * nn[d], u[d + 1] / u[0] + (ustarn - VnL) * nn[d])
+              for d in range(D)]
+        rhoR = np.power(rhoR, 1.0 / (g - 1))
+        out = np.empty_like(u)
+        out[0] = rhoR
+        for d in range(D):
+            out[d + 1] = rhoR * VR[d]
+        PRs = rhoR / g * cstar * cstar
+        E = PRs / (g - 1)
+        for d in range(D):
+            E = E + 0.5 * rhoR * VR[d] * VR[d]
+        out[D + 1] = E
+        UR[:, m] = out
+        UB[:, m] = out
+    m = (bc == BC_SLIP) | (bc == BC_SYM)
+    if m.any():
+        u = UL[:, m]
+        nn = n[:, m]
+        momN = sum(u[d + 1] * nn[d] for d in range(D))
+        for d in range(D):
+            UR[d + 1, m] = u[d + 1] - 2.0 * momN * nn[d]
+        UB[:, m] = UR[:, m]
+    for code in (BC_ISO, BC_ISO_MOVE):
+        m = bc == code
+        if not m.any():
+            continue
+        moving = code == BC_ISO_MOVE
+        u = UL[:, m]
+        rhoL = u[0]
+        vsq = 0.0
+        vwsq = 0.0
+        for d in range(D):
+            vw = V_wall[d] if moving else 0.0
+            V = -(u[d + 1] / rhoL) + 2 * vw
+            UR[d + 1, m] = rhoL * V
+            vsq = vsq + V * V
+            UB[d + 1, m] = rhoL * vw if moving else vw
+            vwsq += vw * vw
+        cpg = p["R_ref"] / (g - 1)
+        UR[D + 1, m] = rhoL * (cpg * p["T_wall"] + 0.5 * vsq)
+        UB[D + 1, m] = rhoL * (cpg * p["T_wall"] + 0.5 * vwsq) if moving else rhoL * cpg * p["T_wall"]
+    for code in (BC_ADI, BC_ADI_MOVE):
+        m = bc == code
+        if not m.any():
+            continue
+        moving = code == BC_ADI_MOVE
+        u = UL[:, m]
+        rhoL = u[0]
+        vsq = 0.0
+        vlsq = 0.0
+        vwsq = 0.0
+        for d in range(D):
+            vw = V_wall[d] if moving else 0.0
+            VL = u[d + 1] / rhoL
+            V = -VL + 2 * vw
+            UR[d + 1, m] = rhoL * V
+            UB[d + 1, m] = rhoL * vw
+            vsq = vsq + V * V
+            vlsq = vlsq + VL * VL
+            vwsq += vw * vw
+        EL = u[D + 1]
+        UR[D + 1, m] = EL + 0.5 * rhoL * (vsq - vlsq)
+        UB[D + 1, m] = EL - 0.5 * rhoL * (vlsq + vwsq) if moving else EL + 0.5 * rhoL * (vwsq - vlsq)
+    return UR, UB
+
+
+def _ghost_grad(bc: np.ndarray, UL: np.ndarray, dUL: np.ndarray, n: np.ndarray) -> np.ndarray:
+    """Right-state gradient on boundaries (src/faces.cpp:508-710). dUL [V, D, M]."""
+    dUR = dUL.copy()
+    V = UL.shape[0]
+    D = V - 2
+    m = (bc == BC_ADI) | (bc == BC_ADI_MOVE)
+    if m.any():
+        u = UL[:, m]
+        du = dUL[:, :, m]
+        nn = n[:, m]
+        rho, E = u[0], u[D + 1]
+        vel = [u[d + 1] / rho for d in range(D)]
+        dTn = 0.0
+        for j in range(D):
+            s = 0.0
+            for i in range(D):
+                s = s + vel[i] * ((du[i + 1, j] - du[0, j] * vel[i]) / rho)
+            dT = du[D + 1, j] - du[0, j] * E / rho - rho * s
+            dTn = dTn + dT * nn[j]
+        for j in range(D):
+            dUR[D + 1, j, m] = du[D + 1, j] - dTn * nn[j]
+    return dUR
+
+
+def _normal(F: np.ndarray, n: np.ndarray) -> np.ndarray:
+    """F [V, D, M], n [D, M] -> F.n [V, M] (sum in dimension order)."""
+    out = F[:, 0] * n[0]
+    for d in range(1, n.shape[0]):
+        out = out + F[:, d] * n[d]
+    return out
+
+
+def residual(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, fconv: str = "rusanov") -> np.ndarray:
+    """divF_spts(stage) for state U [S, V, E] (reference form, |J| div F)."""
+    if fconv != "rusanov":
+        raise ValueError("the reference has only the Rusanov convective flux")
+    S, V, E = U.shape
+    D = st.ndims
+    Fp = st.oppE.shape[0]
+    gamma = p["gamma"]
+    # 1. extrapolate
+    Ufp = np.einsum("fs,sve->fve", st.oppE, U)
+    # per element fpt: own and partner states, flattened over (f, e)
+    own = Ufp.transpose(1, 0, 2).reshape(V, Fp * E)                    # [V, Fp*E] index f*E+e
+    part = st.partner.reshape(-1)
+    interior = part >= 0
+    pe = np.where(interior, part // Fp, 0)
+    pf = np.where(interior, part % Fp, 0)
+    other = Ufp[pf, :, pe].T                                            # [V, M]
+    slot = st.slot.reshape(-1)
+    n = st.norm.transpose(1, 0, 2).reshape(D, Fp * E)
+    dA = st.dA.reshape(-1)
+    bc = np.where(interior, 0, -1 - part)
+    UL = np.where(slot == 0, own, other)
+    URi = np.where(slot == 0, other, own)
+    URg, UBg = _ghost(bc, own, n, p)
+    UR = np.where(interior, URi, URg)   # Rusanov right state
+    UB = np.where(interior, URi, UBg)   # LDG right state
+    inv = st.inv_jaco  # [D1, S, D2, E]
+    det = st.jaco_det
+    dU_phys = None
+    beta = p["ldg_b"]
+    if viscous:
+        # 3. corrected gradient
+        dU = np.einsum("dst,tve->dsve", st.oppD, U)
+        if beta == 0.5:
+            UC = UB.copy()
+        elif beta == -0.5:
+            UC = UL.copy()
+        else:
+            UC = 0.5 * (UL + UB) - beta * (UL - UB)
+        UC = np.where(interior, UC, UBg)
+        Ucomm = UC.reshape(V, Fp, E).transpose(1, 0, 2)
+        dU = dU + np.einsum("dsf,fve->dsve", st.oppD_fpts, Ucomm)
+        # physical gradient dU[d1] = sum_d2 tdU[d2] inv[d2][d1] / |J|
+        dU_phys = np.zeros_like(dU)
+        for d1 in range(D):
+            acc = 0.0
+            for d2 in range(D):
+                acc = acc + dU[d2] * inv[d2, :, d1][:, None, :]
+            dU_phys[d1] = acc * (1.0 / det)[:, None, :]
+    # 4. flux at solution points
+    Uv = U.transpose(1, 0, 2)                                           # [V, S, E]
+    F, _ = _flux_conv(Uv, gamma)                                        # [V, D, S, E]
+    if viscous:
+        _flux_visc_add(Uv, dU_phys.transpose(2, 0, 1, 3), F, p)        # dU as [V, D, S, E]
+    Ft = np.zeros((D, S, V, E))
+    for d1 in range(D):
+        acc = 0.0
+        for d2 in range(D):
+            acc = acc + F[:, d2] * inv[d1, :, d2][None, :, :]
+        Ft[d1] = acc.transpose(1, 0, 2)
+    # 6. volume divergence
+    divF = np.einsum("sdt,dtve->sve", st.oppDiv, Ft)
+    # 7. common flux
+    FL, PL = _flux_conv(UL, gamma)
+    FR, PR = _flux_conv(UR, gamma)
+    aL = np.sqrt(gamma * PL / UL[0])
+    aR = np.sqrt(gamma * PR / UR[0])
+    VnL = sum(UL[d + 1] / UL[0] * n[d] for d in range(D))
+    VnR = sum(UR[d + 1] / UR[0] * n[d] for d in range(D))
+    eig = np.maximum(np.abs(VnL) + aL, np.abs(VnR) + aR)
+    Fc = 0.5 * (_normal(FR, n) + _normal(FL, n)) - 0.5 * eig * (1.0 - p["rus_k"]) * (UR - UL)
+    sign = np.where(slot == 0, 1.0, -1.0)
+    Fcomm = sign * Fc * dA
+    if viscous:
+        dUf = np.einsum("fs,dsve->vdfe", st.oppE, dU_phys).reshape(V, D, Fp * E)
+        dUo = dUf
+        dUp = dUf.reshape(V, D, Fp, E)[:, :, pf, pe]
+        dUL = np.where(slot == 0, dUo, dUp)
+        dUR = np.where(slot == 0, dUp, dUo)
+        dURg = _ghost_grad(bc, own, dUo, n)
+        dUR = np.where(interior, dUR, dURg)
+        ULv = UL
+        URv = UB
+        tau = p["ldg_tau"]
+        if beta == 0.5:
+            dUR = np.where(interior, 0.0, dUR)
+        elif beta == -0.5:
+            dUL = np.where(interior, 0.0, dUL)
+        FvL = np.zeros((V, D, Fp * E))
+        FvR = np.zeros((V, D, Fp * E))
+        _flux_visc_add(ULv, dUL, FvL, p)
+        _flux_visc_add(URv, dUR, FvR, p)
+        FnL = _normal(FvL, n)
+        FnR = _normal(FvR, n)
+        Fv_int = 0.5 * (FnL + FnR) + tau * (ULv - URv) + beta * (FnL - FnR)
+        Fv_bnd = FnR + tau * (ULv - URv)
+        Fv = np.where(interior, Fv_int, Fv_bnd)
+        Fcomm = Fcomm + sign * Fv * dA
+    Fcomm = Fcomm.reshape(V, Fp, E).transpose(1, 0, 2)
+    # 8. surface correction
+    return divF + np.einsum("sf,fve->sve", st.oppDiv_fpts, Fcomm)
+
+
+def rk44_step(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, dt: float) -> np.ndarray:
+    """One explicit RK44 step (FRSolver::step_RK, src/solver.cpp:2864-3097)."""
+    alpha = [0.5, 0.5, 1.0]
+    beta = [1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0]
+    U_ini = U.copy()
+    det = st.jaco_det[:, None, :]
+    regs = []
+    Us = U
+    for s in range(3):
+        r = residual(st, Us, p, viscous)
+        regs.append(r)
+        Us = U_ini - alpha[s] * dt / det * r
+    regs.append(residual(st, Us, p, viscous))
+    Un = U_ini.copy()
+    for s in range(4):
+        Un = Un - beta[s] * dt / det * regs[s]
+    return Un

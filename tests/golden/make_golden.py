@@ -1,0 +1,165 @@
+"""Generate the golden fixtures in tests/golden/*.npz from the reference solver.
+
+Runs the reference's own CPU FRSolver (built by ``make -C oracle``) on small
+synthetic meshes of every workload shape, with seeded states, and stores:
+
+  mesh          nodes, elements, boundary faces, boundary-condition map
+  params        the reference InputStruct values after its non-dimensionalisation
+  setup arrays  the reference's operators, metrics and per-flux-point face data
+  U0, R0        input state and divF_spts(0) = reference compute_residual(0)
+  Un            state after ``nsteps`` reference RK44 steps (FRSolver::update)
+
+Usage:  python tests/golden/make_golden.py  (needs oracle/_ref/libzefr_ref.so)
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+import tempfile
+import zlib
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import refcpu  # noqa: E402
+from zefr_b200 import ics, meshgen  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# name -> (mesh builder, ndims, order, viscous, bounds, deck params, state builder, nsteps)
+def _cases():
+    tgv_deck = {"disable_nondim": 1, "fix_vis": 1, "mach_fs": 0.1, "Re_fs": 1600, "prandtl": 0.71,
+                "P_fs": 1.0, "rho_fs": 1.0, "L_fs": 1.0, "ldg_b": 0.5, "ldg_tau": 0.1, "dt": 1e-3}
+    cyl_deck = {"disable_nondim": 1, "fix_vis": 1, "mach_fs": 0.2, "Re_fs": 100, "prandtl": 0.72,
+                "P_fs": 1.0, "rho_fs": 1.0, "L_fs": 1.0, "ldg_b": 0.5, "ldg_tau": 0.1, "dt": 1e-3}
+    eul = {"mach_fs": 0.3, "rho_fs": 1.0, "P_fs": 1.0, "dt": 1e-3}
+
+    def vortex(X, g):
+        return ics.isentropic_vortex(X, beta=5.0, gamma=g)
+
+    def tgv(X, g):
+        return ics.taylor_green(X, mach=0.1, gamma=g)
+
+    def tgv_fast(X, g):
+        return ics.taylor_green(X, mach=0.3, gamma=g)
+
+    def cyl_state(X, g):
+        c = 0.2 * np.sqrt(g)
+        return ics.uniform(X, 1.0, (c, 0.0), 1.0, g)
+
+    def shear(X, g):
+        return ics.double_shear_layer(X * 0.1 + 0.5, mach=0.2, gamma=g)
+
+    per = {"PERIODIC": "periodic"}
+    return {
+        "quad_p3_euler_vortex": (lambda: meshgen.box_quads(8, 8), 2, 3, False, per, eul, vortex, 3),
+        "quad_p2_ns_jitter": (lambda: meshgen.jitter_interior(meshgen.box_quads(6, 5), 0.4, 11), 2, 2, True, per,
+                              dict(cyl_deck, ldg_tau=1.0), shear, 2),
+        "quad_p1_euler": (lambda: meshgen.box_quads(5, 5), 2, 1, False, per, eul, vortex, 2),
+        "quad_p5_euler": (lambda: meshgen.box_quads(4, 4), 2, 5, False, per, eul, vortex, 2),
+        "hex_p3_ns_tgv": (lambda: meshgen.box_hexes(3, 3, 3), 3, 3, True, per, tgv_deck, tgv, 2),
+        "hex_p2_euler_jitter": (lambda: meshgen.jitter_interior(meshgen.box_hexes(3, 4, 2), 0.15, 5), 3, 2, False,
+                                per, eul, tgv_fast, 2),
+        "hex_p1_ns": (lambda: meshgen.box_hexes(3, 2, 2), 3, 1, True, per, tgv_deck, tgv, 2),
+        "hex_p4_euler": (lambda: meshgen.box_hexes(2, 2, 2), 3, 4, False, per, eul, tgv_fast, 1),
+        "cyl_p3_ns_char_adi": (lambda: meshgen.cylinder_omesh(4, 8, r1=5.0), 2, 3, True,
+                               {"WALL": "wall_ns_adi", "FARFIELD": "char"}, cyl_deck, cyl_state, 2),
+        "cyl_p2_ns_iso_farfield_b03": (lambda: meshgen.cylinder_omesh(3, 8, r1=4.0), 2, 2, True,
+                                       {"WALL": "wall_ns_iso", "FARFIELD": "farfield"},
+                                       {"mach_fs": 0.2, "Re_fs": 100, "fix_vis": 0, "ldg_b": 0.3, "ldg_tau": 0.2,
+                                        "T_wall": 300.0, "dt": 1e-4}, None, 2),
+        "cyl_p3_euler_slip_char": (lambda: meshgen.cylinder_omesh(4, 8, r1=5.0), 2, 3, False,
+                                   {"WALL": "wall_slip", "FARFIELD": "char"}, dict(eul, mach_fs=0.2), cyl_state, 2),
+        "cyl_p2_euler_supin_sym": (lambda: meshgen.cylinder_omesh(3, 8, r1=4.0), 2, 2, False,
+                                   {"WALL": "symmetry", "FARFIELD": "farfield"}, dict(eul, mach_fs=0.2), cyl_state, 2),
+    }
+
+
+def reference_setup(r: refcpu.RefSolver):
+    """Reference set-up arrays in the per-element-flux-point form of oracle.dfr_numpy.Setup."""
+    Fp, E, D = r.nfpts, r.neles, r.ndims
+    g = r.array("fpt2gfpt").astype(np.int64).reshape(Fp, E)
+    sl = r.array("fpt2gfpt_slot").astype(np.int64).reshape(Fp, E)
+    nG = r.ngfpts
+    gfpt2bnd = r.array("gfpt2bnd").astype(np.int64)
+    owners = np.full((nG, 2), -1, dtype=np.int64)
+    for e in range(E):
+        for f in range(Fp):
+            owners[g[f, e], sl[f, e]] = e * Fp + f
+    partner = np.empty((Fp, E), dtype=np.int64)
+    for e in range(E):
+        for f in range(Fp):
+            gg = g[f, e]
+            if gg < r.ngfpts_int:
+                partner[f, e] = owners[gg, 1 - sl[f, e]]
+            else:
+                partner[f, e] = -1 - gfpt2bnd[gg - r.ngfpts_int]
+    norm = r.array("norm").reshape(D, nG)
+    dA = r.array("dA").reshape(2, nG)
+    fnorm = np.transpose(norm[:, g], (1, 0, 2))            # [Fp, D, E]
+    fdA = np.take_along_axis(dA[:, g.reshape(-1)], sl.reshape(1, -1), axis=0).reshape(Fp, E)
+    S = r.nspts
+    return {
+        "oppE": r.array("oppE"), "oppD": r.array("oppD"), "oppD_fpts": r.array("oppD_fpts"),
+        "oppDiv": r.array("oppDiv"), "oppDiv_fpts": r.array("oppDiv_fpts"),
+        "inv_jaco_spts": r.array("inv_jaco_spts"), "jaco_det_spts": r.array("jaco_det_spts"),
+        "coord_spts": r.array("coord_spts"),
+        "fpt_partner": partner.reshape(-1).astype(np.float64), "fpt_slot": sl.reshape(-1).astype(np.float64),
+        "fpt_norm": fnorm.reshape(-1), "fpt_dA": fdA.reshape(-1),
+    }
+
+
+def make_case(name, spec, tmp):
+    build, ndims, order, viscous, bounds, deck, state_fn, nsteps = spec
+    mesh = build()
+    msh = os.path.join(tmp, name + ".msh")
+    meshgen.write_gmsh(mesh, msh)
+    deck_path = refcpu.write_deck(os.path.join(tmp, name + ".deck"), name + ".msh", ndims, order, viscous,
+                                  bounds, deck)
+    r = refcpu.RefSolver(deck_path)
+    S, V, E = r.state_shape
+    X = r.array("coord_spts").reshape(S, ndims, E)
+    g = r.params["gamma"]
+    if state_fn is None:  # free stream at the reference's non-dimensional values
+        p = r.params
+        U0 = ics.uniform(X, p["rho_fs"], (p["V_fs0"], p["V_fs1"], p["V_fs2"]), p["P_fs"], g)
+    else:
+        U0 = state_fn(X, g)
+    U0 = ics.perturb(U0, 1e-3, seed=zlib.crc32(name.encode()))
+    R0 = r.residual(U0, 0)
+    r.set_state(U0)
+    r.update(nsteps)
+    Un = r.get_state()
+    setup = reference_setup(r)
+    faces_t = np.array([f[0] for f in mesh.bnd_faces], dtype=np.int64)
+    npf = max(len(f[1]) for f in mesh.bnd_faces)
+    faces_n = np.full((len(mesh.bnd_faces), npf), -1, dtype=np.int64)
+    for i, f in enumerate(mesh.bnd_faces):
+        faces_n[i, :len(f[1])] = f[1]
+    faces_name = np.array([f[2] for f in mesh.bnd_faces])
+    meta = {"name": name, "ndims": ndims, "order": order, "viscous": bool(viscous), "bounds": bounds,
+            "deck": deck, "params": r.params, "nsteps": nsteps, "dt": r.params["dt"],
+            "shape": [S, V, E], "nfpts": r.nfpts, "gmsh_type": mesh.gmsh_type}
+    out = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(out, meta=json.dumps(meta), nodes=mesh.nodes, elements=mesh.elements, faces_type=faces_t,
+                        faces_nodes=faces_n, faces_name=faces_name, U0=U0, R0=R0, Un=Un,
+                        **{"setup_" + k: v for k, v in setup.items()})
+    r.close()
+    return out
+
+
+def main(names=None):
+    cases = _cases()
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, spec in cases.items():
+            if names and name not in names:
+                continue
+            out = make_case(name, spec, tmp)
+            print(f"{name}: {os.path.getsize(out) / 1024:.1f} KiB")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

@@ -1,0 +1,63 @@
+"""Loading helpers for the golden fixtures written by tests/golden/make_golden.py."""
+from __future__ import annotations
+
+import glob
+import json
+import os
+from dataclasses import dataclass
+from typing import Dict, List
+
+import numpy as np
+
+from oracle.dfr_numpy import Setup
+from zefr_b200.meshgen import Mesh
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@dataclass
+class Golden:
+    name: str
+    meta: Dict
+    mesh: Mesh
+    bounds: Dict[str, str]
+    params: Dict[str, float]
+    U0: np.ndarray
+    R0: np.ndarray
+    Un: np.ndarray
+    setup_arrays: Dict[str, np.ndarray]
+
+    @property
+    def viscous(self) -> bool:
+        return bool(self.meta["viscous"])
+
+    @property
+    def order(self) -> int:
+        return int(self.meta["order"])
+
+    def setup(self) -> Setup:
+        S, V, E = self.meta["shape"]
+        return Setup.from_arrays(self.meta["ndims"], S, self.meta["nfpts"], E, lambda k: self.setup_arrays[k])
+
+
+def names() -> List[str]:
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+
+
+def load(name: str) -> Golden:
+    z = np.load(os.path.join(GOLDEN_DIR, name + ".npz"), allow_pickle=False)
+    meta = json.loads(str(z["meta"]))
+    faces = []
+    for t, nodes, nm in zip(z["faces_type"], z["faces_nodes"], z["faces_name"]):
+        faces.append((int(t), tuple(int(n) for n in nodes if n >= 0), str(nm)))
+    mesh = Mesh(ndims=meta["ndims"], nodes=z["nodes"], gmsh_type=meta["gmsh_type"], elements=z["elements"],
+                bnd_faces=faces)
+    setup = {k[len("setup_"):]: z[k] for k in z.files if k.startswith("setup_")}
+    return Golden(name=name, meta=meta, mesh=mesh, bounds=meta["bounds"], params=meta["params"], U0=z["U0"],
+                  R0=z["R0"], Un=z["Un"], setup_arrays=setup)
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    """max |a-b| over the tensor, relative to the largest |b| of the same variable."""
+    scale = np.abs(b).max(axis=(0, 2), keepdims=True)
+    return float((np.abs(a - b) / np.maximum(scale, 1e-300)).max())

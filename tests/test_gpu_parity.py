@@ -1,0 +1,194 @@
+"""CUDA residual vs the reference: golden fixtures (produced by the compiled
+reference) and the numpy oracle on larger meshes.  Tolerances are written per
+test: plain FP64 form 1e-12 relative per variable (scale = max |reference| of
+that variable), mixed form 1e-5 relative L2."""
+import numpy as np
+import pytest
+
+import golden_cases as gc
+from oracle import dfr_numpy
+from zefr_b200 import ics, meshgen
+from zefr_b200.solver import FRSolver, Plan, make_params, params_from_reference
+
+pytestmark = pytest.mark.gpu
+
+CASES = gc.names()
+TOL_FP64 = 1e-12
+TOL_MIXED_L2 = 1e-5
+
+
+def solver_for(g, precision="fp64", **kw):
+    return FRSolver(g.mesh, params_from_reference(g.params, g.order, precision=precision, **kw), g.bounds)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_residual_fp64_matches_reference(name):
+    g = gc.load(name)
+    s = solver_for(g)
+    R = s.residual(g.U0, 0)
+    assert gc.rel_err(R, g.R0) < TOL_FP64
+
+
+@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "hex_p3_ns_tgv", "cyl_p3_ns_char_adi"])
+def test_every_stage_register(name):
+    g = gc.load(name)
+    s = solver_for(g)
+    s.set_state(g.U0)
+    for st in range(4):
+        s.compute_residual(st)
+    for st in range(4):
+        assert gc.rel_err(s.get_residual(st), g.R0) < TOL_FP64
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_rk44_steps_match_reference(name):
+    g = gc.load(name)
+    s = solver_for(g)
+    s.set_state(g.U0)
+    s.step(g.meta["nsteps"])
+    assert gc.rel_err(s.get_state(), g.Un) < TOL_FP64
+
+
+def _oracle_case(mesh, order, viscous, bounds, params, U):
+    plan = Plan(mesh, make_params(order, viscous), bounds)
+    S, V, E = U.shape
+    st = dfr_numpy.Setup.from_arrays(mesh.ndims, S, plan.info.nfpts, E, plan.get)
+    return dfr_numpy.residual(st, U, params, viscous)
+
+
+def _ref_params(viscous, mu=0.0, ldg_b=0.5, ldg_tau=0.1, V_fs=(0.3, 0.0, 0.0)):
+    return {"gamma": 1.4, "prandtl": 0.72, "mu": mu, "rt": 0.0, "c_sth": 0.0, "fix_vis": 1.0, "rus_k": 0.0,
+            "ldg_b": ldg_b, "ldg_tau": ldg_tau, "rho_fs": 1.0, "V_fs0": V_fs[0], "V_fs1": V_fs[1], "V_fs2": V_fs[2],
+            "P_fs": 1.0, "T_wall": 1.0, "R_ref": 1.0, "V_wall0": 0.0, "V_wall1": 0.0, "V_wall2": 0.0, "dt": 1e-3,
+            "viscous": float(viscous)}
+
+
+@pytest.mark.parametrize("case", ["quad32_p3_euler", "hex6_p3_ns", "cyl_12x24_p3_ns", "quad_jitter_p4_ns"])
+def test_residual_matches_oracle_larger(case):
+    if case == "quad32_p3_euler":
+        mesh, order, visc, bounds = meshgen.box_quads(32, 32), 3, False, {"PERIODIC": "periodic"}
+        p = _ref_params(False)
+        mk = lambda X: ics.isentropic_vortex(X, beta=5.0)
+    elif case == "hex6_p3_ns":
+        mesh, order, visc = meshgen.box_hexes(6, 6, 6), 3, True
+        bounds = {"PERIODIC": "periodic"}
+        p = _ref_params(True, mu=0.1 * np.sqrt(1.4) / 1600.0)
+        mk = lambda X: ics.taylor_green(X, mach=0.1)
+    elif case == "cyl_12x24_p3_ns":
+        mesh, order, visc = meshgen.cylinder_omesh(12, 24, r1=8.0), 3, True
+        bounds = {"WALL": "wall_ns_adi", "FARFIELD": "char"}
+        p = _ref_params(True, mu=0.2 * np.sqrt(1.4) / 100.0, V_fs=(0.2 * np.sqrt(1.4), 0.0, 0.0))
+        mk = lambda X: ics.uniform(X, 1.0, (0.2 * np.sqrt(1.4), 0.0), 1.0)
+    else:
+        mesh = meshgen.jitter_interior(meshgen.box_quads(10, 9, 0.0, 1.0, 0.0, 1.0), 0.02, 3)
+        order, visc, bounds = 4, True, {"PERIODIC": "periodic"}
+        p = _ref_params(True, mu=1e-3, ldg_b=0.25, ldg_tau=0.5)
+        mk = lambda X: ics.double_shear_layer(X, mach=0.2)
+    params = make_params(order, visc, mu=p["mu"], ldg_b=p["ldg_b"], ldg_tau=p["ldg_tau"], prandtl=p["prandtl"],
+                         V_fs=(p["V_fs0"], p["V_fs1"], p["V_fs2"]), rho_fs=1.0, P_fs=1.0, T_wall=1.0, R_ref=1.0)
+    s = FRSolver(mesh, params, bounds)
+    X = s.plan.get("coord_spts").reshape(s.nspts, mesh.ndims, s.neles)
+    U = ics.perturb(mk(X), 1e-3, seed=7)
+    R = s.residual(U, 0)
+    Ro = _oracle_case(mesh, order, visc, bounds, p, U)
+    assert gc.rel_err(R, Ro) < TOL_FP64
+
+
+@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "hex_p3_ns_tgv", "cyl_p3_ns_char_adi", "quad_p2_ns_jitter"])
+def test_mixed_precision_error(name):
+    g = gc.load(name)
+    s = solver_for(g, precision="mixed")
+    R = s.residual(g.U0, 0)
+    err = np.linalg.norm(R - g.R0) / np.linalg.norm(g.R0)
+    assert err < TOL_MIXED_L2
+
+
+def test_mixed_rk_steps_track_fp64():
+    g = gc.load("hex_p3_ns_tgv")
+    s = solver_for(g, precision="mixed")
+    s.set_state(g.U0)
+    s.step(g.meta["nsteps"])
+    U = s.get_state()
+    err = np.linalg.norm(U - g.Un) / np.linalg.norm(g.Un)
+    assert err < 1e-6
+
+
+@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "hex_p3_ns_tgv", "hex_p2_euler_jitter", "quad_p2_ns_jitter"])
+def test_conservation_periodic(name):
+    """Periodic domain: sum_e sum_s w_s divF = boundary flux = 0."""
+    g = gc.load(name)
+    s = solver_for(g)
+    R = s.residual(g.U0, 0)
+    w = s.plan.get("weights_spts")
+    tot = np.einsum("s,sve->v", w, R)
+    mag = np.einsum("s,sve->v", w, np.abs(R))
+    assert np.all(np.abs(tot) <= 1e-12 * mag + 1e-14)
+
+
+@pytest.mark.parametrize("fconv", ["rusanov", "roe"])
+def test_free_stream_preservation(fconv):
+    """Uniform flow on a jittered (non-affine) mesh is a steady solution."""
+    mesh = meshgen.jitter_interior(meshgen.box_hexes(4, 4, 4), 0.2, 9)
+    params = make_params(3, True, mu=1e-3, fconv=fconv)
+    s = FRSolver(mesh, params, {"PERIODIC": "periodic"})
+    X = s.plan.get("coord_spts").reshape(s.nspts, 3, s.neles)
+    U = ics.uniform(X, 1.2, (0.3, -0.2, 0.1), 0.9)
+    R = s.residual(U, 0)
+    assert np.abs(R).max() < 1e-11
+
+
+def test_roe_close_to_rusanov_on_smooth_flow():
+    g = gc.load("quad_p3_euler_vortex")
+    R1 = solver_for(g).residual(g.U0, 0)
+    R2 = solver_for(g, fconv="roe").residual(g.U0, 0)
+    assert np.isfinite(R2).all()
+    assert np.linalg.norm(R2 - R1) / np.linalg.norm(R1) < 0.05
+
+
+def test_device_pointer_state_roundtrip():
+    import torch
+    g = gc.load("hex_p3_ns_tgv")
+    s = solver_for(g)
+    Ut = torch.from_numpy(g.U0).cuda()
+    s.set_state(Ut)
+    s.compute_residual(0)
+    out = torch.zeros_like(Ut)
+    s.get_residual_device(out, 0)
+    assert gc.rel_err(out.cpu().numpy(), g.R0) < TOL_FP64
+
+
+def test_residual_norms_match_host():
+    g = gc.load("cyl_p3_ns_char_adi")
+    s = solver_for(g)
+    s.set_state(g.U0)
+    s.compute_residual(0)
+    n = s.residual_norms()
+    det = g.setup_arrays["jaco_det_spts"].reshape(g.R0.shape[0], 1, g.R0.shape[2])
+    r = g.R0 / det
+    ndof = r.shape[0] * r.shape[2]
+    assert np.allclose(n["linf"], np.abs(r).max(axis=(0, 2)) / ndof, rtol=1e-12)
+    assert np.allclose(n["l1"], np.abs(r).sum(axis=(0, 2)) / ndof, rtol=1e-10)
+    assert np.allclose(n["l2"], np.sqrt((r * r).sum(axis=(0, 2))) / ndof, rtol=1e-10)
+
+
+def test_nan_state_reported():
+    g = gc.load("quad_p1_euler")
+    s = solver_for(g)
+    U = g.U0.copy()
+    U[0, 0, 0] = np.nan
+    s.set_state(U)
+    s.compute_residual(0)
+    from zefr_b200._lib import ZbError
+    with pytest.raises(ZbError) as ei:
+        s.residual_norms()
+    assert ei.value.status == -5
+
+
+def test_kernels_launched():
+    g = gc.load("hex_p3_ns_tgv")
+    s = solver_for(g)
+    s.set_state(g.U0)
+    n0 = s.launch_count()
+    s.step(1)
+    # viscous RK44 step: two kernels per stage
+    assert s.launch_count() - n0 == 8

@@ -92,6 +92,33 @@ static void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w
     w[n - 1 - i] = wi;
   }
   if (n % 2 == 1) x[n / 2] = 0.0;
+  // Closed forms of the nodes for n <= 5 (the textbook expressions; the
+  // reference evaluates the same ones, src/points.cpp:9-60), so the operators
+  // built from them agree with the reference bit for bit.
+  if (n == 2)
+  {
+    x[0] = -std::sqrt(1. / 3.);
+    x[1] = std::sqrt(1. / 3.);
+  }
+  else if (n == 3)
+  {
+    x[0] = -std::sqrt(3. / 5.);
+    x[2] = std::sqrt(3. / 5.);
+  }
+  else if (n == 4)
+  {
+    x[0] = -std::sqrt((3. + 2. * std::sqrt(6. / 5.)) / 7.);
+    x[1] = -std::sqrt((3. - 2. * std::sqrt(6. / 5.)) / 7.);
+    x[2] = std::sqrt((3. - 2. * std::sqrt(6. / 5.)) / 7.);
+    x[3] = std::sqrt((3. + 2. * std::sqrt(6. / 5.)) / 7.);
+  }
+  else if (n == 5)
+  {
+    x[0] = -(1. / 3.) * std::sqrt(5. + 2. * std::sqrt(10. / 7.));
+    x[1] = -(1. / 3.) * std::sqrt(5. - 2. * std::sqrt(10. / 7.));
+    x[3] = (1. / 3.) * std::sqrt(5. - 2. * std::sqrt(10. / 7.));
+    x[4] = (1. / 3.) * std::sqrt(5. + 2. * std::sqrt(10. / 7.));
+  }
 }
 
 std::vector<double> gauss_legendre_points(int n)
