@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Throughput of the DFR residual on one B200 (or N independent replicas).
+
+Workload: 3D Taylor-Green vortex, 64^3 linear hexes on periodic [0,2pi]^3,
+P = 3 (64 solution points per element, 5 conserved variables, 83.9 M DOF),
+Re = 1600, Ma = 0.1, Pr = 0.71, Roe convective + LDG viscous flux (beta 0.5,
+tau 0.1).  Synthetic: the mesh and the Taylor-Green initial state are
+generated in-process.
+
+One step = one residual evaluation FRSolver::compute_residual(stage):
+extrapolation to flux points, gradients, fluxes, common fluxes and the
+divergence.  value = GDOF/s of the mixed form (FP32 state and pointwise
+arithmetic); the FP64 plain form is timed the same way beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NCELL = 64
+ORDER = 3
+METRIC = "GDOF/s per residual (TGV 64^3 hex P3 NS, mixed form; FP64 plain form beside it)"
+WORKLOAD = "taylor_green_64^3_hex_P3_navier_stokes_roe_ldg"
+TGV_DECK = dict(ndims=3, order=ORDER, viscous=1, disable_nondim=1, fix_vis=1, mach_fs=0.1, Re_fs=1600.0,
+                prandtl=0.71, P_fs=1.0, rho_fs=1.0, L_fs=1.0, ldg_b=0.5, ldg_tau=0.1, dt=1e-4, gamma=1.4)
+
+
+def b_alg(E: int, S: int, V: int, D: int, G: int, Fp: int, w: int) -> float:
+    """Compulsory bytes of one residual: state in + residual out, adjugate + |J|
+    at solution points, face normal + two dA per face point, int32 partner +
+    int8 slot per element flux point."""
+    return E * S * V * (w + w) + E * S * (D * D + 1) * w + G * (D + 2) * w + E * Fp * 5
+
+
+# ---------------------------------------------------------------------------
+# process / timing helpers
+# ---------------------------------------------------------------------------
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def build_solver(precision: str, n: int):
+    import torch
+    from zefr_b200 import ics, meshgen
+    from zefr_b200.solver import FRSolver, params_from_deck
+
+    mesh = meshgen.box_hexes(n, n, n)
+    p = params_from_deck(fconv=2, precision=0 if precision == "fp64" else 1, **TGV_DECK)
+    s = FRSolver(mesh, p, {"PERIODIC": "periodic"})
+    s.set_stream(torch.cuda.current_stream().cuda_stream)
+    X = s.plan.get("coord_spts").reshape(s.nspts, 3, s.neles)
+    U = ics.taylor_green(X, mach=TGV_DECK["mach_fs"], gamma=TGV_DECK["gamma"])
+    return s, U
+
+
+def barrier_sync(world):
+    import torch
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_residuals(s, K: int, W: int, world: int):
+    import torch
+    for i in range(W):
+        s.compute_residual(i % 4)
+    barrier_sync(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = s.launch_count()
+    e0.record()
+    for i in range(K):
+        s.compute_residual(i % 4)
+    e1.record()
+    barrier_sync(world)
+    ms = e0.elapsed_time(e1) / K
+    return max_over_ranks(ms, world), s.launch_count() - n0
+
+
+def kernel_profile(s, K: int):
+    s.profile(True)
+    s.profile_read()
+    for i in range(K):
+        s.compute_residual(i % 4)
+    prof = s.profile_read()
+    s.profile(False)
+    return {k: {"ms_avg": v[0] / max(v[1], 1), "launches": v[1], "ms_total": v[0]} for k, v in prof.items()}
+
+
+def time_rk_stage(s, K: int, world: int):
+    import torch
+    for st in range(4):
+        s.step_RK_stage(st)
+    barrier_sync(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    n = max(4, (K // 4) * 4)
+    for i in range(n):
+        s.step_RK_stage(i % 4)
+    e1.record()
+    barrier_sync(world)
+    return max_over_ranks(e0.elapsed_time(e1) / n, world)
+
+
+def time_e2e(s, U, K: int, W: int, world: int):
+    """Public API with host buffers: pinned host state -> set_state -> residual -> pinned host residual."""
+    import torch
+    Uh = torch.from_numpy(np.ascontiguousarray(U)).pin_memory()
+    Rh = torch.empty_like(Uh).pin_memory()
+    Un, Rn = Uh.numpy(), Rh.numpy()
+    for i in range(W):
+        s.set_state(Un)
+        s.compute_residual(i % 4)
+        s.get_residual(i % 4, out=Rn)
+    barrier_sync(world)
+    t0 = time.perf_counter()
+    for i in range(K):
+        s.set_state(Un)
+        s.compute_residual(i % 4)
+        s.get_residual(i % 4, out=Rn)
+    barrier_sync(world)
+    ms = (time.perf_counter() - t0) * 1e3 / K
+    return max_over_ranks(ms, world), Un.nbytes, Rn.nbytes
+
+
+def cpu_baseline_sample(n: int = 16, min_seconds: float = 10.0, max_calls: int = 40):
+    """Reference CPU residual (compiled reference, release flags, OpenMP on all
+    host cores) on a bounded sample: the same TGV workload at n^3 hexes."""
+    from oracle import refcpu
+    from zefr_b200 import ics, meshgen
+    if not refcpu.available(fast=True):
+        return None
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    with tempfile.TemporaryDirectory() as tmp:
+        mesh = meshgen.box_hexes(n, n, n)
+        meshgen.write_gmsh(mesh, os.path.join(tmp, "tgv.msh"))
+        deck = {k: v for k, v in TGV_DECK.items() if k not in ("ndims", "order", "viscous")}
+        refcpu.write_deck(os.path.join(tmp, "tgv.deck"), "tgv.msh", 3, ORDER, True, {"PERIODIC": "periodic"}, deck)
+        r = refcpu.RefSolver(os.path.join(tmp, "tgv.deck"), fast=True)
+        S, V, E = r.state_shape
+        X = r.array("coord_spts").reshape(S, 3, E)
+        r.set_state(ics.taylor_green(X, mach=TGV_DECK["mach_fs"]))
+        r.compute_residual(0)
+        calls, t0 = 0, time.perf_counter()
+        while calls < max_calls and (time.perf_counter() - t0) < min_seconds:
+            r.compute_residual(calls % 4)
+            calls += 1
+        dt = (time.perf_counter() - t0) / calls
+        r.close()
+    dof = S * V * E
+    return {"value": dof / dt / 1e9, "unit": "GDOF/s", "cores": threads, "kind": "reference",
+            "ms_per_residual": dt * 1e3,
+            "sample": f"reference CPU compute_residual (-Ofast, OpenMP {threads} threads, GiMMiK stand-in GEMM; "
+                      f"compute_F serial in the reference) on TGV {n}^3 hex P3 ({dof} DOF), {calls} calls"}
+
+
+def gpu_arm(args):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    else:
+        torch.cuda.set_device(0)
+    n = args.cells
+    K, W = args.steps, args.warmup
+    out = {}
+    # --- mixed form (value) ---
+    s, U = build_solver("mixed", n)
+    S, V, E, D, Fp = s.nspts, s.nvars, s.neles, s.ndims, s.info.nfpts
+    G = int(s.info.n_gfpts)
+    dof = S * V * E
+    s.set_state(U)
+    clocks = Clocks(local)
+    clocks.start()
+    ms_mixed, launches = time_residuals(s, K, W, world)
+    clk = clocks.stop()
+    prof_mixed = kernel_profile(s, K)
+    rk_mixed = time_rk_stage(s, K, world)
+    R_mixed = s.get_residual(0) if rank == 0 else None
+    s.set_state(U)
+    e2e_ms, h2d, d2h = time_e2e(s, U, max(3, min(K, 10)), min(W, 2), world)
+    s.close()
+    del s
+    torch.cuda.empty_cache()
+    # --- FP64 plain form ---
+    s, _ = build_solver("fp64", n)
+    s.set_state(U)
+    ms_fp64, _ = time_residuals(s, K, W, world)
+    prof_fp64 = kernel_profile(s, K)
+    rk_fp64 = time_rk_stage(s, K, world)
+    R_fp64 = None
+    if rank == 0:
+        s.set_state(U)
+        s.compute_residual(0)
+        R_fp64 = s.get_residual(0)
+    s.close()
+    del s
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    err = float(np.linalg.norm(R_mixed - R_fp64) / np.linalg.norm(R_fp64))
+    peak, peak_kind = measured_peaks()
+    res_kernels = [k for k in prof_mixed if k in ("k_extrap", "k_ns_grad", "k_ns_face", "k_euler")]
+    t_res = sum(prof_mixed[k]["ms_avg"] for k in res_kernels)
+    dom = max(res_kernels, key=lambda k: prof_mixed[k]["ms_avg"])
+    bm = b_alg(E, S, V, D, G, Fp, 4)
+    b64 = b_alg(E, S, V, D, G, Fp, 8)
+    achieved = bm / (t_res * 1e-3) / 1e9
+    t_res64 = sum(prof_fp64[k]["ms_avg"] for k in prof_fp64 if k in res_kernels)
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic_per_element.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf))["mixed_bytes_per_element_per_residual"] * E
+        except Exception:
+            traffic = None
+    value = world * dof / (ms_mixed * 1e-3) / 1e9
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "GDOF/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": ms_mixed,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "mesh": f"{n}^3 linear hexes, periodic [0,2pi]^3", "order": ORDER,
+                   "dof_per_gpu": dof, "elements_per_gpu": E, "flux": "Roe + LDG (beta 0.5, tau 0.1)",
+                   "Re": 1600, "Ma": 0.1, "step": "one compute_residual(stage) incl. extrapolation",
+                   "l2": "inputs larger than L2 (mixed state 336 MB, FP64 state 671 MB)",
+                   "parallelism": "replicas only" if world > 1 else "single GPU"},
+        "fp64": {"value": world * dof / (ms_fp64 * 1e-3) / 1e9, "ms_per_step": ms_fp64, "dtype": "f64",
+                 "rk_stage_ms": rk_fp64, "kernels": prof_fp64,
+                 "roofline_frac_of_measured": b64 / (t_res64 * 1e-3) / 1e9 / peak},
+        "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "mixed_rel_l2_err_vs_fp64": err,
+        "rk_stage_ms": rk_mixed,
+        "kernels": prof_mixed,
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "residual = " + " + ".join(res_kernels) + f" (dominant {dom})",
+                     "algorithmic_bytes_per_launch": bm, "peak_kind": peak_kind},
+        "e2e": {"value": world * dof / (e2e_ms * 1e-3) / 1e9, "unit": "GDOF/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                "path": "zb_set_state(host, pinned) + zb_compute_residual + zb_get_residual(host, pinned)"},
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    return line
+
+
+def profile_run(args):
+    """Short run of one form for an external profiler: W + K residuals, no timing."""
+    import torch
+    torch.cuda.set_device(0)
+    s, U = build_solver(args.profile_form, args.cells)
+    s.set_state(U)
+    for i in range(args.warmup + args.steps):
+        s.compute_residual(i % 4)
+    torch.cuda.synchronize()
+    s.close()
+
+
+# ---------------------------------------------------------------------------
+# reference arm (CPU)
+# ---------------------------------------------------------------------------
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return None
+    from oracle import refcpu
+    if not refcpu.available(fast=True):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libzefr_ref_fast.so not built (make -C oracle)"}
+    from zefr_b200 import ics, meshgen
+    n = args.ref_cells
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    with tempfile.TemporaryDirectory() as tmp:
+        mesh = meshgen.box_hexes(n, n, n)
+        meshgen.write_gmsh(mesh, os.path.join(tmp, "tgv.msh"))
+        deck = {k: v for k, v in TGV_DECK.items() if k not in ("ndims", "order", "viscous")}
+        refcpu.write_deck(os.path.join(tmp, "tgv.deck"), "tgv.msh", 3, ORDER, True, {"PERIODIC": "periodic"}, deck)
+        r = refcpu.RefSolver(os.path.join(tmp, "tgv.deck"), fast=True)
+        S, V, E = r.state_shape
+        X = r.array("coord_spts").reshape(S, 3, E)
+        r.set_state(ics.taylor_green(X, mach=TGV_DECK["mach_fs"]))
+        for i in range(args.warmup):
+            r.compute_residual(i % 4)
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            r.compute_residual(i % 4)
+        dt = (time.perf_counter() - t0) / args.steps
+        r.close()
+    dof = S * V * E
+    value = dof / dt / 1e9
+    sample = (f"reference CPU FRSolver::compute_residual (-Ofast, OpenMP {threads} threads, GiMMiK stand-in GEMM) "
+              f"on TGV {n}^3 hex P3 ({dof} DOF) per step")
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "GDOF/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_mesh": f"{n}^3 linear hexes", "order": ORDER, "dof": dof},
+            "cpu_baseline": {"value": value, "unit": "GDOF/s", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=NCELL, help=argparse.SUPPRESS)
+    ap.add_argument("--ref-cells", type=int, default=20, help=argparse.SUPPRESS)
+    ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--profile-form", choices=["mixed", "fp64"], default=None, help=argparse.SUPPRESS)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.profile_form:
+        profile_run(args)
+        return
+    line = reference_arm(args) if args.impl == "reference" else gpu_arm(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

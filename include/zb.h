@@ -74,6 +74,18 @@ enum { ZB_FP64 = 0, ZB_MIXED = 1 };
 /* Where a buffer lives. */
 enum { ZB_HOST = 0, ZB_DEVICE = 1 };
 
+/* Kernel ids for zb_profile_read. */
+enum {
+  ZB_K_EXTRAP = 0,     /* state -> flux points */
+  ZB_K_EULER = 1,      /* Euler volume + common flux + divergence (+RK) */
+  ZB_K_NS_GRAD = 2,    /* NS common solution, gradient, flux, volume divergence */
+  ZB_K_NS_FACE = 3,    /* NS common flux + surface correction (+RK) */
+  ZB_K_TO_TILES = 4,   /* state import */
+  ZB_K_FROM_TILES = 5, /* state / residual export */
+  ZB_K_NORMS = 6,      /* FP64 residual norms */
+  ZB_NKERNELS = 8
+};
+
 typedef struct zb_mesh {
   int ndims;                 /* 2 or 3 */
   int gmsh_type;             /* volume element: 2 tri3, 3 quad4, 10 quad9, 5 hex8 */
@@ -196,6 +208,15 @@ zb_status zb_synchronize(zb_ctx *ctx);
 
 /* Number of kernels this library launched on the context since creation. */
 int64_t zb_launch_count(const zb_ctx *ctx);
+
+/* Per-kernel device timing with CUDA events recorded on the context's stream
+ * around every launch (no reference counterpart; the reference brackets
+ * stages with std::chrono timers, include/inputstruct.hpp:35-95).
+ * zb_profile_read synchronises, returns total milliseconds and launch counts
+ * per ZB_K_* id accumulated since the last read, and resets them. */
+zb_status zb_profile_enable(zb_ctx *ctx, int on);
+zb_status zb_profile_read(zb_ctx *ctx, double *ms, int64_t *count);
+const char *zb_kernel_name(int id);
 
 #ifdef __cplusplus
 }

@@ -32,8 +32,9 @@ EXPORTED = [
     "zb_plan_create", "zb_plan_free", "zb_plan_info", "zb_plan_get", "zb_create", "zb_create_from_mesh",
     "zb_destroy", "zb_info_get", "zb_set_stream", "zb_set_dt", "zb_set_state", "zb_get_state",
     "zb_compute_residual", "zb_get_residual", "zb_rk_stage", "zb_step", "zb_residual_norms",
-    "zb_synchronize", "zb_launch_count",
+    "zb_synchronize", "zb_launch_count", "zb_profile_enable", "zb_profile_read", "zb_kernel_name",
 ]
+ZB_NKERNELS = 8
 
 
 class ZbMesh(ctypes.Structure):
@@ -119,6 +120,10 @@ def lib() -> ctypes.CDLL:
         L.zb_synchronize.argtypes = [vp]
         L.zb_launch_count.argtypes = [vp]
         L.zb_launch_count.restype = ctypes.c_int64
+        L.zb_profile_enable.argtypes = [vp, ctypes.c_int]
+        L.zb_profile_read.argtypes = [vp, dp, ctypes.POINTER(i64)]
+        L.zb_kernel_name.restype = ctypes.c_char_p
+        L.zb_kernel_name.argtypes = [ctypes.c_int]
         _lib = L
     return _lib
 

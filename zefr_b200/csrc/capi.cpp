@@ -323,4 +323,27 @@ zb_status zb_synchronize(zb_ctx *ctx)
 
 int64_t zb_launch_count(const zb_ctx *ctx) { return ctx ? zb::ctx_launches(ctx->impl) : -1; }
 
+zb_status zb_profile_enable(zb_ctx *ctx, int on)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_profile_enable(ctx->impl, on);
+  })
+}
+
+zb_status zb_profile_read(zb_ctx *ctx, double *ms, int64_t *count)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_profile_read(ctx->impl, ms, count);
+  })
+}
+
+const char *zb_kernel_name(int id)
+{
+  static const char *names[ZB_NKERNELS] = {"k_extrap", "k_euler", "k_ns_grad", "k_ns_face",
+                                           "k_to_tiles", "k_from_tiles", "k_norms", "unused"};
+  return (id >= 0 && id < ZB_NKERNELS) ? names[id] : "unknown";
+}
+
 }  // extern "C"

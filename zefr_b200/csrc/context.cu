@@ -54,8 +54,53 @@ struct Ctx
   bool ufp_valid = false;
   double dt = 0.0;
   int64_t launches = 0;
+  // per-kernel CUDA-event timing (zb_profile_*)
+  bool profiling = false;
+  struct Rec { int kid; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  double prof_ms[ZB_NKERNELS] = {0};
+  int64_t prof_n[ZB_NKERNELS] = {0};
   void (*launch_extrap)(Ctx &) = nullptr;
   void (*launch_stage)(Ctx &, const StageCfg &) = nullptr;
+};
+
+static cudaEvent_t take_event(Ctx &c)
+{
+  if (!c.pool.empty())
+  {
+    cudaEvent_t e = c.pool.back();
+    c.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CK(cudaEventCreate(&e));
+  return e;
+}
+
+// Brackets one kernel launch with events when profiling is on.
+struct ProfScope
+{
+  Ctx &c;
+  int kid;
+  cudaEvent_t a = nullptr;
+  ProfScope(Ctx &cc, int k) : c(cc), kid(k)
+  {
+    if (c.profiling)
+    {
+      a = take_event(c);
+      CK(cudaEventRecord(a, c.stream));
+    }
+  }
+  ~ProfScope()
+  {
+    if (c.profiling && a)
+    {
+      cudaEvent_t b = take_event(c);
+      cudaEventRecord(b, c.stream);
+      c.recs.push_back({kid, a, b});
+    }
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -218,6 +263,7 @@ static void launch_extrap_impl(Ctx &c)
 {
   using G = Shape<D, N>;
   const int64_t work = c.ntiles * G::Fp * TW;
+  ProfScope ps(c, ZB_K_EXTRAP);
   dev::k_extrap<T, D, N><<<grid_for(work, 256), 256, 0, c.stream>>>((const T *)c.U, (T *)c.Ufp[c.cur], c.ntiles,
                                                                       line_ops<T, N>(c.plan));
   c.launches++;
@@ -270,6 +316,7 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
   {
     const size_t smem = (size_t)(S * V + D * S * V + Fp * V) * TW * sizeof(T) + ops_bytes;
     set_smem(dev::k_euler<T, D, N>, smem);
+    ProfScope ps(c, ZB_K_EULER);
     dev::k_euler<T, D, N><<<(unsigned)c.ntiles, NT, smem, c.stream>>>(a, ops);
     c.launches++;
     CK(cudaGetLastError());
@@ -278,11 +325,15 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
   {
     const size_t smem1 = (size_t)(S * V + Fp * V + D * S * V) * TW * sizeof(T) + ops_bytes;
     set_smem(dev::k_ns_grad<T, D, N>, smem1);
-    dev::k_ns_grad<T, D, N><<<(unsigned)c.ntiles, NT, smem1, c.stream>>>(a, ops);
-    c.launches++;
-    CK(cudaGetLastError());
+    {
+      ProfScope ps(c, ZB_K_NS_GRAD);
+      dev::k_ns_grad<T, D, N><<<(unsigned)c.ntiles, NT, smem1, c.stream>>>(a, ops);
+      c.launches++;
+      CK(cudaGetLastError());
+    }
     const size_t smem2 = (size_t)(Fp * V + S * V) * TW * sizeof(T) + ops_bytes;
     set_smem(dev::k_ns_face<T, D, N>, smem2);
+    ProfScope ps(c, ZB_K_NS_FACE);
     dev::k_ns_face<T, D, N><<<(unsigned)c.ntiles, NT, smem2, c.stream>>>(a, ops);
     c.launches++;
     CK(cudaGetLastError());
@@ -331,6 +382,12 @@ static void free_all(Ctx *c)
                   c->Ufp[1], c->Fvn, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred};
   for (void *b : bufs)
     if (b) cudaFree(b);
+  for (auto &r : c->recs)
+  {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : c->pool) cudaEventDestroy(e);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -513,6 +570,7 @@ void ctx_set_state(Ctx *c, const double *U, int64_t ss, int64_t vs, int64_t es, 
   const size_t ext = extent(c, ss, vs, es, c->S);
   const double *src = stage_in(c, U, ext, where);
   const int64_t work = c->ntiles * c->S * c->V * TW;
+  ProfScope ps(*c, ZB_K_TO_TILES);
   if (c->prec == ZB_FP64)
     k_to_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>(src, (double *)c->U, nullptr, c->plan.neles,
                                                                      c->ntiles, c->S, c->V, ss, vs, es);
@@ -541,10 +599,14 @@ static void from_tiles(Ctx *c, const void *srcT, const void *comp, double *out, 
       c->dtmp_bytes = bytes;
     }
     dst = c->dtmp;
-    // keep caller's holes intact: start from the caller's buffer
-    CK(cudaMemcpyAsync(dst, out, bytes, cudaMemcpyHostToDevice, c->stream));
+    // a strided caller buffer has holes the export must leave intact: start
+    // from its contents (a dense buffer is overwritten entirely)
+    if (ext != (size_t)c->S * c->V * c->plan.neles)
+      CK(cudaMemcpyAsync(dst, out, bytes, cudaMemcpyHostToDevice, c->stream));
   }
   const int64_t work = c->plan.neles * c->S * c->V;
+  {
+  ProfScope ps(*c, ZB_K_FROM_TILES);
   if (c->prec == ZB_FP64)
     k_from_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>((const double *)srcT, (const double *)comp, dst,
                                                                        c->plan.neles, c->S, c->V, ss, vs, es);
@@ -553,6 +615,7 @@ static void from_tiles(Ctx *c, const void *srcT, const void *comp, double *out, 
                                                                       c->plan.neles, c->S, c->V, ss, vs, es);
   c->launches++;
   CK(cudaGetLastError());
+  }
   if (where == ZB_HOST)
   {
     CK(cudaMemcpyAsync(out, dst, ext * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -578,6 +641,8 @@ static void ensure_ufp(Ctx *c)
 void ctx_compute_residual(Ctx *c, unsigned stage)
 {
   if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  // extrapolate_U is step 1 of the reference residual (src/solver.cpp:1516-1518)
+  c->ufp_valid = false;
   ensure_ufp(c);
   StageCfg sc{stage, 0, 0, 0};
   c->launch_stage(*c, sc);
@@ -615,6 +680,8 @@ void ctx_norms(Ctx *c, double *out)
   CK(cudaMemsetAsync(c->dred, 0, 3 * 8 * sizeof(double), c->stream));
   const int64_t work = c->plan.neles * c->S;
   const int blocks = grid_for(work, 256);
+  {
+  ProfScope ps(*c, ZB_K_NORMS);
   if (c->prec == ZB_FP64)
     k_norms<double><<<blocks, 256, 0, c->stream>>>((const double *)c->divF[0], (const double *)c->mets, c->plan.neles,
                                                    c->S, V, c->D * c->D + 1, c->D * c->D, c->dred);
@@ -623,6 +690,7 @@ void ctx_norms(Ctx *c, double *out)
                                                   c->S, V, c->D * c->D + 1, c->D * c->D, c->dred);
   c->launches++;
   CK(cudaGetLastError());
+  }
   double h[24];
   CK(cudaMemcpyAsync(h, c->dred, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -641,5 +709,33 @@ void ctx_norms(Ctx *c, double *out)
 void ctx_sync(Ctx *c) { CK(cudaStreamSynchronize(c->stream)); }
 
 int64_t ctx_launches(const Ctx *c) { return c->launches; }
+
+void ctx_profile_enable(Ctx *c, int on)
+{
+  CK(cudaStreamSynchronize(c->stream));
+  c->profiling = (on != 0);
+}
+
+void ctx_profile_read(Ctx *c, double *ms, int64_t *count)
+{
+  CK(cudaStreamSynchronize(c->stream));
+  for (auto &r : c->recs)
+  {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, r.a, r.b));
+    c->prof_ms[r.kid] += t;
+    c->prof_n[r.kid] += 1;
+    c->pool.push_back(r.a);
+    c->pool.push_back(r.b);
+  }
+  c->recs.clear();
+  for (int k = 0; k < ZB_NKERNELS; k++)
+  {
+    if (ms) ms[k] = c->prof_ms[k];
+    if (count) count[k] = c->prof_n[k];
+    c->prof_ms[k] = 0.0;
+    c->prof_n[k] = 0;
+  }
+}
 
 }  // namespace zb

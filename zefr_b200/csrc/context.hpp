@@ -30,6 +30,8 @@ void ctx_step(Ctx *c, int n);
 void ctx_norms(Ctx *c, double *out);
 void ctx_sync(Ctx *c);
 int64_t ctx_launches(const Ctx *c);
+void ctx_profile_enable(Ctx *c, int on);
+void ctx_profile_read(Ctx *c, double *ms, int64_t *count);
 
 }  // namespace zb
 

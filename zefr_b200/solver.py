@@ -202,8 +202,11 @@ class FRSolver:
     def compute_residual(self, stage: int = 0) -> None:
         check(lib().zb_compute_residual(self.h, stage))
 
-    def get_residual(self, stage: int = 0) -> np.ndarray:
-        out = np.zeros(self.state_shape)
+    def get_residual(self, stage: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(self.state_shape)
+        elif out.shape != self.state_shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of state_shape")
         check(lib().zb_get_residual(self.h, stage, out.ctypes.data_as(_DP), *self._strides(), _lib.ZB_HOST))
         return out
 
@@ -243,3 +246,15 @@ class FRSolver:
 
     def launch_count(self) -> int:
         return int(lib().zb_launch_count(self.h))
+
+    def profile(self, on: bool = True) -> None:
+        """Record CUDA events around every kernel launch (device timing per kernel)."""
+        check(lib().zb_profile_enable(self.h, int(on)))
+
+    def profile_read(self) -> Dict[str, tuple]:
+        """{kernel name: (total ms, launches)} since the last read."""
+        ms = np.zeros(_lib.ZB_NKERNELS)
+        cnt = np.zeros(_lib.ZB_NKERNELS, dtype=np.int64)
+        check(lib().zb_profile_read(self.h, ms.ctypes.data_as(_DP), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return {lib().zb_kernel_name(k).decode(): (float(ms[k]), int(cnt[k])) for k in range(_lib.ZB_NKERNELS)
+                if cnt[k] > 0}
