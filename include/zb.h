@@ -218,6 +218,25 @@ zb_status zb_profile_enable(zb_ctx *ctx, int on);
 zb_status zb_profile_read(zb_ctx *ctx, double *ms, int64_t *count);
 const char *zb_kernel_name(int id);
 
+/* FP64 residual divF_spts = |J| div F for callers that cannot allocate device
+ * memory.  No counterpart in the reference (its residual lives in FRSolver's
+ * own allocated arrays).
+ *
+ * U and divF are device pointers the caller owns, dense in the reference
+ * layout [nspts][nvars][n_eles].  Every intermediate lives in one file-scope
+ * device array of 32 MiB that each GPU loading this library holds until the
+ * process exits; meshes whose geometry and intermediates exceed it are
+ * rejected with ZB_ERR_ARG and a message giving the bytes needed.  The call
+ * itself allocates nothing: it copies the plan's geometry from host memory
+ * into that array, packs it, and runs the same kernels as
+ * zb_compute_residual on `stream` (a cudaStream_t, or NULL for the default
+ * stream), returning without synchronising.
+ * The first call on each device looks up the array's device address, with
+ * that device current; make that first call before any stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU (other
+ * streams, other host threads, other plans) race on it. */
+zb_status zb_compute_residual_noalloc(const zb_plan *plan, const double *U, double *divF, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -339,6 +339,14 @@ zb_status zb_profile_read(zb_ctx *ctx, double *ms, int64_t *count)
   })
 }
 
+zb_status zb_compute_residual_noalloc(const zb_plan *plan, const double *U, double *divF, void *stream)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(plan, "null plan");
+    zb::noalloc_residual(plan->plan, U, divF, (cudaStream_t)stream);
+  })
+}
+
 const char *zb_kernel_name(int id)
 {
   static const char *names[ZB_NKERNELS] = {"k_extrap", "k_euler", "k_ns_grad", "k_ns_face",

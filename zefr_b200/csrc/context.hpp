@@ -32,6 +32,7 @@ void ctx_sync(Ctx *c);
 int64_t ctx_launches(const Ctx *c);
 void ctx_profile_enable(Ctx *c, int on);
 void ctx_profile_read(Ctx *c, double *ms, int64_t *count);
+void noalloc_residual(const Plan &p, const double *U, double *divF, cudaStream_t st);
 
 }  // namespace zb
 
