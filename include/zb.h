@@ -66,9 +66,14 @@ enum {
 /* Common convective flux (reference FC_TYPE, include/input.hpp:28-31, plus Roe). */
 enum { ZB_FLUX_RUSANOV = 0, ZB_FLUX_ROE = 2 };
 
-/* Arithmetic of the residual.  ZB_FP64: FP64 throughout (the form checked
- * against the reference).  ZB_MIXED: FP32 state, residual and pointwise flux,
- * FP64 metrics at set-up only, compensated RK accumulation. */
+/* Arithmetic of the residual.
+ *  ZB_FP64:  FP64 storage and arithmetic (the form checked against the
+ *            reference).
+ *  ZB_MIXED: FP32 state (stored as deviations from its mean), traces, metrics,
+ *            residual and pointwise arithmetic, with the inviscid flux
+ *            evaluated as a deviation from the reference state; FP64 for the
+ *            set-up (metrics, operators) and for the norm and functional
+ *            reductions; Kahan-compensated RK accumulation. */
 enum { ZB_FP64 = 0, ZB_MIXED = 1 };
 
 /* Where a buffer lives. */
@@ -202,6 +207,14 @@ zb_status zb_step(zb_ctx *ctx, int n);
 /* Residual norms of report_residuals (src/solver.cpp:6990-7137), FP64 device
  * reduction of divF(stage 0)/|J| per variable: out[3*nvars] = L1, L2, Linf. */
 zb_status zb_residual_norms(zb_ctx *ctx, double *out);
+
+/* Volume integrals of FRSolver::report_turbulent_stats (src/solver.cpp:
+ * 7813-7917) in FP64 over the current state: out[0] = integral of
+ * 1/2 rho |u|^2, out[1] = integral of 1/2 rho |curl u|^2 (Navier-Stokes only:
+ * the gradient is evaluated with the LDG corrected gradient of the residual),
+ * out[2] = domain volume.  The reference prints out[0..1] / (out[2] rho_fs
+ * |V_fs|^2). */
+zb_status zb_functionals(zb_ctx *ctx, double *out);
 
 /* Wait for all work queued on the context's stream. */
 zb_status zb_synchronize(zb_ctx *ctx);

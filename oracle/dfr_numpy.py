@@ -258,10 +258,57 @@ def _normal(F: np.ndarray, n: np.ndarray) -> np.ndarray:
     return out
 
 
+def roe_flux(UL: np.ndarray, UR: np.ndarray, n: np.ndarray, gamma: float) -> np.ndarray:
+    """Roe approximate Riemann flux (Roe 1981; eigen-decomposition as in Toro,
+    Riemann Solvers and Numerical Methods, sec. 11.3) with Harten's entropy fix
+    (|l| < delta -> (l^2 + delta^2)/(2 delta), delta = 0.1 (|u_n| + a) of the
+    Roe state).  No reference counterpart: the reference has only Rusanov.
+    UL, UR [V, M]; n [D, M] unit normals."""
+    V = UL.shape[0]
+    D = V - 2
+    FL, PL = _flux_conv(UL, gamma)
+    FR, PR = _flux_conv(UR, gamma)
+    rL, rR = UL[0], UR[0]
+    sL, sR = np.sqrt(rL), np.sqrt(rR)
+    inv = 1.0 / (sL + sR)
+    uL = [UL[d + 1] / rL for d in range(D)]
+    uR = [UR[d + 1] / rR for d in range(D)]
+    u = [(sL * uL[d] + sR * uR[d]) * inv for d in range(D)]
+    unL = sum(uL[d] * n[d] for d in range(D))
+    unR = sum(uR[d] * n[d] for d in range(D))
+    H = (sL * (UL[D + 1] + PL) / rL + sR * (UR[D + 1] + PR) / rR) * inv
+    q2 = sum(u[d] * u[d] for d in range(D))
+    un = sum(u[d] * n[d] for d in range(D))
+    a2 = np.maximum((gamma - 1.0) * (H - 0.5 * q2), 1e-30)
+    a = np.sqrt(a2)
+    rho = sL * sR
+    dp, dr, dun = PR - PL, rR - rL, unR - unL
+    a1 = (dp - rho * a * dun) / (2.0 * a2)
+    a3 = (dp + rho * a * dun) / (2.0 * a2)
+    a2w = dr - dp / a2
+    delta = 0.1 * (np.abs(un) + a)
+
+    def fix(lam):
+        lam = np.abs(lam)
+        return np.where(lam < delta, (lam * lam + delta * delta) / (2.0 * delta), lam)
+
+    l1, l2, l3 = fix(un - a), fix(un), fix(un + a)
+    dvt = [(uR[d] - uL[d]) - dun * n[d] for d in range(D)]
+    diss = np.empty_like(UL)
+    diss[0] = l1 * a1 + l2 * a2w + l3 * a3
+    for d in range(D):
+        diss[d + 1] = l1 * a1 * (u[d] - a * n[d]) + l2 * (a2w * u[d] + rho * dvt[d]) + l3 * a3 * (u[d] + a * n[d])
+    udvt = sum(u[d] * dvt[d] for d in range(D))
+    diss[D + 1] = l1 * a1 * (H - a * un) + l2 * (a2w * 0.5 * q2 + rho * udvt) + l3 * a3 * (H + a * un)
+    return 0.5 * (_normal(FL, n) + _normal(FR, n)) - 0.5 * diss
+
+
 def residual(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, fconv: str = "rusanov") -> np.ndarray:
-    """divF_spts(stage) for state U [S, V, E] (reference form, |J| div F)."""
-    if fconv != "rusanov":
-        raise ValueError("the reference has only the Rusanov convective flux")
+    """divF_spts(stage) for state U [S, V, E] (reference form, |J| div F).
+
+    fconv "rusanov" restates the reference; "roe" swaps in :func:`roe_flux`."""
+    if fconv not in ("rusanov", "roe"):
+        raise ValueError("unknown convective flux " + fconv)
     S, V, E = U.shape
     D = st.ndims
     Fp = st.oppE.shape[0]
@@ -328,7 +375,10 @@ def residual(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, fconv
     VnL = sum(UL[d + 1] / UL[0] * n[d] for d in range(D))
     VnR = sum(UR[d + 1] / UR[0] * n[d] for d in range(D))
     eig = np.maximum(np.abs(VnL) + aL, np.abs(VnR) + aR)
-    Fc = 0.5 * (_normal(FR, n) + _normal(FL, n)) - 0.5 * eig * (1.0 - p["rus_k"]) * (UR - UL)
+    if fconv == "roe":
+        Fc = roe_flux(UL, UR, n, gamma)
+    else:
+        Fc = 0.5 * (_normal(FR, n) + _normal(FL, n)) - 0.5 * eig * (1.0 - p["rus_k"]) * (UR - UL)
     sign = np.where(slot == 0, 1.0, -1.0)
     Fcomm = sign * Fc * dA
     if viscous:
@@ -359,6 +409,66 @@ def residual(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, fconv
     Fcomm = Fcomm.reshape(V, Fp, E).transpose(1, 0, 2)
     # 8. surface correction
     return divF + np.einsum("sf,fve->sve", st.oppDiv_fpts, Fcomm)
+
+
+def physical_gradient(st: Setup, U: np.ndarray, p: Dict[str, float]) -> np.ndarray:
+    """LDG-corrected physical gradient [D, S, V, E] of compute_dU_spts/_fpts +
+    compute_F (src/elements.cpp:1393-1447, 1620-1653)."""
+    S, V, E = U.shape
+    D = st.ndims
+    Fp = st.oppE.shape[0]
+    Ufp = np.einsum("fs,sve->fve", st.oppE, U)
+    own = Ufp.transpose(1, 0, 2).reshape(V, Fp * E)
+    part = st.partner.reshape(-1)
+    interior = part >= 0
+    pe = np.where(interior, part // Fp, 0)
+    pf = np.where(interior, part % Fp, 0)
+    other = Ufp[pf, :, pe].T
+    slot = st.slot.reshape(-1)
+    n = st.norm.transpose(1, 0, 2).reshape(D, Fp * E)
+    bc = np.where(interior, 0, -1 - part)
+    UL = np.where(slot == 0, own, other)
+    URi = np.where(slot == 0, other, own)
+    _, UBg = _ghost(bc, own, n, p)
+    UB = np.where(interior, URi, UBg)
+    beta = p["ldg_b"]
+    if beta == 0.5:
+        UC = UB.copy()
+    elif beta == -0.5:
+        UC = UL.copy()
+    else:
+        UC = 0.5 * (UL + UB) - beta * (UL - UB)
+    UC = np.where(interior, UC, UBg)
+    Ucomm = UC.reshape(V, Fp, E).transpose(1, 0, 2)
+    dU = np.einsum("dst,tve->dsve", st.oppD, U) + np.einsum("dsf,fve->dsve", st.oppD_fpts, Ucomm)
+    out = np.zeros_like(dU)
+    for d1 in range(D):
+        acc = 0.0
+        for d2 in range(D):
+            acc = acc + dU[d2] * st.inv_jaco[d2, :, d1][:, None, :]
+        out[d1] = acc * (1.0 / st.jaco_det)[:, None, :]
+    return out
+
+
+def functionals(st: Setup, U: np.ndarray, weights: np.ndarray, p: Dict[str, float], viscous: bool):
+    """Kinetic energy, enstrophy and volume integrals (report_turbulent_stats,
+    src/solver.cpp:7813-7917), unnormalised."""
+    S, V, E = U.shape
+    D = st.ndims
+    jw = st.jaco_det * weights[:, None]
+    rho = U[:, 0]
+    vel = [U[:, d + 1] / rho for d in range(D)]
+    ke = float((jw * 0.5 * rho * sum(v * v for v in vel)).sum())
+    en = 0.0
+    if viscous:
+        g = physical_gradient(st, U, p)  # [D, S, V, E]
+        du = [[(g[j, :, i + 1] - g[j, :, 0] * vel[i]) / rho for j in range(D)] for i in range(D)]
+        if D == 3:
+            w2 = (du[2][1] - du[1][2]) ** 2 + (du[0][2] - du[2][0]) ** 2 + (du[1][0] - du[0][1]) ** 2
+        else:
+            w2 = (du[1][0] - du[0][1]) ** 2
+        en = float((jw * 0.5 * rho * w2).sum())
+    return {"ke": ke, "enstrophy": en, "volume": float(jw.sum())}
 
 
 def rk44_step(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, dt: float) -> np.ndarray:

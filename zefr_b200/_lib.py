@@ -33,7 +33,7 @@ EXPORTED = [
     "zb_destroy", "zb_info_get", "zb_set_stream", "zb_set_dt", "zb_set_state", "zb_get_state",
     "zb_compute_residual", "zb_get_residual", "zb_rk_stage", "zb_step", "zb_residual_norms",
     "zb_synchronize", "zb_launch_count", "zb_profile_enable", "zb_profile_read", "zb_kernel_name",
-    "zb_compute_residual_noalloc",
+    "zb_compute_residual_noalloc", "zb_functionals",
 ]
 ZB_NKERNELS = 8
 
@@ -126,6 +126,7 @@ def lib() -> ctypes.CDLL:
         L.zb_kernel_name.restype = ctypes.c_char_p
         L.zb_kernel_name.argtypes = [ctypes.c_int]
         L.zb_compute_residual_noalloc.argtypes = [vp, dp, dp, vp]
+        L.zb_functionals.argtypes = [vp, dp]
         _lib = L
     return _lib
 

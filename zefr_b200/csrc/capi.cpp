@@ -313,6 +313,14 @@ zb_status zb_residual_norms(zb_ctx *ctx, double *out)
   })
 }
 
+zb_status zb_functionals(zb_ctx *ctx, double *out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && out, "null argument");
+    zb::ctx_functionals(ctx->impl, out);
+  })
+}
+
 zb_status zb_synchronize(zb_ctx *ctx)
 {
   ZB_GUARD({

@@ -5,7 +5,7 @@
 #include <mutex>
 
 #include "context.hpp"
-#include "dfr_kernels.cuh"
+#include "hex_kernels.cuh"
 
 namespace zb {
 
@@ -27,6 +27,8 @@ struct StageCfg
   int rk_mode;      // 0 none, 1 stage update, 2 final combination
   int save_ini;
   int extrap_next;
+  int want_dU = 0;     // write the physical gradient (NS)
+  int grad_only = 0;   // NS: stop after the gradient kernel
 };
 
 // RK44 tables (src/solver.cpp:722-735)
@@ -40,7 +42,8 @@ struct Ctx
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int prec = ZB_FP64;
-  size_t tsz = 8;
+  size_t tsz = 8;  // storage type size
+  size_t asz = 8;  // arithmetic type size
   int D = 0, N = 0, S = 0, Fp = 0, V = 0, nstages = 4;
   int64_t ntiles = 0;
   void *U = nullptr, *U_ini = nullptr, *divF[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -53,6 +56,13 @@ struct Ctx
   int cur = 0;
   bool ufp_valid = false;
   double dt = 0.0;
+  // mixed form: reference state (FP32-representable values) the stored state
+  // deviates from; zero for the FP64 form
+  double uref[5] = {0, 0, 0, 0, 0};
+  double *dref = nullptr;  // device copy for the conversion kernels
+  void *dU = nullptr;          // physical gradient side output (functionals)
+  double *dweights = nullptr;  // quadrature weights of the solution points
+  double *dfun = nullptr;      // functional reduction buffer
   int64_t launches = 0;
   // per-kernel CUDA-event timing (zb_profile_*)
   bool profiling = false;
@@ -107,10 +117,12 @@ struct ProfScope
 // layout conversion kernels
 // ---------------------------------------------------------------------------
 
-// reference-strided FP64 -> tile-major T; padded elements copy element 0
+// reference-strided FP64 -> tile-major T, minus the reference state ref[v]
+// (nullptr: none); padded elements copy element 0
 template <typename T>
-__global__ void k_to_tiles(const double *__restrict__ src, T *__restrict__ dst, T *__restrict__ comp, int64_t neles,
-                           int64_t ntiles, int npts, int nv, int64_t ss, int64_t vs, int64_t es)
+__global__ void k_to_tiles(const double *__restrict__ src, T *__restrict__ dst, T *__restrict__ comp,
+                           const double *__restrict__ ref, int64_t neles, int64_t ntiles, int npts, int nv, int64_t ss,
+                           int64_t vs, int64_t es)
 {
   const int64_t total = ntiles * npts * nv * TW;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
@@ -121,14 +133,16 @@ __global__ void k_to_tiles(const double *__restrict__ src, T *__restrict__ dst, 
     const int64_t t = i / ((int64_t)TW * nv * npts);
     int64_t e = t * TW + l;
     if (e >= neles) e = 0;
-    dst[i] = (T)src[p * ss + v * vs + e * es];
+    const double x = src[p * ss + v * vs + e * es];
+    dst[i] = (T)(ref ? x - ref[v] : x);
     if (comp) comp[i] = T(0);
   }
 }
 
 template <typename T>
-__global__ void k_from_tiles(const T *__restrict__ srcT, const T *__restrict__ comp, double *__restrict__ dst,
-                             int64_t neles, int npts, int nv, int64_t ss, int64_t vs, int64_t es)
+__global__ void k_from_tiles(const T *__restrict__ srcT, const T *__restrict__ comp, const double *__restrict__ ref,
+                             double *__restrict__ dst, int64_t neles, int npts, int nv, int64_t ss, int64_t vs,
+                             int64_t es)
 {
   const int64_t total = neles * npts * nv;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
@@ -141,7 +155,28 @@ __global__ void k_from_tiles(const T *__restrict__ srcT, const T *__restrict__ c
     const int64_t j = ((t * npts + p) * nv + v) * TW + l;
     double val = (double)srcT[j];
     if (comp) val -= (double)comp[j];
+    if (ref) val += ref[v];
     dst[p * ss + v * vs + e * es] = val;
+  }
+}
+
+// per-variable sum over all points and elements of a reference-strided array
+__global__ void k_var_sums(const double *__restrict__ src, int64_t neles, int npts, int nv, int64_t ss, int64_t vs,
+                           int64_t es, double *out)
+{
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int64_t n = neles * npts;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int64_t e = i % neles;
+    const int p = (int)(i / neles);
+    for (int v = 0; v < nv; v++) acc[v] += src[p * ss + v * vs + e * es];
+  }
+  for (int v = 0; v < nv; v++)
+  {
+    double x = acc[v];
+    for (int o = 16; o > 0; o /= 2) x += __shfl_down_sync(0xffffffff, x, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&out[v], x);
   }
 }
 
@@ -205,6 +240,74 @@ __global__ void k_norms(const T *__restrict__ divF, const T *__restrict__ mets, 
   }
 }
 
+// FP64 volume integrals of report_turbulent_stats (src/solver.cpp:7813-7917):
+// out[0] = sum |J| w 1/2 rho |u|^2, out[1] = sum |J| w 1/2 rho |curl u|^2 (when
+// the physical gradient is given), out[2] = sum |J| w (volume)
+template <typename T>
+__global__ void k_functionals(const T *__restrict__ U, const T *__restrict__ dU, const T *__restrict__ mets,
+                              const double *__restrict__ w, const double *__restrict__ ref, int64_t neles, int S,
+                              int D, double *out)
+{
+  const int V = D + 2, NM = D * D + 1;
+  double ke = 0.0, en = 0.0, vol = 0.0;
+  const int64_t n = neles * S;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int64_t e = i % neles;
+    const int s = (int)(i / neles);
+    const int64_t t = e / TW;
+    const int l = (int)(e % TW);
+    double u[5];
+    for (int v = 0; v < V; v++)
+      u[v] = (double)U[((t * S + s) * V + v) * TW + l] + (ref ? ref[v] : 0.0);
+    const double jw = (double)mets[((t * S + s) * NM + D * D) * TW + l] * w[s];
+    const double rho = u[0];
+    double vel[3] = {0, 0, 0}, q2 = 0.0;
+    for (int d = 0; d < D; d++)
+    {
+      vel[d] = u[d + 1] / rho;
+      q2 += vel[d] * vel[d];
+    }
+    ke += jw * 0.5 * rho * q2;
+    vol += jw;
+    if (dU)
+    {
+      double g[3][3] = {{0}};  // g[i][j] = d u_i / d x_j
+      for (int i2 = 0; i2 < D; i2++)
+        for (int j = 0; j < D; j++)
+        {
+          const double dm = (double)dU[(((t * D + j) * S + s) * V + i2 + 1) * TW + l];
+          const double dr = (double)dU[(((t * D + j) * S + s) * V + 0) * TW + l];
+          g[i2][j] = (dm - dr * vel[i2]) / rho;
+        }
+      double w2;
+      if (D == 3)
+      {
+        const double wx = g[2][1] - g[1][2], wy = g[0][2] - g[2][0], wz = g[1][0] - g[0][1];
+        w2 = wx * wx + wy * wy + wz * wz;
+      }
+      else
+      {
+        const double wz = g[1][0] - g[0][1];
+        w2 = wz * wz;
+      }
+      en += jw * 0.5 * rho * w2;
+    }
+  }
+  for (int o = 16; o > 0; o /= 2)
+  {
+    ke += __shfl_down_sync(0xffffffff, ke, o);
+    en += __shfl_down_sync(0xffffffff, en, o);
+    vol += __shfl_down_sync(0xffffffff, vol, o);
+  }
+  if ((threadIdx.x & 31) == 0)
+  {
+    atomicAdd(&out[0], ke);
+    atomicAdd(&out[1], en);
+    atomicAdd(&out[2], vol);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
@@ -225,9 +328,24 @@ static LineOpsT<T, N> line_ops(const Plan &p)
 }
 
 template <typename T>
-static dev::Phys<T> phys_of(const zb_params &p)
+static dev::Phys<T> phys_of(const zb_params &p, const double *uref, int ndims, bool deviations)
 {
   dev::Phys<T> ph;
+  std::memset(&ph, 0, sizeof(ph));
+  ph.dev = deviations ? 1 : 0;
+  // perturbation-form constants of the reference state (FP64, then rounded)
+  const int V = ndims + 2;
+  double m2 = 0.0;
+  for (int d = 0; d < ndims; d++) m2 += uref[d + 1] * uref[d + 1];
+  for (int v = 0; v < V; v++) ph.Ur[v] = (T)uref[v];
+  if (uref[0] != 0.0)
+  {
+    const double Pr = (p.gamma - 1.0) * (uref[V - 1] - 0.5 * m2 / uref[0]);
+    ph.Pr = (T)Pr;
+    ph.er = (T)(uref[V - 1] + Pr);
+    ph.inv_rr = (T)(1.0 / uref[0]);
+    ph.mr2 = (T)m2;
+  }
   ph.gamma = (T)p.gamma;
   ph.prandtl = (T)p.prandtl;
   ph.mu = (T)p.mu;
@@ -258,14 +376,18 @@ static int grid_for(int64_t work, int threads)
   return (int)b;
 }
 
-template <typename T, int D, int N>
+template <typename T, typename A, int D, int N>
 static void launch_extrap_impl(Ctx &c)
 {
   using G = Shape<D, N>;
   const int64_t work = c.ntiles * G::Fp * TW;
   ProfScope ps(c, ZB_K_EXTRAP);
-  dev::k_extrap<T, D, N><<<grid_for(work, 256), 256, 0, c.stream>>>((const T *)c.U, (T *)c.Ufp[c.cur], c.ntiles,
-                                                                      line_ops<T, N>(c.plan));
+  if constexpr (D == 3)
+    dev::k_hex_extrap<T, A, N><<<(unsigned)c.ntiles, TW * N * N, 0, c.stream>>>((const T *)c.U, (T *)c.Ufp[c.cur],
+                                                                                c.ntiles, line_ops<A, N>(c.plan));
+  else
+    dev::k_extrap<T, A, D, N><<<grid_for(work, 256), 256, 0, c.stream>>>((const T *)c.U, (T *)c.Ufp[c.cur],
+                                                                           c.ntiles, line_ops<A, N>(c.plan));
   c.launches++;
   CK(cudaGetLastError());
 }
@@ -276,12 +398,12 @@ static void set_smem(K kernel, size_t bytes)
   CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
-template <typename T, int D, int N>
+template <typename T, typename A, int D, int N>
 static void launch_stage_impl(Ctx &c, const StageCfg &sc)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, NT = G::NT;
-  Args<T> a;
+  Args<T, A> a;
   std::memset(&a, 0, sizeof(a));
   a.U = (const T *)c.U;
   a.Ufp = (const T *)c.Ufp[c.cur];
@@ -290,7 +412,7 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
   a.fgeo = (const T *)c.fgeo;
   a.nbr = c.nbr;
   a.divF = (T *)c.divF[sc.stage];
-  a.divF_vol = (T *)c.divF_vol;
+  a.divF_vol = (A *)c.divF_vol;
   a.Fvn = (T *)c.Fvn;
   a.rk_mode = sc.rk_mode;
   a.save_ini = sc.save_ini;
@@ -298,62 +420,98 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
   a.Uout = (T *)c.U;
   a.U_ini = (T *)c.U_ini;
   a.Ucomp = nullptr;
-  a.dt = (T)c.dt;
+  a.dt = (A)c.dt;
   a.ntiles = c.ntiles;
-  a.ph = phys_of<T>(c.plan.params);
+  a.dU_out = sc.want_dU ? (T *)c.dU : nullptr;
+  a.ph = phys_of<A>(c.plan.params, c.uref, c.D, sizeof(T) < sizeof(double));
   if (sc.rk_mode == 1)
-    a.rk_coef[0] = (T)kRkAlpha[sc.stage];
+    a.rk_coef[0] = (A)kRkAlpha[sc.stage];
   else if (sc.rk_mode == 2)
   {
     a.nprev = (int)sc.stage;
-    for (unsigned s = 0; s <= sc.stage; s++) a.rk_coef[s] = (T)kRkBeta[s];
+    for (unsigned s = 0; s <= sc.stage; s++) a.rk_coef[s] = (A)kRkBeta[s];
     for (unsigned s = 0; s < sc.stage; s++) a.divF_prev[s] = (const T *)c.divF[s];
-    if (c.prec == ZB_MIXED) a.Ucomp = (T *)c.Ucomp;
+    if (c.Ucomp) a.Ucomp = (T *)c.Ucomp;
   }
-  const LineOpsT<T, N> ops = line_ops<T, N>(c.plan);
-  const size_t ops_bytes = sizeof(LineOpsT<T, N>);
+  const LineOpsT<A, N> ops = line_ops<A, N>(c.plan);
+  const size_t ops_bytes = sizeof(LineOpsT<A, N>);
+  if constexpr (D == 3)
+  {
+    // hexahedra: column-mapped kernels, TW x N^2 threads per tile
+    constexpr int HT = TW * N * N;
+    if (!c.plan.params.viscous)
+    {
+      const size_t smem = (size_t)(S * V + 3 * S * V + Fp * V) * TW * sizeof(A);
+      set_smem(dev::k_hex_euler<T, A, N>, smem);
+      ProfScope ps(c, ZB_K_EULER);
+      dev::k_hex_euler<T, A, N><<<(unsigned)c.ntiles, HT, smem, c.stream>>>(a, ops);
+      c.launches++;
+      CK(cudaGetLastError());
+    }
+    else
+    {
+      const size_t smem1 = (size_t)(S * V + Fp * V + 3 * S * V) * TW * sizeof(A);
+      set_smem(dev::k_hex_ns_grad<T, A, N>, smem1);
+      {
+        ProfScope ps(c, ZB_K_NS_GRAD);
+        dev::k_hex_ns_grad<T, A, N><<<(unsigned)c.ntiles, HT, smem1, c.stream>>>(a, ops);
+        c.launches++;
+        CK(cudaGetLastError());
+      }
+      if (sc.grad_only) return;
+      const size_t smem2 = (size_t)(Fp * V + S * V) * TW * sizeof(A);
+      set_smem(dev::k_hex_ns_face<T, A, N>, smem2);
+      ProfScope ps(c, ZB_K_NS_FACE);
+      dev::k_hex_ns_face<T, A, N><<<(unsigned)c.ntiles, HT, smem2, c.stream>>>(a, ops);
+      c.launches++;
+      CK(cudaGetLastError());
+    }
+    if (sc.extrap_next) c.cur ^= 1;
+    return;
+  }
   if (!c.plan.params.viscous)
   {
-    const size_t smem = (size_t)(S * V + D * S * V + Fp * V) * TW * sizeof(T) + ops_bytes;
-    set_smem(dev::k_euler<T, D, N>, smem);
+    const size_t smem = (size_t)(S * V + D * S * V + Fp * V) * TW * sizeof(A) + ops_bytes;
+    set_smem(dev::k_euler<T, A, D, N>, smem);
     ProfScope ps(c, ZB_K_EULER);
-    dev::k_euler<T, D, N><<<(unsigned)c.ntiles, NT, smem, c.stream>>>(a, ops);
+    dev::k_euler<T, A, D, N><<<(unsigned)c.ntiles, NT, smem, c.stream>>>(a, ops);
     c.launches++;
     CK(cudaGetLastError());
   }
   else
   {
-    const size_t smem1 = (size_t)(S * V + Fp * V + D * S * V) * TW * sizeof(T) + ops_bytes;
-    set_smem(dev::k_ns_grad<T, D, N>, smem1);
+    const size_t smem1 = (size_t)(S * V + Fp * V + D * S * V) * TW * sizeof(A) + ops_bytes;
+    set_smem(dev::k_ns_grad<T, A, D, N>, smem1);
     {
       ProfScope ps(c, ZB_K_NS_GRAD);
-      dev::k_ns_grad<T, D, N><<<(unsigned)c.ntiles, NT, smem1, c.stream>>>(a, ops);
+      dev::k_ns_grad<T, A, D, N><<<(unsigned)c.ntiles, NT, smem1, c.stream>>>(a, ops);
       c.launches++;
       CK(cudaGetLastError());
     }
-    const size_t smem2 = (size_t)(Fp * V + S * V) * TW * sizeof(T) + ops_bytes;
-    set_smem(dev::k_ns_face<T, D, N>, smem2);
+    if (sc.grad_only) return;
+    const size_t smem2 = (size_t)(Fp * V + S * V) * TW * sizeof(A) + ops_bytes;
+    set_smem(dev::k_ns_face<T, A, D, N>, smem2);
     ProfScope ps(c, ZB_K_NS_FACE);
-    dev::k_ns_face<T, D, N><<<(unsigned)c.ntiles, NT, smem2, c.stream>>>(a, ops);
+    dev::k_ns_face<T, A, D, N><<<(unsigned)c.ntiles, NT, smem2, c.stream>>>(a, ops);
     c.launches++;
     CK(cudaGetLastError());
   }
   if (sc.extrap_next) c.cur ^= 1;
 }
 
-template <typename T, int D, int N>
+template <typename T, typename A, int D, int N>
 static void bind(Ctx &c)
 {
-  c.launch_extrap = &launch_extrap_impl<T, D, N>;
-  c.launch_stage = &launch_stage_impl<T, D, N>;
+  c.launch_extrap = &launch_extrap_impl<T, A, D, N>;
+  c.launch_stage = &launch_stage_impl<T, A, D, N>;
 }
 
-template <typename T>
+template <typename T, typename A>
 static void bind_t(Ctx &c)
 {
   const int D = c.D, N = c.N;
 #define ZB_BIND(DD, NN) \
-  if (D == DD && N == NN) { bind<T, DD, NN>(c); return; }
+  if (D == DD && N == NN) { bind<T, A, DD, NN>(c); return; }
   ZB_BIND(2, 2) ZB_BIND(2, 3) ZB_BIND(2, 4) ZB_BIND(2, 5) ZB_BIND(2, 6)
   ZB_BIND(3, 2) ZB_BIND(3, 3) ZB_BIND(3, 4) ZB_BIND(3, 5)
 #undef ZB_BIND
@@ -379,7 +537,8 @@ static void *dalloc(size_t bytes)
 static void free_all(Ctx *c)
 {
   void *bufs[] = {c->U, c->U_ini, c->divF[0], c->divF[1], c->divF[2], c->divF[3], c->divF_vol, c->Ufp[0],
-                  c->Ufp[1], c->Fvn, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred};
+                  c->Ufp[1], c->Fvn, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
+                  c->dU, c->dweights, c->dfun};
   for (void *b : bufs)
     if (b) cudaFree(b);
   for (auto &r : c->recs)
@@ -457,6 +616,7 @@ Ctx *ctx_create(const Plan &plan)
   c->prec = plan.params.precision;
   if (c->prec != ZB_FP64 && c->prec != ZB_MIXED) ZB_THROW(ZB_ERR_ARG, "unknown precision");
   c->tsz = (c->prec == ZB_FP64) ? sizeof(double) : sizeof(float);
+  c->asz = c->tsz;
   c->D = plan.ndims;
   c->N = plan.N;
   c->S = plan.nspts;
@@ -466,9 +626,9 @@ Ctx *ctx_create(const Plan &plan)
   c->dt = plan.params.dt;
   if (plan.tile != TW) ZB_THROW(ZB_ERR_INTERNAL, "plan tile width does not match kernels");
   if (c->prec == ZB_FP64)
-    bind_t<double>(*c);
+    bind_t<double, double>(*c);
   else
-    bind_t<float>(*c);
+    bind_t<float, float>(*c);
   try
   {
     const size_t nU = (size_t)c->ntiles * c->S * c->V * TW;
@@ -480,14 +640,16 @@ Ctx *ctx_create(const Plan &plan)
     c->Ufp[1] = dalloc(nF * c->tsz);
     if (plan.params.viscous)
     {
-      c->divF_vol = dalloc(nU * c->tsz);
+      c->divF_vol = dalloc(nU * c->asz);
       c->Fvn = dalloc(nF * c->tsz);
     }
-    if (c->prec == ZB_MIXED) c->Ucomp = dalloc(nU * c->tsz);
+    if (c->prec != ZB_FP64) c->Ucomp = dalloc(nU * c->tsz);
     c->mets = dalloc((size_t)c->ntiles * c->S * (c->D * c->D + 1) * TW * c->tsz);
     c->fgeo = dalloc((size_t)c->ntiles * c->Fp * (c->D + 1) * TW * c->tsz);
     c->nbr = (int *)dalloc((size_t)c->ntiles * c->Fp * TW * sizeof(int));
     c->dred = (double *)dalloc(3 * 8 * sizeof(double));
+    c->dref = (double *)dalloc(8 * sizeof(double));
+    CK(cudaMemsetAsync(c->dref, 0, 8 * sizeof(double), c->stream));
     if (c->prec == ZB_FP64)
       upload_static<double>(*c);
     else
@@ -570,21 +732,42 @@ void ctx_set_state(Ctx *c, const double *U, int64_t ss, int64_t vs, int64_t es, 
   const size_t ext = extent(c, ss, vs, es, c->S);
   const double *src = stage_in(c, U, ext, where);
   const int64_t work = c->ntiles * c->S * c->V * TW;
-  ProfScope ps(*c, ZB_K_TO_TILES);
-  if (c->prec == ZB_FP64)
-    k_to_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>(src, (double *)c->U, nullptr, c->plan.neles,
-                                                                     c->ntiles, c->S, c->V, ss, vs, es);
-  else
-    k_to_tiles<float><<<grid_for(work, 256), 256, 0, c->stream>>>(src, (float *)c->U, (float *)c->Ucomp,
-                                                                    c->plan.neles, c->ntiles, c->S, c->V, ss, vs, es);
-  c->launches++;
-  CK(cudaGetLastError());
+  if (c->prec != ZB_FP64)
+  {
+    // reference state of the perturbation form: the state's mean per variable
+    // (FP64 reduction), rounded to FP32 so U = Ur + U' holds exactly in FP32
+    CK(cudaMemsetAsync(c->dred, 0, 8 * sizeof(double), c->stream));
+    const int64_t n = c->plan.neles * c->S;
+    k_var_sums<<<grid_for(n, 256), 256, 0, c->stream>>>(src, c->plan.neles, c->S, c->V, ss, vs, es, c->dred);
+    c->launches++;
+    CK(cudaGetLastError());
+    double h[8];
+    CK(cudaMemcpyAsync(h, c->dred, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < c->V; v++)
+    {
+      const double mean = h[v] / (double)n;
+      c->uref[v] = std::isfinite(mean) ? (double)(float)mean : 0.0;
+    }
+    CK(cudaMemcpyAsync(c->dref, c->uref, sizeof(c->uref), cudaMemcpyHostToDevice, c->stream));
+  }
+  {
+    ProfScope ps(*c, ZB_K_TO_TILES);
+    if (c->prec == ZB_FP64)
+      k_to_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>(src, (double *)c->U, nullptr, nullptr,
+                                                                       c->plan.neles, c->ntiles, c->S, c->V, ss, vs, es);
+    else
+      k_to_tiles<float><<<grid_for(work, 256), 256, 0, c->stream>>>(src, (float *)c->U, (float *)c->Ucomp, c->dref,
+                                                                      c->plan.neles, c->ntiles, c->S, c->V, ss, vs, es);
+    c->launches++;
+    CK(cudaGetLastError());
+  }
   if (where == ZB_HOST) CK(cudaStreamSynchronize(c->stream));
   c->ufp_valid = false;
 }
 
-static void from_tiles(Ctx *c, const void *srcT, const void *comp, double *out, int64_t ss, int64_t vs, int64_t es,
-                       int where)
+static void from_tiles(Ctx *c, const void *srcT, const void *comp, const double *ref, double *out, int64_t ss,
+                       int64_t vs, int64_t es, int where)
 {
   const size_t ext = extent(c, ss, vs, es, c->S);
   double *dst = out;
@@ -608,11 +791,11 @@ static void from_tiles(Ctx *c, const void *srcT, const void *comp, double *out, 
   {
   ProfScope ps(*c, ZB_K_FROM_TILES);
   if (c->prec == ZB_FP64)
-    k_from_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>((const double *)srcT, (const double *)comp, dst,
-                                                                       c->plan.neles, c->S, c->V, ss, vs, es);
+    k_from_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>((const double *)srcT, (const double *)comp, ref,
+                                                                       dst, c->plan.neles, c->S, c->V, ss, vs, es);
   else
-    k_from_tiles<float><<<grid_for(work, 256), 256, 0, c->stream>>>((const float *)srcT, (const float *)comp, dst,
-                                                                      c->plan.neles, c->S, c->V, ss, vs, es);
+    k_from_tiles<float><<<grid_for(work, 256), 256, 0, c->stream>>>((const float *)srcT, (const float *)comp, ref,
+                                                                      dst, c->plan.neles, c->S, c->V, ss, vs, es);
   c->launches++;
   CK(cudaGetLastError());
   }
@@ -626,7 +809,7 @@ static void from_tiles(Ctx *c, const void *srcT, const void *comp, double *out, 
 void ctx_get_state(Ctx *c, double *U, int64_t ss, int64_t vs, int64_t es, int where)
 {
   if (!U) ZB_THROW(ZB_ERR_ARG, "null state");
-  from_tiles(c, c->U, c->Ucomp, U, ss, vs, es, where);
+  from_tiles(c, c->U, c->Ucomp, c->prec != ZB_FP64 ? c->dref : nullptr, U, ss, vs, es, where);
 }
 
 static void ensure_ufp(Ctx *c)
@@ -652,7 +835,7 @@ void ctx_get_residual(Ctx *c, unsigned stage, double *out, int64_t ss, int64_t v
 {
   if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
   if (!out) ZB_THROW(ZB_ERR_ARG, "null output");
-  from_tiles(c, c->divF[stage], nullptr, out, ss, vs, es, where);
+  from_tiles(c, c->divF[stage], nullptr, nullptr, out, ss, vs, es, where);
 }
 
 void ctx_rk_stage(Ctx *c, unsigned stage)
@@ -709,6 +892,49 @@ void ctx_norms(Ctx *c, double *out)
 void ctx_sync(Ctx *c) { CK(cudaStreamSynchronize(c->stream)); }
 
 int64_t ctx_launches(const Ctx *c) { return c->launches; }
+
+void ctx_functionals(Ctx *c, double *out)
+{
+  const size_t nU = (size_t)c->ntiles * c->S * c->V * TW;
+  if (!c->dweights)
+  {
+    c->dweights = (double *)dalloc(c->S * sizeof(double));
+    c->dfun = (double *)dalloc(4 * sizeof(double));
+    CK(cudaMemcpyAsync(c->dweights, c->plan.weights_spts.data(), c->S * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+  }
+  const bool grad = c->plan.params.viscous != 0;
+  if (grad)
+  {
+    if (!c->dU) c->dU = dalloc(nU * c->D * c->tsz);
+    // gradient of the current state: extrapolation + the gradient kernel only
+    c->ufp_valid = false;
+    ensure_ufp(c);
+    StageCfg sc{0, 0, 0, 0};
+    sc.want_dU = 1;
+    sc.grad_only = 1;
+    c->launch_stage(*c, sc);
+  }
+  CK(cudaMemsetAsync(c->dfun, 0, 4 * sizeof(double), c->stream));
+  const int64_t n = c->plan.neles * c->S;
+  const double *ref = c->prec == ZB_FP64 ? nullptr : c->dref;
+  if (c->prec == ZB_FP64)
+    k_functionals<double><<<grid_for(n, 256), 256, 0, c->stream>>>(
+        (const double *)c->U, grad ? (const double *)c->dU : nullptr, (const double *)c->mets, c->dweights, ref,
+        c->plan.neles, c->S, c->D, c->dfun);
+  else
+    k_functionals<float><<<grid_for(n, 256), 256, 0, c->stream>>>(
+        (const float *)c->U, grad ? (const float *)c->dU : nullptr, (const float *)c->mets, c->dweights, ref,
+        c->plan.neles, c->S, c->D, c->dfun);
+  c->launches++;
+  CK(cudaGetLastError());
+  double h[4];
+  CK(cudaMemcpyAsync(h, c->dfun, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  out[0] = h[0];
+  out[1] = grad ? h[1] : 0.0;
+  out[2] = h[2];
+}
 
 void ctx_profile_enable(Ctx *c, int on)
 {

@@ -31,6 +31,7 @@ void ctx_norms(Ctx *c, double *out);
 void ctx_sync(Ctx *c);
 int64_t ctx_launches(const Ctx *c);
 void ctx_profile_enable(Ctx *c, int on);
+void ctx_functionals(Ctx *c, double *out);
 void ctx_profile_read(Ctx *c, double *ms, int64_t *count);
 void noalloc_residual(const Plan &p, const double *U, double *divF, cudaStream_t st);
 

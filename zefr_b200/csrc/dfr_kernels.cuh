@@ -42,7 +42,8 @@ struct LineOpsT
   T Em[N], Ep[N], Dbm[N], Dbp[N];
 };
 
-template <typename T>
+// T: storage type of state, traces and metrics; A: arithmetic type.
+template <typename T, typename A>
 struct Args
 {
   const T *U;        // [tile][S][V][TW]
@@ -52,8 +53,11 @@ struct Args
   const T *fgeo;     // [tile][Fp][D+1][TW]: face unit normal (left side), own dA
   const int *nbr;    // [tile][Fp][TW]: 2*partner+slot, or -1-bc
   T *divF;           // [tile][S][V][TW] residual of this stage
-  T *divF_vol;       // NS: volume part of the residual
+  A *divF_vol;       // NS: volume part of the residual (arithmetic type: it cancels
+                     // against the surface part)
   T *Fvn;            // NS: viscous normal flux at own flux points
+  T *dU_out;         // NS, optional: physical gradient [tile][D][S][V][TW] (the
+                     // reference keeps it in dU_spts for diagnostics)
   // RK update fused into the last kernel of a stage
   int rk_mode;       // 0: none; 1: U = U_ini - a dt/|J| divF; 2: final combination
   int save_ini;      // stage 0: write U_ini = U before updating
@@ -63,10 +67,10 @@ struct Args
   T *U_ini;          // RK start state
   T *Ucomp;          // compensated-summation remainder (final stage, nullptr = off)
   const T *divF_prev[6];
-  T rk_coef[6];      // a_s (mode 1: [0]) or b_s (mode 2)
-  T dt;
+  A rk_coef[6];      // a_s (mode 1: [0]) or b_s (mode 2)
+  A dt;
   int64_t ntiles;
-  Phys<T> ph;
+  Phys<A> ph;
 };
 
 // Flux point f -> normal dimension, side (-1/+1), first spt of its line and
@@ -144,51 +148,51 @@ __device__ __forceinline__ void face_dim_side(int face, int &dim, int &side)
   }
 }
 
-template <typename T, int N>
-__device__ __forceinline__ void load_ops(T *sops, const LineOpsT<T, N> &ops)
+template <typename A, int N>
+__device__ __forceinline__ void load_ops(A *sops, const LineOpsT<A, N> &ops)
 {
-  const T *src = reinterpret_cast<const T *>(&ops);
+  const A *src = reinterpret_cast<const A *>(&ops);
   constexpr int n = N * N + 4 * N;
   for (int i = threadIdx.x; i < n; i += blockDim.x) sops[i] = src[i];
 }
 
 // Shared-memory views of the line operators
-template <typename T, int N>
+template <typename A, int N>
 struct SOps
 {
-  const T *Dm, *Em, *Ep, *Dbm, *Dbp;
-  __device__ SOps(const T *p) : Dm(p), Em(p + N * N), Ep(p + N * N + N), Dbm(p + N * N + 2 * N), Dbp(p + N * N + 3 * N) {}
+  const A *Dm, *Em, *Ep, *Dbm, *Dbp;
+  __device__ SOps(const A *p) : Dm(p), Em(p + N * N), Ep(p + N * N + N), Dbm(p + N * N + 2 * N), Dbp(p + N * N + 3 * N) {}
 };
 
 // extrapolate component v of the tile state in smem (layout [S][V][TW]) to flux point f
-template <typename T, int D, int N>
-__device__ __forceinline__ T extrap_smem(const T *sX, const SOps<T, N> &o, int f, int v, int l, int nv)
+template <typename A, int D, int N>
+__device__ __forceinline__ A extrap_smem(const A *sX, const SOps<A, N> &o, int f, int v, int l, int nv)
 {
   int dim, side, base, stride;
   fpt_line<D, N>(f, dim, side, base, stride);
-  const T *E = side < 0 ? o.Em : o.Ep;
-  T acc = E[0] * sX[((base)*nv + v) * TW + l];
+  const A *E = side < 0 ? o.Em : o.Ep;
+  A acc = E[0] * sX[((base)*nv + v) * TW + l];
 #pragma unroll
   for (int m = 1; m < N; m++) acc += E[m] * sX[((base + m * stride) * nv + v) * TW + l];
   return acc;
 }
 
 // read the neighbour's copy of a [tile][Fp][V][TW] array
-template <typename T, int V>
-__device__ __forceinline__ void gather_fpt(const T *A, int pidx, T out[V])
+template <typename T, typename A, int V>
+__device__ __forceinline__ void gather_fpt(const T *src, int pidx, A out[V])
 {
   const int64_t row = (int64_t)(pidx / TW) * V;
   const int lane = pidx % TW;
 #pragma unroll
-  for (int v = 0; v < V; v++) out[v] = A[(row + v) * TW + lane];
+  for (int v = 0; v < V; v++) out[v] = (A)src[(row + v) * TW + lane];
 }
 
 // ---------------------------------------------------------------------------
 // Extrapolate the state to flux points: U_fpts = oppE U_spts (src/elements.cpp:1337-1360)
 // ---------------------------------------------------------------------------
-template <typename T, int D, int N>
+template <typename T, typename A, int D, int N>
 __global__ void __launch_bounds__(256) k_extrap(const T *__restrict__ U, T *__restrict__ Ufp, int64_t ntiles,
-                                                LineOpsT<T, N> ops)
+                                                const __grid_constant__ LineOpsT<A, N> ops)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V;
@@ -205,10 +209,11 @@ __global__ void __launch_bounds__(256) k_extrap(const T *__restrict__ U, T *__re
 #pragma unroll
     for (int v = 0; v < V; v++)
     {
-      T acc = (side < 0 ? ops.Em[0] : ops.Ep[0]) * Ut[((base)*V + v) * TW + l];
+      A acc = (side < 0 ? ops.Em[0] : ops.Ep[0]) * (A)Ut[((base)*V + v) * TW + l];
 #pragma unroll
-      for (int m = 1; m < N; m++) acc += (side < 0 ? ops.Em[m] : ops.Ep[m]) * Ut[((base + m * stride) * V + v) * TW + l];
-      out[v * TW + l] = acc;
+      for (int m = 1; m < N; m++)
+        acc += (side < 0 ? ops.Em[m] : ops.Ep[m]) * (A)Ut[((base + m * stride) * V + v) * TW + l];
+      out[v * TW + l] = (T)acc;
     }
   }
 }
@@ -219,9 +224,9 @@ __global__ void __launch_bounds__(256) k_extrap(const T *__restrict__ U, T *__re
 // (src/faces.cpp:1243-1364, 1616-1640).  For viscous runs the LDG part is
 // added by the caller.
 // ---------------------------------------------------------------------------
-template <typename T, int D>
-__device__ __forceinline__ void conv_common(const Args<T> &a, const T Uo[D + 2], const T Un[D + 2], int code,
-                                            const T n[D], T UL[D + 2], T UR[D + 2], T UB[D + 2], T F[D + 2])
+template <typename T, typename A, int D>
+__device__ __forceinline__ void conv_common(const Args<T, A> &a, const A Uo[D + 2], const A Un[D + 2], int code,
+                                            const A n[D], A UL[D + 2], A UR[D + 2], A UB[D + 2], A F[D + 2])
 {
   if (code >= 0)
   {
@@ -236,29 +241,33 @@ __device__ __forceinline__ void conv_common(const Args<T> &a, const T Uo[D + 2],
   }
   else
   {
+    A Ua[D + 2], URa[D + 2], UBa[D + 2];
 #pragma unroll
     for (int v = 0; v < D + 2; v++) UL[v] = Uo[v];
-    ghost_state<T, D>(-code - 1, UL, n, UR, UB, a.ph);
+    to_abs<A, D>(Uo, Ua, a.ph);
+    ghost_state<A, D>(-code - 1, Ua, n, URa, UBa, a.ph);
+    to_stored<A, D>(URa, UR, a.ph);
+    to_stored<A, D>(UBa, UB, a.ph);
   }
   if (a.ph.fconv == 2)
-    roe<T, D>(UL, UR, n, F, a.ph);
+    roe<A, D>(UL, UR, n, F, a.ph);
   else
-    rusanov<T, D>(UL, UR, n, F, a.ph);
+    rusanov<A, D>(UL, UR, n, F, a.ph);
 }
 
 // ---------------------------------------------------------------------------
 // Final per-point residual: volume part + surface correction, then optional
 // RK update (src/solver.cpp:2916-2937, 3040-3094).
 // ---------------------------------------------------------------------------
-template <typename T, int D, int N>
-__device__ __forceinline__ void finish_point(const Args<T> &a, int64_t tile, int s, int l, const T vol[D + 2],
-                                             const T *sFc, const SOps<T, N> &o, T *sUnew)
+template <typename T, typename A, int D, int N>
+__device__ __forceinline__ void finish_point(const Args<T, A> &a, int64_t tile, int s, int l, const A vol[D + 2],
+                                             const A *sFc, const SOps<A, N> &o, A *sUnew)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, V = G::V, NM = G::NM;
-  T surf[V];
+  A surf[V];
 #pragma unroll
-  for (int v = 0; v < V; v++) surf[v] = T(0);
+  for (int v = 0; v < V; v++) surf[v] = A(0);
   // surface terms in ascending flux point order = ascending face order
 #pragma unroll
   for (int face = 0; face < 2 * D; face++)
@@ -268,12 +277,12 @@ __device__ __forceinline__ void finish_point(const Args<T> &a, int64_t tile, int
     int i, fm, fp;
     spt_ends<D, N>(s, dim, i, fm, fp);
     const int f = side < 0 ? fm : fp;
-    const T c = side < 0 ? -o.Dbm[i] : o.Dbp[i];
+    const A c = side < 0 ? -o.Dbm[i] : o.Dbp[i];
 #pragma unroll
     for (int v = 0; v < V; v++) surf[v] += c * sFc[(f * V + v) * TW + l];
   }
   const int64_t base = (tile * S + s) * (int64_t)V * TW;
-  T res[V];
+  A res[V];
 #pragma unroll
   for (int v = 0; v < V; v++)
   {
@@ -281,12 +290,12 @@ __device__ __forceinline__ void finish_point(const Args<T> &a, int64_t tile, int
     a.divF[base + v * TW + l] = res[v];
   }
   if (a.rk_mode == 0) return;
-  const T detJ = a.mets[((tile * S + s) * NM + D * D) * TW + l];
+  const A detJ = a.mets[((tile * S + s) * NM + D * D) * TW + l];
 #pragma unroll
   for (int v = 0; v < V; v++)
   {
     const int64_t idx = base + v * TW + l;
-    T u_ini;
+    A u_ini;
     if (a.save_ini)
     {
       u_ini = a.U[idx];
@@ -294,22 +303,22 @@ __device__ __forceinline__ void finish_point(const Args<T> &a, int64_t tile, int
     }
     else
       u_ini = a.U_ini[idx];
-    T unew;
+    A unew;
     if (a.rk_mode == 1)
       unew = u_ini - a.rk_coef[0] * a.dt / detJ * res[v];
     else
     {
-      T delta = T(0);
-      // sum of stage increments in stage order
-      for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * a.dt / detJ * a.divF_prev[st][idx];
-      delta -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
       if (a.Ucomp)
       {
-        // Kahan-compensated accumulation of the step increment
-        const T c = a.Ucomp[idx];
-        const T y = delta - c;
-        unew = u_ini + y;
-        a.Ucomp[idx] = (unew - u_ini) - y;
+        // Kahan-compensated accumulation of the step increment; the
+        // remainder includes the rounding of the stored state
+        A delta = A(0);
+        for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * a.dt / detJ * (A)a.divF_prev[st][idx];
+        delta -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
+        const A c = a.Ucomp[idx];
+        const A y = delta - c;
+        unew = (A)(T)(u_ini + y);
+        a.Ucomp[idx] = (T)((unew - u_ini) - y);
       }
       else
       {
@@ -320,12 +329,12 @@ __device__ __forceinline__ void finish_point(const Args<T> &a, int64_t tile, int
       }
     }
     a.Uout[idx] = unew;
-    if (sUnew) sUnew[(s * V + v) * TW + l] = unew;
+    if (sUnew) sUnew[(s * V + v) * TW + l] = (A)(T)unew;  // the state as stored
   }
 }
 
-template <typename T, int D, int N>
-__device__ __forceinline__ void extrap_next_tile(const Args<T> &a, int64_t tile, const T *sUnew, const SOps<T, N> &o)
+template <typename T, typename A, int D, int N>
+__device__ __forceinline__ void extrap_next_tile(const Args<T, A> &a, int64_t tile, const A *sUnew, const SOps<A, N> &o)
 {
   using G = Shape<D, N>;
   constexpr int Fp = G::Fp, V = G::V;
@@ -334,24 +343,25 @@ __device__ __forceinline__ void extrap_next_tile(const Args<T> &a, int64_t tile,
     const int f = it / TW, l = it % TW;
     T *out = a.Ufp_next + (tile * Fp + f) * (int64_t)V * TW;
 #pragma unroll
-    for (int v = 0; v < V; v++) out[v * TW + l] = extrap_smem<T, D, N>(sUnew, o, f, v, l, V);
+    for (int v = 0; v < V; v++) out[v * TW + l] = extrap_smem<A, D, N>(sUnew, o, f, v, l, V);
   }
 }
 
 // ---------------------------------------------------------------------------
 // Euler: volume flux, common flux and divergence of one tile in one kernel.
 // ---------------------------------------------------------------------------
-template <typename T, int D, int N>
-__global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(Args<T> a, LineOpsT<T, N> ops)
+template <typename T, typename A, int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(const __grid_constant__ Args<T, A> a,
+                                                                   const __grid_constant__ LineOpsT<A, N> ops)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, NM = G::NM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *sU = reinterpret_cast<T *>(smem_raw);
-  T *sF = sU + S * V * TW;
-  T *sFc = sF + D * S * V * TW;
-  T *sops = sFc + Fp * V * TW;
-  load_ops<T, N>(sops, ops);
+  A *sU = reinterpret_cast<A *>(smem_raw);
+  A *sF = sU + S * V * TW;
+  A *sFc = sF + D * S * V * TW;
+  A *sops = sFc + Fp * V * TW;
+  load_ops<A, N>(sops, ops);
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
   {
@@ -359,17 +369,17 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(Args<T> a, LineOpsT<T
     for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
   }
   __syncthreads();
-  SOps<T, N> o(sops);
+  SOps<A, N> o(sops);
   // transformed volume flux F~ = adj F (src/elements.cpp:1588-1699)
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
   {
     const int s = it / TW, l = it % TW;
-    T U[V], F[V][D], P;
+    A U[V], F[V][D], P, Pp;
 #pragma unroll
     for (int v = 0; v < V; v++) U[v] = sU[(s * V + v) * TW + l];
-    flux_conv<T, D>(U, F, P, a.ph.gamma);
+    flux_conv_stored<A, D>(U, F, P, Pp, a.ph);
     const T *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
-    T adj[D][D];
+    A adj[D][D];
 #pragma unroll
     for (int d1 = 0; d1 < D; d1++)
 #pragma unroll
@@ -379,7 +389,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(Args<T> a, LineOpsT<T
 #pragma unroll
       for (int d1 = 0; d1 < D; d1++)
       {
-        T t = F[v][0] * adj[d1][0];
+        A t = F[v][0] * adj[d1][0];
 #pragma unroll
         for (int d2 = 1; d2 < D; d2++) t += F[v][d2] * adj[d1][d2];
         sF[((d1 * S + s) * V + v) * TW + l] = t;
@@ -391,17 +401,17 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(Args<T> a, LineOpsT<T
     const int f = it / TW, l = it % TW;
     const int64_t fi = (tile * Fp + f) * (int64_t)TW + l;
     const int code = a.nbr[fi];
-    T n[D], dA;
+    A n[D], dA;
     const T *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
 #pragma unroll
     for (int d = 0; d < D; d++) n[d] = g[d * TW];
     dA = g[D * TW];
-    T Uo[V], Un[V], UL[V], UR[V], UB[V], Fc[V];
+    A Uo[V], Un[V], UL[V], UR[V], UB[V], Fc[V];
     const T *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
-    if (code >= 0) gather_fpt<T, V>(a.Ufp, code >> 1, Un);
-    conv_common<T, D>(a, Uo, Un, code, n, UL, UR, UB, Fc);
+    if (code >= 0) gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
+    conv_common<T, A, D>(a, Uo, Un, code, n, UL, UR, UB, Fc);
     const bool right = (code >= 0) && (code & 1);
 #pragma unroll
     for (int v = 0; v < V; v++) sFc[(f * V + v) * TW + l] = right ? -Fc[v] * dA : Fc[v] * dA;
@@ -410,9 +420,9 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(Args<T> a, LineOpsT<T
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
   {
     const int s = it / TW, l = it % TW;
-    T vol[V];
+    A vol[V];
 #pragma unroll
-    for (int v = 0; v < V; v++) vol[v] = T(0);
+    for (int v = 0; v < V; v++) vol[v] = A(0);
 #pragma unroll
     for (int d = 0; d < D; d++)
     {
@@ -423,17 +433,17 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(Args<T> a, LineOpsT<T
 #pragma unroll
       for (int m = 0; m < N; m++)
       {
-        const T c = o.Dm[i * N + m];
+        const A c = o.Dm[i * N + m];
 #pragma unroll
         for (int v = 0; v < V; v++) vol[v] += c * sF[((d * S + b + m * st) * V + v) * TW + l];
       }
     }
-    finish_point<T, D, N>(a, tile, s, l, vol, sFc, o, a.extrap_next ? sU : nullptr);
+    finish_point<T, A, D, N>(a, tile, s, l, vol, sFc, o, a.extrap_next ? sU : nullptr);
   }
   if (a.extrap_next)
   {
     __syncthreads();
-    extrap_next_tile<T, D, N>(a, tile, sU, o);
+    extrap_next_tile<T, A, D, N>(a, tile, sU, o);
   }
 }
 
@@ -443,17 +453,18 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(Args<T> a, LineOpsT<T
 // (src/solver.cpp:1540-1600; src/elements.cpp:1393-1447, 1588-1699;
 //  src/faces.cpp:1366-1474, 508-710).
 // ---------------------------------------------------------------------------
-template <typename T, int D, int N>
-__global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(Args<T> a, LineOpsT<T, N> ops)
+template <typename T, typename A, int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(const __grid_constant__ Args<T, A> a,
+                                                                                       const __grid_constant__ LineOpsT<A, N> ops)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, NM = G::NM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *sU = reinterpret_cast<T *>(smem_raw);
-  T *sUC = sU + S * V * TW;
-  T *sdU = sUC + Fp * V * TW;  // [D][S][V][TW]: physical gradient, then F~
-  T *sops = sdU + D * S * V * TW;
-  load_ops<T, N>(sops, ops);
+  A *sU = reinterpret_cast<A *>(smem_raw);
+  A *sUC = sU + S * V * TW;
+  A *sdU = sUC + Fp * V * TW;  // [D][S][V][TW]: physical gradient, then F~
+  A *sops = sdU + D * S * V * TW;
+  load_ops<A, N>(sops, ops);
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
   {
@@ -461,43 +472,45 @@ __global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(A
     for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
   }
   __syncthreads();
-  SOps<T, N> o(sops);
-  const T beta = a.ph.ldg_b;
+  SOps<A, N> o(sops);
+  const A beta = a.ph.ldg_b;
   // common solution at own flux points (LDG, flip_beta = 1)
   for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
   {
     const int f = it / TW, l = it % TW;
     const int64_t fi = (tile * Fp + f) * (int64_t)TW + l;
     const int code = a.nbr[fi];
-    T Uo[V], UC[V];
+    A Uo[V], UC[V];
     const T *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
     if (code >= 0)
     {
-      T Un[V];
-      gather_fpt<T, V>(a.Ufp, code >> 1, Un);
+      A Un[V];
+      gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
       const int slot = code & 1;
 #pragma unroll
       for (int v = 0; v < V; v++)
       {
-        const T ul = slot ? Un[v] : Uo[v];
-        const T ur = slot ? Uo[v] : Un[v];
-        if (beta == T(0.5))
+        const A ul = slot ? Un[v] : Uo[v];
+        const A ur = slot ? Uo[v] : Un[v];
+        if (beta == A(0.5))
           UC[v] = ur;
-        else if (beta == T(-0.5))
+        else if (beta == A(-0.5))
           UC[v] = ul;
         else
-          UC[v] = T(0.5) * (ul + ur) - beta * (ul - ur);
+          UC[v] = A(0.5) * (ul + ur) - beta * (ul - ur);
       }
     }
     else
     {
-      T n[D], UR[V];
+      A n[D], Ua[V], URa[V], UBa[V];
       const T *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
 #pragma unroll
       for (int d = 0; d < D; d++) n[d] = g[d * TW];
-      ghost_state<T, D>(-code - 1, Uo, n, UR, UC, a.ph);
+      to_abs<A, D>(Uo, Ua, a.ph);
+      ghost_state<A, D>(-code - 1, Ua, n, URa, UBa, a.ph);
+      to_stored<A, D>(UBa, UC, a.ph);
     }
 #pragma unroll
     for (int v = 0; v < V; v++) sUC[(f * V + v) * TW + l] = UC[v];
@@ -507,7 +520,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(A
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
   {
     const int s = it / TW, l = it % TW;
-    T tdU[V][D];
+    A tdU[V][D];
 #pragma unroll
     for (int d = 0; d < D; d++)
     {
@@ -518,61 +531,68 @@ __global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(A
 #pragma unroll
       for (int v = 0; v < V; v++)
       {
-        T acc = T(0);
+        A acc = A(0);
 #pragma unroll
         for (int m = 0; m < N; m++) acc += o.Dm[i * N + m] * sU[((b + m * st) * V + v) * TW + l];
-        const T cm = o.Dbm[i] * sUC[(fm * V + v) * TW + l];
-        const T cp = o.Dbp[i] * sUC[(fp * V + v) * TW + l];
+        const A cm = o.Dbm[i] * sUC[(fm * V + v) * TW + l];
+        const A cp = o.Dbp[i] * sUC[(fp * V + v) * TW + l];
         tdU[v][d] = acc + ((fm < fp) ? (cm + cp) : (cp + cm));
       }
     }
     const T *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
-    T adj[D][D];
+    A adj[D][D];
 #pragma unroll
     for (int d1 = 0; d1 < D; d1++)
 #pragma unroll
       for (int d2 = 0; d2 < D; d2++) adj[d1][d2] = m[(d1 * D + d2) * TW];
-    const T inv_det = T(1) / m[D * D * TW];
+    const A inv_det = A(1) / m[D * D * TW];
 #pragma unroll
     for (int v = 0; v < V; v++)
 #pragma unroll
       for (int d1 = 0; d1 < D; d1++)
       {
-        T g = tdU[v][0] * adj[0][d1];
+        A g = tdU[v][0] * adj[0][d1];
 #pragma unroll
         for (int d2 = 1; d2 < D; d2++) g += tdU[v][d2] * adj[d2][d1];
         sdU[((d1 * S + s) * V + v) * TW + l] = g * inv_det;
       }
   }
   __syncthreads();
+  if (a.dU_out)
+  {
+    T *g = a.dU_out + tile * (int64_t)D * S * V * TW;
+    for (int i = threadIdx.x; i < D * S * V * TW; i += blockDim.x) g[i] = (T)sdU[i];
+  }
   // viscous normal flux at own flux points (own side; boundaries: prescribed side)
   for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
   {
     const int f = it / TW, l = it % TW;
     const int64_t fi = (tile * Fp + f) * (int64_t)TW + l;
     const int code = a.nbr[fi];
-    if (code >= 0 && ((beta == T(0.5) && (code & 1)) || (beta == T(-0.5) && !(code & 1)))) continue;
-    T n[D];
+    if (code >= 0 && ((beta == A(0.5) && (code & 1)) || (beta == A(-0.5) && !(code & 1)))) continue;
+    A n[D];
     const T *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
 #pragma unroll
     for (int d = 0; d < D; d++) n[d] = g[d * TW];
-    T Uf[V], dUf[V][D], Fn[V];
+    A Uf[V], dUf[V][D], Fn[V];
     const T *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++)
     {
       Uf[v] = uo[v * TW];
 #pragma unroll
-      for (int d = 0; d < D; d++) dUf[v][d] = extrap_smem<T, D, N>(sdU + d * S * V * TW, o, f, v, l, V);
+      for (int d = 0; d < D; d++) dUf[v][d] = extrap_smem<A, D, N>(sdU + d * S * V * TW, o, f, v, l, V);
     }
+    A Ua[V];
+    to_abs<A, D>(Uf, Ua, a.ph);
     if (code >= 0)
-      visc_normal<T, D>(Uf, dUf, n, Fn, a.ph);
+      visc_normal<A, D>(Ua, dUf, n, Fn, a.ph);
     else
     {
-      T UR[V], UB[V], dUB[V][D];
-      ghost_state<T, D>(-code - 1, Uf, n, UR, UB, a.ph);
-      ghost_grad<T, D>(-code - 1, Uf, dUf, n, dUB);
-      visc_normal<T, D>(UB, dUB, n, Fn, a.ph);
+      A UR[V], UB[V], dUB[V][D];
+      ghost_state<A, D>(-code - 1, Ua, n, UR, UB, a.ph);
+      ghost_grad<A, D>(-code - 1, Ua, dUf, n, dUB);
+      visc_normal<A, D>(UB, dUB, n, Fn, a.ph);
     }
     T *out = a.Fvn + (tile * Fp + f) * (int64_t)V * TW + l;
 #pragma unroll
@@ -583,7 +603,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(A
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
   {
     const int s = it / TW, l = it % TW;
-    T U[V], dU[V][D], F[V][D], P;
+    A U[V], dU[V][D], F[V][D];
 #pragma unroll
     for (int v = 0; v < V; v++)
     {
@@ -591,10 +611,12 @@ __global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(A
 #pragma unroll
       for (int d = 0; d < D; d++) dU[v][d] = sdU[((d * S + s) * V + v) * TW + l];
     }
-    flux_conv<T, D>(U, F, P, a.ph.gamma);
-    flux_visc_add<T, D>(U, dU, F, a.ph);
+    A P, Pp, Ua[V];
+    flux_conv_stored<A, D>(U, F, P, Pp, a.ph);
+    to_abs<A, D>(U, Ua, a.ph);
+    flux_visc_add<A, D>(Ua, dU, F, a.ph);
     const T *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
-    T adj[D][D];
+    A adj[D][D];
 #pragma unroll
     for (int d1 = 0; d1 < D; d1++)
 #pragma unroll
@@ -604,7 +626,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(A
 #pragma unroll
       for (int d1 = 0; d1 < D; d1++)
       {
-        T t = F[v][0] * adj[d1][0];
+        A t = F[v][0] * adj[d1][0];
 #pragma unroll
         for (int d2 = 1; d2 < D; d2++) t += F[v][d2] * adj[d1][d2];
         sdU[((d1 * S + s) * V + v) * TW + l] = t;
@@ -615,9 +637,9 @@ __global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(A
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
   {
     const int s = it / TW, l = it % TW;
-    T vol[V];
+    A vol[V];
 #pragma unroll
-    for (int v = 0; v < V; v++) vol[v] = T(0);
+    for (int v = 0; v < V; v++) vol[v] = A(0);
 #pragma unroll
     for (int d = 0; d < D; d++)
     {
@@ -628,12 +650,12 @@ __global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(A
 #pragma unroll
       for (int m = 0; m < N; m++)
       {
-        const T c = o.Dm[i * N + m];
+        const A c = o.Dm[i * N + m];
 #pragma unroll
         for (int v = 0; v < V; v++) vol[v] += c * sdU[((d * S + b + m * st) * V + v) * TW + l];
       }
     }
-    T *out = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
+    A *out = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++) out[v * TW] = vol[v];
   }
@@ -643,44 +665,45 @@ __global__ void __launch_bounds__(Shape<D, N>::NT, (D == 3) ? 2 : 1) k_ns_grad(A
 // Navier-Stokes kernel 2: convective + LDG common flux, surface correction,
 // optional RK update (src/faces.cpp:1476-1614; src/elements.cpp:1476-1501).
 // ---------------------------------------------------------------------------
-template <typename T, int D, int N>
-__global__ void __launch_bounds__(Shape<D, N>::NT) k_ns_face(Args<T> a, LineOpsT<T, N> ops)
+template <typename T, typename A, int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT) k_ns_face(const __grid_constant__ Args<T, A> a,
+                                                                     const __grid_constant__ LineOpsT<A, N> ops)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *sFc = reinterpret_cast<T *>(smem_raw);
-  T *sUnew = sFc + Fp * V * TW;
-  T *sops = sUnew + S * V * TW;
-  load_ops<T, N>(sops, ops);
+  A *sFc = reinterpret_cast<A *>(smem_raw);
+  A *sUnew = sFc + Fp * V * TW;
+  A *sops = sUnew + S * V * TW;
+  load_ops<A, N>(sops, ops);
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
   __syncthreads();
-  SOps<T, N> o(sops);
-  const T beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
+  SOps<A, N> o(sops);
+  const A beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
   for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
   {
     const int f = it / TW, l = it % TW;
     const int64_t fi = (tile * Fp + f) * (int64_t)TW + l;
     const int code = a.nbr[fi];
-    T n[D], dA;
+    A n[D], dA;
     const T *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
 #pragma unroll
     for (int d = 0; d < D; d++) n[d] = g[d * TW];
     dA = g[D * TW];
-    T Uo[V], Un[V], UL[V], UR[V], UB[V], Fc[V], Fv[V];
+    A Uo[V], Un[V], UL[V], UR[V], UB[V], Fc[V], Fv[V];
     const T *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
-    if (code >= 0) gather_fpt<T, V>(a.Ufp, code >> 1, Un);
-    conv_common<T, D>(a, Uo, Un, code, n, UL, UR, UB, Fc);
+    if (code >= 0) gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
+    conv_common<T, A, D>(a, Uo, Un, code, n, UL, UR, UB, Fc);
     const T *fvo = a.Fvn + (tile * Fp + f) * (int64_t)V * TW + l;
     if (code >= 0)
     {
       const int slot = code & 1;
-      T FnL[V], FnR[V];
+      A FnL[V], FnR[V];
       // own side is left when slot == 0
-      if (beta == T(0.5))
+      if (beta == A(0.5))
       {
         if (slot == 0)
         {
@@ -688,11 +711,11 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_ns_face(Args<T> a, LineOpsT
           for (int v = 0; v < V; v++) FnL[v] = fvo[v * TW];
         }
         else
-          gather_fpt<T, V>(a.Fvn, code >> 1, FnL);
+          gather_fpt<T, A, V>(a.Fvn, code >> 1, FnL);
 #pragma unroll
-        for (int v = 0; v < V; v++) FnR[v] = T(0);
+        for (int v = 0; v < V; v++) FnR[v] = A(0);
       }
-      else if (beta == T(-0.5))
+      else if (beta == A(-0.5))
       {
         if (slot == 1)
         {
@@ -700,16 +723,16 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_ns_face(Args<T> a, LineOpsT
           for (int v = 0; v < V; v++) FnR[v] = fvo[v * TW];
         }
         else
-          gather_fpt<T, V>(a.Fvn, code >> 1, FnR);
+          gather_fpt<T, A, V>(a.Fvn, code >> 1, FnR);
 #pragma unroll
-        for (int v = 0; v < V; v++) FnL[v] = T(0);
+        for (int v = 0; v < V; v++) FnL[v] = A(0);
       }
       else
       {
-        T Fo[V], Fx[V];
+        A Fo[V], Fx[V];
 #pragma unroll
         for (int v = 0; v < V; v++) Fo[v] = fvo[v * TW];
-        gather_fpt<T, V>(a.Fvn, code >> 1, Fx);
+        gather_fpt<T, A, V>(a.Fvn, code >> 1, Fx);
 #pragma unroll
         for (int v = 0; v < V; v++)
         {
@@ -719,7 +742,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_ns_face(Args<T> a, LineOpsT
       }
 #pragma unroll
       for (int v = 0; v < V; v++)
-        Fv[v] = T(0.5) * (FnL[v] + FnR[v]) + tau * (UL[v] - UR[v]) + beta * (FnL[v] - FnR[v]);
+        Fv[v] = A(0.5) * (FnL[v] + FnR[v]) + tau * (UL[v] - UR[v]) + beta * (FnL[v] - FnR[v]);
     }
     else
     {
@@ -730,7 +753,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_ns_face(Args<T> a, LineOpsT
 #pragma unroll
     for (int v = 0; v < V; v++)
     {
-      T acc = right ? -Fc[v] * dA : Fc[v] * dA;
+      A acc = right ? -Fc[v] * dA : Fc[v] * dA;
       if (right)
         acc -= Fv[v] * dA;
       else
@@ -742,16 +765,16 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_ns_face(Args<T> a, LineOpsT
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
   {
     const int s = it / TW, l = it % TW;
-    T vol[V];
-    const T *dv = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
+    A vol[V];
+    const A *dv = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++) vol[v] = dv[v * TW];
-    finish_point<T, D, N>(a, tile, s, l, vol, sFc, o, a.extrap_next ? sUnew : nullptr);
+    finish_point<T, A, D, N>(a, tile, s, l, vol, sFc, o, a.extrap_next ? sUnew : nullptr);
   }
   if (a.extrap_next)
   {
     __syncthreads();
-    extrap_next_tile<T, D, N>(a, tile, sUnew, o);
+    extrap_next_tile<T, A, D, N>(a, tile, sUnew, o);
   }
 }
 

@@ -1,0 +1,649 @@
+// Hexahedron DFR kernels with a column mapping (sum factorisation).
+//
+// One CTA processes one tile of TW elements with TW x N^2 threads: thread
+// (l, ix, iy) owns the z-column of solution points (ix, iy, 0..N-1) of element
+// l and exactly six flux points, one on each face:
+//   face 0 (z-) and 1 (z+) at (x=ix, y=iy)    -- the ends of its own column,
+//   face 2 (x-) and 3 (x+) at (y=iy, z=ix),
+//   face 4 (y-) and 5 (y+) at (x=ix, z=iy),
+// so the N^2 threads of an element cover its 6 N^2 flux points once.  z-lines
+// live in registers; x- and y-lines are read from shared memory; the line
+// operator rows a thread needs are held in registers.  Arithmetic and
+// summation order are those of the generic kernels in dfr_kernels.cuh, which
+// follow the reference's operator products (src/elements.cpp:1337-1501).
+#pragma once
+
+#include "dfr_kernels.cuh"
+
+namespace zb {
+namespace dev {
+
+template <int N>
+struct HexIdx
+{
+  static constexpr int N2 = N * N, S = N * N * N, Fp = 6 * N * N;
+  // flux point ids of the thread's six flux points
+  static __device__ __forceinline__ void fpts(int ix, int iy, int f[6])
+  {
+    f[0] = iy * N + ix;                        // z-  (x = ix, y = iy)
+    f[1] = N2 + iy * N + (N - 1 - ix);         // z+
+    f[2] = 2 * N2 + ix * N + iy;               // x-  (y = iy, z = ix)
+    f[3] = 3 * N2 + ix * N + (N - 1 - iy);     // x+
+    f[4] = 4 * N2 + iy * N + (N - 1 - ix);     // y-  (x = ix, z = iy)
+    f[5] = 5 * N2 + iy * N + ix;               // y+
+  }
+  // id of own flux point q (same order as fpts)
+  static __device__ __forceinline__ int fpt(int q, int ix, int iy)
+  {
+    switch (q)
+    {
+      case 0: return iy * N + ix;
+      case 1: return N2 + iy * N + (N - 1 - ix);
+      case 2: return 2 * N2 + ix * N + iy;
+      case 3: return 3 * N2 + ix * N + (N - 1 - iy);
+      case 4: return 4 * N2 + iy * N + (N - 1 - ix);
+      default: return 5 * N2 + iy * N + ix;
+    }
+  }
+  // solution point on the normal line of own flux point q at position m
+  static __device__ __forceinline__ int line_spt(int q, int ix, int iy, int m)
+  {
+    if (q < 2) return ix + N * iy + N2 * m;    // z-line through (ix, iy)
+    if (q < 4) return m + N * iy + N2 * ix;    // x-line at (y = iy, z = ix)
+    return ix + N * m + N2 * iy;               // y-line at (x = ix, z = iy)
+  }
+  // x- and y-face flux points at the ends of the lines through spt (ix, iy, iz)
+  static __device__ __forceinline__ int fxm(int iy, int iz) { return 2 * N2 + iz * N + iy; }
+  static __device__ __forceinline__ int fxp(int iy, int iz) { return 3 * N2 + iz * N + (N - 1 - iy); }
+  static __device__ __forceinline__ int fym(int ix, int iz) { return 4 * N2 + iz * N + (N - 1 - ix); }
+  static __device__ __forceinline__ int fyp(int ix, int iz) { return 5 * N2 + iz * N + ix; }
+};
+
+// The line-operator rows of a thread's x and y coordinates, in registers; the
+// z row (uniform across a warp inside a z loop) is read from the kernel
+// parameter.
+template <typename A, int N>
+struct RowOps
+{
+  A Dx[N], Dy[N], dbxm, dbxp, dbym, dbyp;
+  __device__ __forceinline__ void load(const LineOpsT<A, N> &o, int ix, int iy)
+  {
+#pragma unroll
+    for (int m = 0; m < N; m++)
+    {
+      Dx[m] = o.Dm[ix * N + m];
+      Dy[m] = o.Dm[iy * N + m];
+    }
+    dbxm = o.Dbm[ix];
+    dbxp = o.Dbp[ix];
+    dbym = o.Dbm[iy];
+    dbyp = o.Dbp[iy];
+  }
+};
+
+// own flux point q (0..5): side of the face
+__device__ __forceinline__ bool q_minus(int q) { return (q & 1) == 0; }
+
+template <typename T, typename A, int N>
+__device__ __forceinline__ void load_face_geo(const Args<T, A> &a, int64_t tile, int f, int l, A n[3], A &dA, int &code)
+{
+  using H = HexIdx<N>;
+  const T *g = a.fgeo + (tile * H::Fp + f) * (int64_t)4 * TW + l;
+  n[0] = g[0];
+  n[1] = g[TW];
+  n[2] = g[2 * TW];
+  dA = g[3 * TW];
+  code = a.nbr[(tile * H::Fp + f) * (int64_t)TW + l];
+}
+
+// ---------------------------------------------------------------------------
+// state -> flux points (src/elements.cpp:1337-1360)
+// ---------------------------------------------------------------------------
+template <typename T, typename A, int N>
+__global__ void __launch_bounds__(TW * N * N) k_hex_extrap(const T *__restrict__ U, T *__restrict__ Ufp, int64_t ntiles,
+                                                           const __grid_constant__ LineOpsT<A, N> ops)
+{
+  using H = HexIdx<N>;
+  constexpr int S = H::S, V = 5;
+  const int l = threadIdx.x % TW, c = threadIdx.x / TW, ix = c % N, iy = c / N;
+  const int64_t tile = blockIdx.x;
+  if (tile >= ntiles) return;
+  const T *Ut = U + tile * (int64_t)S * V * TW;
+  int f[6];
+  H::fpts(ix, iy, f);
+#pragma unroll
+  for (int q = 0; q < 6; q++)
+  {
+    T *out = Ufp + (tile * H::Fp + f[q]) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      A acc = (q_minus(q) ? ops.Em[0] : ops.Ep[0]) * Ut[(H::line_spt(q, ix, iy, 0) * V + v) * TW + l];
+#pragma unroll
+      for (int m = 1; m < N; m++)
+        acc += (q_minus(q) ? ops.Em[m] : ops.Ep[m]) * Ut[(H::line_spt(q, ix, iy, m) * V + v) * TW + l];
+      out[v * TW] = acc;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// common convective (+LDG) flux at the thread's six flux points, dA-scaled and
+// signed for this element, into sFc [Fp][V][TW]
+// ---------------------------------------------------------------------------
+template <typename T, typename A, int N, bool VISC>
+__device__ __forceinline__ void hex_common_flux(const Args<T, A> &a, int64_t tile, int l, int ix, int iy, A *sFc)
+{
+  using H = HexIdx<N>;
+  constexpr int V = 5;
+  const A beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
+#pragma unroll 1
+  for (int q = 0; q < 6; q++)
+  {
+    const int fq = H::fpt(q, ix, iy);
+    A n[3], dA;
+    int code;
+    load_face_geo<T, A, N>(a, tile, fq, l, n, dA, code);
+    A Uo[V], Un[V], UL[V], UR[V], UB[V], Fc[V];
+    const T *uo = a.Ufp + (tile * H::Fp + fq) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
+    if (code >= 0) gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
+    conv_common<T, A, 3>(a, Uo, Un, code, n, UL, UR, UB, Fc);
+    const bool right = (code >= 0) && (code & 1);
+    A Fv[V];
+    if (VISC)
+    {
+      const T *fvo = a.Fvn + (tile * H::Fp + fq) * (int64_t)V * TW + l;
+      if (code >= 0)
+      {
+        const int slot = code & 1;
+        A FnL[V], FnR[V];
+        if (beta == A(0.5))
+        {
+          if (slot == 0)
+          {
+#pragma unroll
+            for (int v = 0; v < V; v++) FnL[v] = fvo[v * TW];
+          }
+          else
+            gather_fpt<T, A, V>(a.Fvn, code >> 1, FnL);
+#pragma unroll
+          for (int v = 0; v < V; v++) FnR[v] = A(0);
+        }
+        else if (beta == A(-0.5))
+        {
+          if (slot == 1)
+          {
+#pragma unroll
+            for (int v = 0; v < V; v++) FnR[v] = fvo[v * TW];
+          }
+          else
+            gather_fpt<T, A, V>(a.Fvn, code >> 1, FnR);
+#pragma unroll
+          for (int v = 0; v < V; v++) FnL[v] = A(0);
+        }
+        else
+        {
+          A Fo[V], Fx[V];
+#pragma unroll
+          for (int v = 0; v < V; v++) Fo[v] = fvo[v * TW];
+          gather_fpt<T, A, V>(a.Fvn, code >> 1, Fx);
+#pragma unroll
+          for (int v = 0; v < V; v++)
+          {
+            FnL[v] = slot ? Fx[v] : Fo[v];
+            FnR[v] = slot ? Fo[v] : Fx[v];
+          }
+        }
+#pragma unroll
+        for (int v = 0; v < V; v++)
+          Fv[v] = A(0.5) * (FnL[v] + FnR[v]) + tau * (UL[v] - UR[v]) + beta * (FnL[v] - FnR[v]);
+      }
+      else
+      {
+#pragma unroll
+        for (int v = 0; v < V; v++) Fv[v] = fvo[v * TW] + tau * (UL[v] - UB[v]);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      A acc = right ? -Fc[v] * dA : Fc[v] * dA;
+      if (VISC)
+      {
+        if (right)
+          acc -= Fv[v] * dA;
+        else
+          acc += Fv[v] * dA;
+      }
+      sFc[(fq * V + v) * TW + l] = acc;
+    }
+  }
+}
+
+// surface correction for spt (ix, iy, iz) in flux-point order (faces 0..5)
+template <typename A, int N>
+__device__ __forceinline__ A hex_surface(const LineOpsT<A, N> &ops, const RowOps<A, N> &o, const A *sFc, int ix, int iy,
+                                         int iz, int v, int l)
+{
+  using H = HexIdx<N>;
+  constexpr int V = 5;
+  A s = A(0);
+  s += -ops.Dbm[iz] * sFc[((iy * N + ix) * V + v) * TW + l];
+  s += ops.Dbp[iz] * sFc[((H::N2 + iy * N + (N - 1 - ix)) * V + v) * TW + l];
+  s += -o.dbxm * sFc[(H::fxm(iy, iz) * V + v) * TW + l];
+  s += o.dbxp * sFc[(H::fxp(iy, iz) * V + v) * TW + l];
+  s += -o.dbym * sFc[(H::fym(ix, iz) * V + v) * TW + l];
+  s += o.dbyp * sFc[(H::fyp(ix, iz) * V + v) * TW + l];
+  return s;
+}
+
+// RK update of one spt and optional staging of the new state for extrapolation
+// (src/solver.cpp:2916-2937, 3040-3094)
+template <typename T, typename A, int N>
+__device__ __forceinline__ void hex_finish(const Args<T, A> &a, int64_t tile, int s, int l, const A res[5], A *sUnew)
+{
+  using H = HexIdx<N>;
+  constexpr int V = 5, NM = 10;
+  const int64_t base = (tile * H::S + s) * (int64_t)V * TW;
+#pragma unroll
+  for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
+  if (a.rk_mode == 0) return;
+  const A detJ = a.mets[((tile * H::S + s) * NM + 9) * TW + l];
+#pragma unroll
+  for (int v = 0; v < V; v++)
+  {
+    const int64_t idx = base + v * TW + l;
+    A u_ini;
+    if (a.save_ini)
+    {
+      u_ini = a.U[idx];
+      a.U_ini[idx] = u_ini;
+    }
+    else
+      u_ini = a.U_ini[idx];
+    A unew;
+    if (a.rk_mode == 1)
+      unew = u_ini - a.rk_coef[0] * a.dt / detJ * res[v];
+    else if (a.Ucomp)
+    {
+      // Kahan-compensated step increment; the remainder includes the
+      // rounding of the stored state
+      A delta = A(0);
+      for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * a.dt / detJ * (A)a.divF_prev[st][idx];
+      delta -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
+      const A c = a.Ucomp[idx];
+      const A y = delta - c;
+      unew = (A)(T)(u_ini + y);
+      a.Ucomp[idx] = (T)((unew - u_ini) - y);
+    }
+    else
+    {
+      unew = u_ini;
+      for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * a.dt / detJ * a.divF_prev[st][idx];
+      unew -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
+    }
+    a.Uout[idx] = unew;
+    if (sUnew) sUnew[(s * V + v) * TW + l] = (A)(T)unew;  // the state as stored
+  }
+}
+
+template <typename T, typename A, int N>
+__device__ __forceinline__ void hex_extrap_next(const Args<T, A> &a, int64_t tile, int l, int ix, int iy, const int f[6],
+                                                const A *sUnew, const LineOpsT<A, N> &o)
+{
+  using H = HexIdx<N>;
+  constexpr int V = 5;
+#pragma unroll
+  for (int q = 0; q < 6; q++)
+  {
+    T *out = a.Ufp_next + (tile * H::Fp + f[q]) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      A acc = (q_minus(q) ? o.Em[0] : o.Ep[0]) * sUnew[(H::line_spt(q, ix, iy, 0) * V + v) * TW + l];
+#pragma unroll
+      for (int m = 1; m < N; m++)
+        acc += (q_minus(q) ? o.Em[m] : o.Ep[m]) * sUnew[(H::line_spt(q, ix, iy, m) * V + v) * TW + l];
+      out[v * TW] = acc;
+    }
+  }
+}
+
+template <typename T, typename A>
+__device__ __forceinline__ void load_adj(const Args<T, A> &a, int64_t tile, int S, int s, int l, A adj[3][3], A &det)
+{
+  const T *m = a.mets + (tile * S + s) * (int64_t)10 * TW + l;
+#pragma unroll
+  for (int d1 = 0; d1 < 3; d1++)
+#pragma unroll
+    for (int d2 = 0; d2 < 3; d2++) adj[d1][d2] = m[(d1 * 3 + d2) * TW];
+  det = m[9 * TW];
+}
+
+// ---------------------------------------------------------------------------
+// Euler: volume flux, common flux, divergence (+RK, +next extrapolation)
+// ---------------------------------------------------------------------------
+template <typename T, typename A, int N>
+__global__ void __launch_bounds__(TW * N * N) k_hex_euler(const __grid_constant__ Args<T, A> a,
+                                                          const __grid_constant__ LineOpsT<A, N> ops)
+{
+  using H = HexIdx<N>;
+  constexpr int S = H::S, Fp = H::Fp, V = 5;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  A *sU = reinterpret_cast<A *>(smem_raw);   // [S][V][TW] state, then new state
+  A *sF = sU + S * V * TW;                   // [3][S][V][TW] transformed flux
+  A *sFc = sF + 3 * S * V * TW;              // [Fp][V][TW]
+  const int l = threadIdx.x % TW, c = threadIdx.x / TW, ix = c % N, iy = c / N;
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  RowOps<A, N> o;
+  o.load(ops, ix, iy);
+  int f[6];
+  H::fpts(ix, iy, f);
+  const T *Ut = a.U + tile * (int64_t)S * V * TW;
+#pragma unroll 1
+  for (int iz = 0; iz < N; iz++)
+  {
+    const int s = ix + N * iy + H::N2 * iz;
+    A U[V], F[V][3], P, Pp, adj[3][3], det;
+#pragma unroll
+    for (int v = 0; v < V; v++) U[v] = Ut[(s * V + v) * TW + l];
+    flux_conv_stored<A, 3>(U, F, P, Pp, a.ph);
+    load_adj<T, A>(a, tile, S, s, l, adj, det);
+#pragma unroll
+    for (int v = 0; v < V; v++)
+#pragma unroll
+      for (int d1 = 0; d1 < 3; d1++)
+      {
+        A t = F[v][0] * adj[d1][0];
+        t += F[v][1] * adj[d1][1];
+        t += F[v][2] * adj[d1][2];
+        sF[((d1 * S + s) * V + v) * TW + l] = t;
+      }
+  }
+  hex_common_flux<T, A, N, false>(a, tile, l, ix, iy, sFc);
+  __syncthreads();
+#pragma unroll 1
+  for (int iz = 0; iz < N; iz++)
+  {
+    const int s = ix + N * iy + H::N2 * iz;
+    A res[V];
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      A vol = A(0);
+#pragma unroll
+      for (int m = 0; m < N; m++) vol += o.Dx[m] * sF[((0 * S + m + N * iy + H::N2 * iz) * V + v) * TW + l];
+#pragma unroll
+      for (int m = 0; m < N; m++) vol += o.Dy[m] * sF[((1 * S + ix + N * m + H::N2 * iz) * V + v) * TW + l];
+#pragma unroll
+      for (int m = 0; m < N; m++) vol += ops.Dm[iz * N + m] * sF[((2 * S + ix + N * iy + H::N2 * m) * V + v) * TW + l];
+      res[v] = vol + hex_surface<A, N>(ops, o, sFc, ix, iy, iz, v, l);
+    }
+    hex_finish<T, A, N>(a, tile, s, l, res, a.extrap_next ? sU : nullptr);
+  }
+  if (a.extrap_next)
+  {
+    __syncthreads();
+    hex_extrap_next<T, A, N>(a, tile, l, ix, iy, f, sU, ops);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Navier-Stokes kernel 1 (column mapping): common solution, gradient, viscous
+// normal flux at own flux points, flux, volume divergence
+// ---------------------------------------------------------------------------
+template <typename T, typename A, int N>
+__global__ void __launch_bounds__(TW * N * N) k_hex_ns_grad(const __grid_constant__ Args<T, A> a,
+                                                          const __grid_constant__ LineOpsT<A, N> ops)
+{
+  using H = HexIdx<N>;
+  constexpr int S = H::S, Fp = H::Fp, V = 5;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  A *sU = reinterpret_cast<A *>(smem_raw);   // [S][V][TW]
+  A *sUC = sU + S * V * TW;                  // [Fp][V][TW] common solution
+  A *sX = sUC + Fp * V * TW;                 // [3][S][V][TW] physical gradient, then F~
+  const int l = threadIdx.x % TW, c = threadIdx.x / TW, ix = c % N, iy = c / N;
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  RowOps<A, N> o;
+  o.load(ops, ix, iy);
+  int f[6];
+  H::fpts(ix, iy, f);
+  const A beta = a.ph.ldg_b;
+  // own column of the state -> registers and shared memory
+  A Uc[N][V];
+  {
+    const T *Ut = a.U + tile * (int64_t)S * V * TW;
+#pragma unroll
+    for (int iz = 0; iz < N; iz++)
+#pragma unroll
+      for (int v = 0; v < V; v++)
+      {
+        const int s = ix + N * iy + H::N2 * iz;
+        Uc[iz][v] = Ut[(s * V + v) * TW + l];
+        sU[(s * V + v) * TW + l] = Uc[iz][v];
+      }
+  }
+  // common solution at own flux points (LDG, flip_beta = 1)
+#pragma unroll 1
+  for (int q = 0; q < 6; q++)
+  {
+    const int fq = H::fpt(q, ix, iy);
+    A n[3], dA;
+    int code;
+    load_face_geo<T, A, N>(a, tile, fq, l, n, dA, code);
+    A Uo[V], UC[V];
+    const T *uo = a.Ufp + (tile * Fp + fq) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
+    if (code >= 0)
+    {
+      A Un[V];
+      gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
+      const int slot = code & 1;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+      {
+        const A ul = slot ? Un[v] : Uo[v];
+        const A ur = slot ? Uo[v] : Un[v];
+        if (beta == A(0.5))
+          UC[v] = ur;
+        else if (beta == A(-0.5))
+          UC[v] = ul;
+        else
+          UC[v] = A(0.5) * (ul + ur) - beta * (ul - ur);
+      }
+    }
+    else
+    {
+      A Ua[V], URa[V], UBa[V];
+      to_abs<A, 3>(Uo, Ua, a.ph);
+      ghost_state<A, 3>(-code - 1, Ua, n, URa, UBa, a.ph);
+      to_stored<A, 3>(UBa, UC, a.ph);
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) sUC[(fq * V + v) * TW + l] = UC[v];
+  }
+  __syncthreads();
+  // corrected reference gradient -> physical gradient
+  const int fzm = H::fpt(0, ix, iy), fzp = H::fpt(1, ix, iy);
+#pragma unroll 1
+  for (int iz = 0; iz < N; iz++)
+  {
+    const int s = ix + N * iy + H::N2 * iz;
+    const int fxm = H::fxm(iy, iz), fxp = H::fxp(iy, iz), fym = H::fym(ix, iz), fyp = H::fyp(ix, iz);
+    A adj[3][3], det;
+    load_adj<T, A>(a, tile, S, s, l, adj, det);
+    const A inv_det = A(1) / det;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      A td[3];
+      {
+        A acc = A(0);
+#pragma unroll
+        for (int m = 0; m < N; m++) acc += o.Dx[m] * sU[((m + N * iy + H::N2 * iz) * V + v) * TW + l];
+        const A cm = o.dbxm * sUC[(fxm * V + v) * TW + l];
+        const A cp = o.dbxp * sUC[(fxp * V + v) * TW + l];
+        td[0] = acc + (cm + cp);
+      }
+      {
+        A acc = A(0);
+#pragma unroll
+        for (int m = 0; m < N; m++) acc += o.Dy[m] * sU[((ix + N * m + H::N2 * iz) * V + v) * TW + l];
+        const A cm = o.dbym * sUC[(fym * V + v) * TW + l];
+        const A cp = o.dbyp * sUC[(fyp * V + v) * TW + l];
+        td[1] = acc + (cm + cp);
+      }
+      {
+        A acc = A(0);
+#pragma unroll
+        for (int m = 0; m < N; m++) acc += ops.Dm[iz * N + m] * Uc[m][v];
+        const A cm = ops.Dbm[iz] * sUC[(fzm * V + v) * TW + l];
+        const A cp = ops.Dbp[iz] * sUC[(fzp * V + v) * TW + l];
+        td[2] = acc + (cm + cp);
+      }
+#pragma unroll
+      for (int d1 = 0; d1 < 3; d1++)
+      {
+        A g = td[0] * adj[0][d1];
+        g += td[1] * adj[1][d1];
+        g += td[2] * adj[2][d1];
+        sX[((d1 * S + s) * V + v) * TW + l] = g * inv_det;
+        if (a.dU_out) a.dU_out[(((tile * 3 + d1) * S + s) * V + v) * TW + l] = (T)(g * inv_det);
+      }
+    }
+  }
+  __syncthreads();
+  // viscous normal flux at own flux points
+#pragma unroll 1
+  for (int q = 0; q < 6; q++)
+  {
+    const int fq = H::fpt(q, ix, iy);
+    A n[3], dA;
+    int code;
+    load_face_geo<T, A, N>(a, tile, fq, l, n, dA, code);
+    if (code >= 0 && ((beta == A(0.5) && (code & 1)) || (beta == A(-0.5) && !(code & 1)))) continue;
+    A Uf[V], dUf[V][3], Fn[V];
+    const T *uo = a.Ufp + (tile * Fp + fq) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      Uf[v] = uo[v * TW];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+      {
+        A acc = (q_minus(q) ? ops.Em[0] : ops.Ep[0]) * sX[((d * S + H::line_spt(q, ix, iy, 0)) * V + v) * TW + l];
+#pragma unroll
+        for (int m = 1; m < N; m++)
+          acc += (q_minus(q) ? ops.Em[m] : ops.Ep[m]) * sX[((d * S + H::line_spt(q, ix, iy, m)) * V + v) * TW + l];
+        dUf[v][d] = acc;
+      }
+    }
+    A Ua[V];
+    to_abs<A, 3>(Uf, Ua, a.ph);
+    if (code >= 0)
+      visc_normal<A, 3>(Ua, dUf, n, Fn, a.ph);
+    else
+    {
+      A UR[V], UB[V], dUB[V][3];
+      ghost_state<A, 3>(-code - 1, Ua, n, UR, UB, a.ph);
+      ghost_grad<A, 3>(-code - 1, Ua, dUf, n, dUB);
+      visc_normal<A, 3>(UB, dUB, n, Fn, a.ph);
+    }
+    T *out = a.Fvn + (tile * Fp + fq) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) out[v * TW] = Fn[v];
+  }
+  __syncthreads();
+  // flux at own column, transformed F~ = adj F (overwrites the gradient in place)
+#pragma unroll 1
+  for (int iz = 0; iz < N; iz++)
+  {
+    const int s = ix + N * iy + H::N2 * iz;
+    A dU[V][3], F[V][3], P, Pp, Ua[V], adj[3][3], det;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+#pragma unroll
+      for (int d = 0; d < 3; d++) dU[v][d] = sX[((d * S + s) * V + v) * TW + l];
+    flux_conv_stored<A, 3>(Uc[iz], F, P, Pp, a.ph);
+    to_abs<A, 3>(Uc[iz], Ua, a.ph);
+    flux_visc_add<A, 3>(Ua, dU, F, a.ph);
+    load_adj<T, A>(a, tile, S, s, l, adj, det);
+#pragma unroll
+    for (int v = 0; v < V; v++)
+#pragma unroll
+      for (int d1 = 0; d1 < 3; d1++)
+      {
+        A t = F[v][0] * adj[d1][0];
+        t += F[v][1] * adj[d1][1];
+        t += F[v][2] * adj[d1][2];
+        sX[((d1 * S + s) * V + v) * TW + l] = t;
+      }
+  }
+  __syncthreads();
+  // volume divergence
+#pragma unroll 1
+  for (int iz = 0; iz < N; iz++)
+  {
+    const int s = ix + N * iy + H::N2 * iz;
+    A *out = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      A vol = A(0);
+#pragma unroll
+      for (int m = 0; m < N; m++) vol += o.Dx[m] * sX[((0 * S + m + N * iy + H::N2 * iz) * V + v) * TW + l];
+#pragma unroll
+      for (int m = 0; m < N; m++) vol += o.Dy[m] * sX[((1 * S + ix + N * m + H::N2 * iz) * V + v) * TW + l];
+#pragma unroll
+      for (int m = 0; m < N; m++) vol += ops.Dm[iz * N + m] * sX[((2 * S + ix + N * iy + H::N2 * m) * V + v) * TW + l];
+      out[v * TW] = vol;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Navier-Stokes kernel 2 (column mapping): common flux, surface correction,
+// RK update, next-stage extrapolation
+// ---------------------------------------------------------------------------
+template <typename T, typename A, int N>
+__global__ void __launch_bounds__(TW * N * N) k_hex_ns_face(const __grid_constant__ Args<T, A> a,
+                                                          const __grid_constant__ LineOpsT<A, N> ops)
+{
+  using H = HexIdx<N>;
+  constexpr int S = H::S, Fp = H::Fp, V = 5;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  A *sFc = reinterpret_cast<A *>(smem_raw);  // [Fp][V][TW]
+  A *sUnew = sFc + Fp * V * TW;              // [S][V][TW]
+  const int l = threadIdx.x % TW, c = threadIdx.x / TW, ix = c % N, iy = c / N;
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  RowOps<A, N> o;
+  o.load(ops, ix, iy);
+  int f[6];
+  H::fpts(ix, iy, f);
+  hex_common_flux<T, A, N, true>(a, tile, l, ix, iy, sFc);
+  __syncthreads();
+#pragma unroll 1
+  for (int iz = 0; iz < N; iz++)
+  {
+    const int s = ix + N * iy + H::N2 * iz;
+    const A *dv = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
+    A res[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) res[v] = dv[v * TW] + hex_surface<A, N>(ops, o, sFc, ix, iy, iz, v, l);
+    hex_finish<T, A, N>(a, tile, s, l, res, a.extrap_next ? sUnew : nullptr);
+  }
+  if (a.extrap_next)
+  {
+    __syncthreads();
+    hex_extrap_next<T, A, N>(a, tile, l, ix, iy, f, sUnew, ops);
+  }
+}
+
+}  // namespace dev
+}  // namespace zb

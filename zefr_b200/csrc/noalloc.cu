@@ -200,7 +200,7 @@ void run_kernels(const Plan &p, unsigned char *base, const Regions &r, cudaStrea
   using G = dev::Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, NT = G::NT;
   const auto ops = line_ops_d<N>(p);
-  dev::Args<double> a;
+  dev::Args<double, double> a;
   std::memset(&a, 0, sizeof(a));
   a.U = reinterpret_cast<const double *>(base + r.U);
   a.Ufp = reinterpret_cast<const double *>(base + r.Ufp);
@@ -231,26 +231,26 @@ void run_kernels(const Plan &p, unsigned char *base, const Regions &r, cudaStrea
   }
   a.ph.fix_vis = q.fix_vis;
   a.ph.fconv = q.fconv;
-  dev::k_extrap<double, D, N><<<blocks_for(p.ntiles * Fp * TW), 256, 0, st>>>(
+  dev::k_extrap<double, double, D, N><<<blocks_for(p.ntiles * Fp * TW), 256, 0, st>>>(
       a.U, reinterpret_cast<double *>(base + r.Ufp), p.ntiles, ops);
   NA_CK(cudaGetLastError());
   const size_t ob = sizeof(dev::LineOpsT<double, N>);
   if (!p.params.viscous)
   {
     const size_t smem = (size_t)(S * V + D * S * V + Fp * V) * TW * sizeof(double) + ob;
-    NA_CK(cudaFuncSetAttribute(dev::k_euler<double, D, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dev::k_euler<double, D, N><<<(unsigned)p.ntiles, NT, smem, st>>>(a, ops);
+    NA_CK(cudaFuncSetAttribute(dev::k_euler<double, double, D, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dev::k_euler<double, double, D, N><<<(unsigned)p.ntiles, NT, smem, st>>>(a, ops);
     NA_CK(cudaGetLastError());
   }
   else
   {
     const size_t smem1 = (size_t)(S * V + Fp * V + D * S * V) * TW * sizeof(double) + ob;
-    NA_CK(cudaFuncSetAttribute(dev::k_ns_grad<double, D, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
-    dev::k_ns_grad<double, D, N><<<(unsigned)p.ntiles, NT, smem1, st>>>(a, ops);
+    NA_CK(cudaFuncSetAttribute(dev::k_ns_grad<double, double, D, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
+    dev::k_ns_grad<double, double, D, N><<<(unsigned)p.ntiles, NT, smem1, st>>>(a, ops);
     NA_CK(cudaGetLastError());
     const size_t smem2 = (size_t)(Fp * V + S * V) * TW * sizeof(double) + ob;
-    NA_CK(cudaFuncSetAttribute(dev::k_ns_face<double, D, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-    dev::k_ns_face<double, D, N><<<(unsigned)p.ntiles, NT, smem2, st>>>(a, ops);
+    NA_CK(cudaFuncSetAttribute(dev::k_ns_face<double, double, D, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    dev::k_ns_face<double, double, D, N><<<(unsigned)p.ntiles, NT, smem2, st>>>(a, ops);
     NA_CK(cudaGetLastError());
   }
 }

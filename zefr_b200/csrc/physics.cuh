@@ -16,7 +16,16 @@ struct Phys
   T rus_k, ldg_b, ldg_tau;
   T rho_fs, V_fs[3], P_fs, T_wall, R_ref, V_wall[3];
   int fix_vis, fconv;
+  // Reference state of the perturbation form (mixed precision): the stored
+  // state is U' = U - Ur.  Pr = p(Ur), er = Er + Pr, inv_rr = 1/rho_r,
+  // mr2 = |m_r|^2.
+  T Ur[5], Pr, er, inv_rr, mr2;
+  int dev;  // 1: stored states are deviations from Ur (FP32 storage)
 };
+
+// Arithmetic of the perturbation form: FP32 stores deviations from Ur.
+template <typename T> struct Pert { static constexpr bool on = false; };
+template <> struct Pert<float> { static constexpr bool on = true; };
 
 template <typename T> __device__ __forceinline__ T dsqrt(T x);
 template <> __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
@@ -45,6 +54,76 @@ __device__ __forceinline__ void flux_conv(const T U[D + 2], T F[D + 2][D], T &P,
 #pragma unroll
     for (int k = 0; k < D; k++) F[k + 1][d] = U[d + 1] * U[k + 1] * invrho + (k == d ? P : T(0));
     F[D + 1][d] = U[d + 1] * H;
+  }
+}
+
+// Inviscid flux deviation F(Ur + Up) - F(Ur), absolute pressure P and its
+// deviation Pp, written so no O(1) constant cancels (the flux of
+// include/flux.hpp:11-63 expanded about the reference state Ur):
+//   |m|^2/rho - |mr|^2/rho_r = (2 mr.m' + |m'|^2)/rho - |mr|^2 rho'/(rho rho_r)
+//   m_k m_d/rho - mr_k mr_d/rho_r = (mr_k m'_d + m'_k mr_d + m'_k m'_d)/rho
+//                                   - mr_k mr_d rho'/(rho rho_r)
+//   m_d e/rho - mr_d er/rho_r = (m'_d er + mr_d e' + m'_d e')/rho - mr_d er rho'/(rho rho_r)
+// with e = E + P the total enthalpy per volume.
+template <typename T, int D>
+__device__ __forceinline__ void flux_conv_pert(const T Up[D + 2], T F[D + 2][D], T &P, T &Pp, const Phys<T> &ph)
+{
+  const T *Ur = ph.Ur;
+  const T rho = Ur[0] + Up[0];
+  const T invr = T(1) / rho;
+  const T c = Up[0] * invr * ph.inv_rr;  // rho' / (rho rho_r)
+  T mrmp = Ur[1] * Up[1], mpmp = Up[1] * Up[1];
+#pragma unroll
+  for (int d = 1; d < D; d++)
+  {
+    mrmp += Ur[d + 1] * Up[d + 1];
+    mpmp += Up[d + 1] * Up[d + 1];
+  }
+  const T dke2 = (T(2) * mrmp + mpmp) * invr - ph.mr2 * c;
+  Pp = (ph.gamma - T(1)) * (Up[D + 1] - T(0.5) * dke2);
+  P = ph.Pr + Pp;
+  const T ep = Up[D + 1] + Pp;
+#pragma unroll
+  for (int d = 0; d < D; d++)
+  {
+    F[0][d] = Up[d + 1];
+#pragma unroll
+    for (int k = 0; k < D; k++)
+      F[k + 1][d] = (Ur[k + 1] * Up[d + 1] + Up[k + 1] * Ur[d + 1] + Up[k + 1] * Up[d + 1]) * invr -
+                    Ur[k + 1] * Ur[d + 1] * c + (k == d ? Pp : T(0));
+    F[D + 1][d] = (Up[d + 1] * ph.er + Ur[d + 1] * ep + Up[d + 1] * ep) * invr - Ur[d + 1] * ph.er * c;
+  }
+}
+
+// absolute state from a stored one (identity outside the perturbation form)
+template <typename T, int D>
+__device__ __forceinline__ void to_abs(const T Us[D + 2], T Ua[D + 2], const Phys<T> &ph)
+{
+#pragma unroll
+  for (int v = 0; v < D + 2; v++) Ua[v] = ph.dev ? ph.Ur[v] + Us[v] : Us[v];
+}
+
+template <typename T, int D>
+__device__ __forceinline__ void to_stored(const T Ua[D + 2], T Us[D + 2], const Phys<T> &ph)
+{
+#pragma unroll
+  for (int v = 0; v < D + 2; v++) Us[v] = ph.dev ? Ua[v] - ph.Ur[v] : Ua[v];
+}
+
+// Inviscid flux of a stored state (deviation from Ur in the perturbation form)
+// and the absolute pressure.
+template <typename T, int D>
+__device__ __forceinline__ void flux_conv_stored(const T Us[D + 2], T F[D + 2][D], T &P, T &Pp, const Phys<T> &ph)
+{
+  if constexpr (Pert<T>::on)
+    flux_conv_pert<T, D>(Us, F, P, Pp, ph);
+  else
+  {
+    // FP64 arithmetic: absolute flux (a stored deviation is added back exactly)
+    T Ua[D + 2];
+    to_abs<T, D>(Us, Ua, ph);
+    flux_conv<T, D>(Ua, F, P, ph.gamma);
+    Pp = P;
   }
 }
 
@@ -130,21 +209,26 @@ __device__ __forceinline__ void visc_normal(const T U[D + 2], const T dU[D + 2][
 }
 
 // Rusanov common normal flux, upwinded form (src/faces.cpp:1243-1364, rus_bias 0).
+// UL, UR are stored states (deviations from Ur in the perturbation form); the
+// result is the common flux of the stored form (minus F(Ur).n).
 template <typename T, int D>
 __device__ __forceinline__ void rusanov(const T UL[D + 2], const T UR[D + 2], const T n[D], T Fc[D + 2],
                                         const Phys<T> &ph)
 {
-  T FL[D + 2][D], FR[D + 2][D], PL, PR;
-  flux_conv<T, D>(UL, FL, PL, ph.gamma);
-  flux_conv<T, D>(UR, FR, PR, ph.gamma);
-  const T aL = dsqrt<T>(ph.gamma * PL / UL[0]);
-  const T aR = dsqrt<T>(ph.gamma * PR / UR[0]);
-  T VnL = UL[1] / UL[0] * n[0], VnR = UR[1] / UR[0] * n[0];
+  T FL[D + 2][D], FR[D + 2][D], PL, PR, QL, QR;
+  flux_conv_stored<T, D>(UL, FL, PL, QL, ph);
+  flux_conv_stored<T, D>(UR, FR, PR, QR, ph);
+  T AL[D + 2], AR[D + 2];
+  to_abs<T, D>(UL, AL, ph);
+  to_abs<T, D>(UR, AR, ph);
+  const T aL = dsqrt<T>(ph.gamma * PL / AL[0]);
+  const T aR = dsqrt<T>(ph.gamma * PR / AR[0]);
+  T VnL = AL[1] / AL[0] * n[0], VnR = AR[1] / AR[0] * n[0];
 #pragma unroll
   for (int d = 1; d < D; d++)
   {
-    VnL += UL[d + 1] / UL[0] * n[d];
-    VnR += UR[d + 1] / UR[0] * n[d];
+    VnL += AL[d + 1] / AL[0] * n[d];
+    VnR += AR[d + 1] / AR[0] * n[d];
   }
   const T eig = dmax<T>(dabs<T>(VnL) + aL, dabs<T>(VnR) + aR);
   const T diss = T(0.5) * eig * (T(1) - ph.rus_k);
@@ -168,13 +252,16 @@ __device__ __forceinline__ void rusanov(const T UL[D + 2], const T UR[D + 2], co
 // |l| below delta = 0.1 * (|u_n| + a) of the Roe state is replaced by
 // (l^2 + delta^2) / (2 delta).  No reference counterpart.
 template <typename T, int D>
-__device__ __forceinline__ void roe(const T UL[D + 2], const T UR[D + 2], const T n[D], T Fc[D + 2],
+__device__ __forceinline__ void roe(const T SL[D + 2], const T SR[D + 2], const T n[D], T Fc[D + 2],
                                     const Phys<T> &ph)
 {
   const T g = ph.gamma;
-  T FL[D + 2][D], FR[D + 2][D], PL, PR;
-  flux_conv<T, D>(UL, FL, PL, g);
-  flux_conv<T, D>(UR, FR, PR, g);
+  T FL[D + 2][D], FR[D + 2][D], PL, PR, QL, QR;
+  flux_conv_stored<T, D>(SL, FL, PL, QL, ph);
+  flux_conv_stored<T, D>(SR, FR, PR, QR, ph);
+  T UL[D + 2], UR[D + 2];
+  to_abs<T, D>(SL, UL, ph);
+  to_abs<T, D>(SR, UR, ph);
   const T rL = UL[0], rR = UR[0];
   const T sL = dsqrt<T>(rL), sR = dsqrt<T>(rR);
   const T inv = T(1) / (sL + sR);
@@ -201,7 +288,7 @@ __device__ __forceinline__ void roe(const T UL[D + 2], const T UR[D + 2], const 
   a2 = dmax<T>(a2, T(1e-30));
   const T a = dsqrt<T>(a2);
   const T rho = sL * sR;
-  const T dp = PR - PL, dr = rR - rL, dun = unR - unL;
+  const T dp = QR - QL, dr = SR[0] - SL[0], dun = unR - unL;
   // wave strengths
   const T a1 = (dp - rho * a * dun) / (T(2) * a2);
   const T a3 = (dp + rho * a * dun) / (T(2) * a2);

@@ -238,6 +238,13 @@ class FRSolver:
         V = self.nvars
         return {"linf": out[:V], "l1": out[V:2 * V], "l2": out[2 * V:]}
 
+    def functionals(self) -> Dict[str, float]:
+        """FP64 volume integrals of the current state (report_turbulent_stats):
+        kinetic energy, enstrophy (Navier-Stokes) and volume."""
+        out = np.zeros(4)
+        check(lib().zb_functionals(self.h, out.ctypes.data_as(_DP)))
+        return {"ke": float(out[0]), "enstrophy": float(out[1]), "volume": float(out[2])}
+
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().zb_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
 
