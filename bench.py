@@ -178,6 +178,26 @@ def kernel_profile(s, K: int):
     return {k: {"ms_avg": v[0] / max(v[1], 1), "launches": v[1], "ms_total": v[0]} for k, v in prof.items()}
 
 
+def time_adjoint(s, U, K: int, W: int):
+    """Per-kernel CUDA-event time of one adjoint application (zb_vjp on device
+    tensors) at the state U: traces, lift, volume/face pass, trace pass."""
+    import torch
+    s.set_state(U)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    lam = torch.randn(s.state_shape, dtype=torch.float64, device="cuda", generator=g)
+    for _ in range(max(W, 1)):
+        s.vjp(lam)
+    s.profile(True)
+    s.profile_read()
+    for _ in range(K):
+        s.vjp(lam)
+    prof = s.profile_read()
+    s.profile(False)
+    names = ("k_extrap", "k_adj_lift", "k_adj_vol", "k_adj_trace")
+    kern = {k: {"ms_avg": prof[k][0] / max(prof[k][1], 1), "launches": prof[k][1]} for k in names if prof[k][1]}
+    return {"ms_per_vjp": sum(v["ms_avg"] for v in kern.values()), "kernels": kern}
+
+
 def time_rk_stage(s, K: int, world: int):
     import torch
     for st in range(4):
@@ -279,6 +299,7 @@ def gpu_arm(args):
             launches = nl
         prof = kernel_profile(s, K)
         rk = time_rk_stage(s, K, world)
+        adj = time_adjoint(s, U, K, W) if form == "fp64" else None
         R = None
         if rank == 0:
             s.set_state(U)
@@ -294,7 +315,7 @@ def gpu_arm(args):
             ke.append(s.functionals()["ke"])
             s.step(10)
         ke.append(s.functionals()["ke"])
-        forms[form] = {"ms": ms, "prof": prof, "rk": rk, "R": R, "ke": np.array(ke)}
+        forms[form] = {"ms": ms, "prof": prof, "rk": rk, "R": R, "ke": np.array(ke), "adj": adj}
         s.close()
         del s
         torch.cuda.empty_cache()
@@ -352,6 +373,12 @@ def gpu_arm(args):
                  "rk_stage_ms": rk_fp64, "kernels": prof_fp64,
                  "roofline_frac_of_measured": b64 / (t_res64 * 1e-3) / 1e9 / peak},
         "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "adjoint": {"form": "FP64", "ms_per_vjp": forms["fp64"]["adj"]["ms_per_vjp"],
+                    "forward_residual_ms": t_res64,
+                    "adjoint_over_forward": forms["fp64"]["adj"]["ms_per_vjp"] / t_res64,
+                    "kernels": forms["fp64"]["adj"]["kernels"],
+                    "note": "kernel time of one (d divF/dU)^T lam at the TGV state vs one FP64 residual "
+                            "(the same kernels' CUDA-event times)"},
         "mixed_ke_history_rel_err_vs_fp64": ke_err,
         "mixed_dissipation_rel_err_vs_fp64": eps_err,
         "mixed_residual_rel_l2_err_vs_fp64": err,

@@ -88,7 +88,11 @@ enum {
   ZB_K_TO_TILES = 4,   /* state import */
   ZB_K_FROM_TILES = 5, /* state / residual export */
   ZB_K_NORMS = 6,      /* FP64 residual norms */
-  ZB_NKERNELS = 8
+  ZB_K_ADJ_LIFT = 7,   /* adjoint: residual weight -> surface flux weight */
+  ZB_K_ADJ_VOL = 8,    /* adjoint: volume + face fluxes (+ gradient, NS) */
+  ZB_K_ADJ_TRACE = 9,  /* adjoint NS: common solution -> traces -> state */
+  ZB_K_FUNCTIONALS = 10,
+  ZB_NKERNELS = 11
 };
 
 typedef struct zb_mesh {
@@ -215,6 +219,23 @@ zb_status zb_residual_norms(zb_ctx *ctx, double *out);
  * out[2] = domain volume.  The reference prints out[0..1] / (out[2] rho_fs
  * |V_fs|^2). */
 zb_status zb_functionals(zb_ctx *ctx, double *out);
+
+/* Replace the free-stream state the far-field and characteristic boundaries
+ * prescribe (input rho_fs, V_fs, P_fs of the reference, src/input.cpp:463-539
+ * after non-dimensionalisation); takes effect from the next launch.  Used to
+ * differentiate with respect to the free-stream conditions.  No reference
+ * counterpart (the reference fixes them at set-up). */
+zb_status zb_set_freestream(zb_ctx *ctx, double rho_fs, const double *V_fs, double P_fs);
+
+/* Adjoint (vector-Jacobian product) of the residual at the current state:
+ * Ubar = (d divF / d U)^T lam, both in the strided layout of zb_set_state,
+ * divF as zb_compute_residual computes it.  param_bar, when not NULL,
+ * receives d (lam . divF) / d (rho_fs, V_fs[0..2], P_fs), the free-stream
+ * state the far-field and characteristic boundaries prescribe (5 doubles).
+ * Plain FP64 contexts only; quadrilaterals P1-P5 and hexahedra P1-P3.
+ * No reference counterpart: the reference has no adjoint. */
+zb_status zb_vjp(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride, int64_t var_stride,
+                 int64_t ele_stride, int where, double *param_bar);
 
 /* Wait for all work queued on the context's stream. */
 zb_status zb_synchronize(zb_ctx *ctx);

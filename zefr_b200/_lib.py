@@ -33,9 +33,9 @@ EXPORTED = [
     "zb_destroy", "zb_info_get", "zb_set_stream", "zb_set_dt", "zb_set_state", "zb_get_state",
     "zb_compute_residual", "zb_get_residual", "zb_rk_stage", "zb_step", "zb_residual_norms",
     "zb_synchronize", "zb_launch_count", "zb_profile_enable", "zb_profile_read", "zb_kernel_name",
-    "zb_compute_residual_noalloc", "zb_functionals",
+    "zb_compute_residual_noalloc", "zb_functionals", "zb_vjp", "zb_set_freestream",
 ]
-ZB_NKERNELS = 8
+ZB_NKERNELS = 11
 
 
 class ZbMesh(ctypes.Structure):
@@ -127,6 +127,8 @@ def lib() -> ctypes.CDLL:
         L.zb_kernel_name.argtypes = [ctypes.c_int]
         L.zb_compute_residual_noalloc.argtypes = [vp, dp, dp, vp]
         L.zb_functionals.argtypes = [vp, dp]
+        L.zb_set_freestream.argtypes = [vp, ctypes.c_double, dp, ctypes.c_double]
+        L.zb_vjp.argtypes = [vp, dp, dp, i64, i64, i64, ctypes.c_int, dp]
         _lib = L
     return _lib
 

@@ -1,0 +1,169 @@
+"""PyTorch autograd over the DFR residual and RK44 trajectories.
+
+``residual(U, solver)`` is a differentiable residual: its backward calls the
+library's hand-written adjoint (``zb_vjp``), never a PyTorch trace of the
+kernels.  ``TrajectoryAdjoint`` differentiates a time-averaged objective over
+RK44 steps (``FRSolver::step_RK`` with the RK44 tables of src/solver.cpp:
+722-735) with respect to the initial state and the free-stream state, storing
+a checkpoint every ``checkpoint_every`` steps and recomputing the stage states
+of each segment during the reverse sweep.
+
+Everything is plain FP64 on the device: the adjoint exists for ZB_FP64
+contexts only.
+"""
+from __future__ import annotations
+
+from typing import Callable, Dict, List, Optional, Tuple
+
+import numpy as np
+import torch
+
+from .solver import FRSolver
+
+# RK44 of FRSolver::step_RK: stage states U_{s+1} = U_0 - a_s dt/|J| R_s,
+# update U_new = U_0 - dt/|J| sum_s b_s R_s
+RK_ALPHA = (0.5, 0.5, 1.0)
+RK_BETA = (1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0)
+
+
+class _Residual(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, U: torch.Tensor, solver: FRSolver, stage: int):
+        solver.set_state(U)
+        solver.compute_residual(stage)
+        R = torch.empty_like(U)
+        solver.get_residual_device(R, stage)
+        ctx.solver = solver
+        ctx.save_for_backward(U)
+        return R
+
+    @staticmethod
+    def backward(ctx, gR: torch.Tensor):
+        (U,) = ctx.saved_tensors
+        ctx.solver.set_state(U)
+        return ctx.solver.vjp(gR.contiguous()), None, None
+
+
+def residual(U: torch.Tensor, solver: FRSolver, stage: int = 0) -> torch.Tensor:
+    """divF(U) in the reference layout [spt][var][ele] (float64 CUDA tensor),
+    differentiable with respect to U through the library's adjoint."""
+    if U.dtype != torch.float64 or not U.is_cuda:
+        raise TypeError("residual() takes a float64 CUDA tensor")
+    return _Residual.apply(U.contiguous(), solver, stage)
+
+
+def _device_array(solver: FRSolver, name: str, shape) -> torch.Tensor:
+    return torch.from_numpy(solver.plan.get(name).reshape(shape)).cuda()
+
+
+class TrajectoryAdjoint:
+    """Gradient of J = (1/n) sum_{k=1..n} j(U_k) over n RK44 steps.
+
+    ``objective(U) -> scalar tensor`` is any differentiable torch function of
+    the state (e.g. :func:`kinetic_energy`); its state gradient comes from
+    torch autograd, the residual's from the library adjoint.  The free-stream
+    gradient covers rho_fs, V_fs[0..2], P_fs.
+    """
+
+    def __init__(self, solver: FRSolver, dt: float, checkpoint_every: int = 50):
+        self.s = solver
+        self.dt = float(dt)
+        self.every = int(checkpoint_every)
+        S, V, E = solver.state_shape
+        self.inv_det = (1.0 / _device_array(solver, "jaco_det_spts", (S, E))).reshape(S, 1, E)
+        solver.set_dt(self.dt)
+
+    # -- forward pieces --
+    def _residual(self, U: torch.Tensor) -> torch.Tensor:
+        self.s.set_state(U)
+        self.s.compute_residual(0)
+        R = torch.empty_like(U)
+        self.s.get_residual_device(R, 0)
+        return R
+
+    def _stages(self, U0: torch.Tensor) -> Tuple[List[torch.Tensor], torch.Tensor]:
+        """Stage states U^(0..3) of one RK44 step and the updated state."""
+        Us, Rs = [U0], []
+        for s in range(4):
+            Rs.append(self._residual(Us[s]))
+            if s < 3:
+                Us.append(U0 - RK_ALPHA[s] * self.dt * self.inv_det * Rs[s])
+        Unew = U0.clone()
+        for s in range(4):
+            Unew = Unew - RK_BETA[s] * self.dt * self.inv_det * Rs[s]
+        return Us, Unew
+
+    def _step(self, U: torch.Tensor) -> torch.Tensor:
+        return self._stages(U)[1]
+
+    # -- reverse pieces --
+    def _vjp(self, U: torch.Tensor, lam: torch.Tensor, pbar: np.ndarray) -> torch.Tensor:
+        self.s.set_state(U)
+        g, p = self.s.vjp(lam.contiguous(), params=True)
+        pbar += p
+        return g
+
+    def _step_adjoint(self, U0: torch.Tensor, Ubar_new: torch.Tensor, pbar: np.ndarray) -> torch.Tensor:
+        Us, _ = self._stages(U0)
+        Ubar0 = Ubar_new.clone()
+        Rbar = [-RK_BETA[s] * self.dt * self.inv_det * Ubar_new for s in range(4)]
+        for s in range(3, 0, -1):
+            Ubar_s = self._vjp(Us[s], Rbar[s], pbar)
+            Ubar0 += Ubar_s
+            Rbar[s - 1] = Rbar[s - 1] - RK_ALPHA[s - 1] * self.dt * self.inv_det * Ubar_s
+        Ubar0 += self._vjp(Us[0], Rbar[0], pbar)
+        return Ubar0
+
+    @staticmethod
+    def _obj_grad(objective: Callable, U: torch.Tensor) -> Tuple[float, torch.Tensor]:
+        x = U.detach().clone().requires_grad_(True)
+        j = objective(x)
+        (g,) = torch.autograd.grad(j, x)
+        return float(j.detach()), g
+
+    def run(self, U0, nsteps: int, objective: Callable) -> Dict[str, object]:
+        """Returns J, dJ/dU0 (CUDA tensor) and dJ/d(rho_fs, V_fs[0..2], P_fs)."""
+        U = torch.as_tensor(U0, dtype=torch.float64).cuda().contiguous()
+        checkpoints = {0: U.clone()}
+        J = 0.0
+        with torch.no_grad():
+            for k in range(1, nsteps + 1):
+                U = self._step(U)
+                J += float(objective(U))
+                if k % self.every == 0:
+                    checkpoints[k] = U.clone()
+        J /= nsteps
+        # reverse sweep, one checkpointed segment at a time from the end
+        Ubar = torch.zeros_like(U)
+        pbar = np.zeros(5)
+        starts = [k for k in sorted(checkpoints) if k < nsteps]
+        for i in range(len(starts) - 1, -1, -1):
+            k0 = starts[i]
+            k1 = starts[i + 1] if i + 1 < len(starts) else nsteps
+            # states[m] = U_{k0+m}, recomputed from the checkpoint
+            states = [checkpoints[k0]]
+            for _ in range(k0 + 1, k1):
+                states.append(self._step(states[-1]))
+            for m in range(k1 - k0 - 1, -1, -1):
+                if m + 1 < len(states):
+                    Unext = states[m + 1]
+                else:
+                    Unext = checkpoints[k1] if k1 in checkpoints else self._step(states[m])
+                Ubar = Ubar + self._obj_grad(objective, Unext)[1] / nsteps
+                Ubar = self._step_adjoint(states[m], Ubar, pbar)
+        return {"J": J, "dJ_dU0": Ubar, "dJ_dfreestream": pbar}
+
+
+def kinetic_energy(solver: FRSolver) -> Callable[[torch.Tensor], torch.Tensor]:
+    """Volume integral of 1/2 rho |u|^2 (report_turbulent_stats,
+    src/solver.cpp:7813-7917) as a torch function of the state."""
+    S, V, E = solver.state_shape
+    jw = (_device_array(solver, "jaco_det_spts", (S, E)) *
+          torch.from_numpy(solver.plan.get("weights_spts")).cuda().reshape(S, 1))
+
+    def f(U: torch.Tensor) -> torch.Tensor:
+        rho = U[:, 0, :]
+        m2 = (U[:, 1:V - 1, :] ** 2).sum(dim=1)
+        return (jw * 0.5 * m2 / rho).sum()
+
+    return f

@@ -1,0 +1,79 @@
+// Adjoint launches (plain FP64 form): kernel instantiations live in their own
+// translation unit so they build in parallel with the forward kernels.
+#include "ctx_impl.cuh"
+#include "adjoint.cuh"
+
+namespace zb {
+
+using dev::LineOpsT;
+using dev::Shape;
+using dev::TW;
+
+// Adjoint of the residual (plain FP64 form): lift, then the volume/face
+// pass, then for Navier-Stokes the common-solution pass.
+template <int D, int N>
+static void launch_vjp_impl(Ctx &c, bool params)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V, NT = G::NT;
+  dev::AdjArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.U = (const double *)c.U;
+  a.Ufp = (const double *)c.Ufp[c.cur];
+  a.mets = (const double *)c.mets;
+  a.fgeo = (const double *)c.fgeo;
+  a.nbr = c.nbr;
+  a.lam = c.lam;
+  a.Lfp = c.Lfp;
+  a.Ubfp = c.Ubfp;
+  a.dUbfp = c.dUbfp;
+  a.UCb = c.UCb;
+  a.Ubar = c.Ubar;
+  a.pbar = params ? c.pbar : nullptr;
+  a.ntiles = c.ntiles;
+  a.ph = phys_of<double>(c.plan.params, c.uref, D, false);
+  const LineOpsT<double, N> ops = line_ops<double, N>(c.plan);
+  {
+    ProfScope ps(c, ZB_K_ADJ_LIFT);
+    dev::k_adj_lift<D, N><<<grid_for(c.ntiles * Fp * TW, 256), 256, 0, c.stream>>>(a, ops);
+    c.launches++;
+    CK(cudaGetLastError());
+  }
+  if (!c.plan.params.viscous)
+  {
+    const size_t smem = (size_t)(S * V + Fp * V) * TW * sizeof(double);
+    set_smem(dev::k_adj_euler<D, N>, smem);
+    ProfScope ps(c, ZB_K_ADJ_VOL);
+    dev::k_adj_euler<D, N><<<(unsigned)c.ntiles, NT, smem, c.stream>>>(a, ops);
+    c.launches++;
+    CK(cudaGetLastError());
+    return;
+  }
+  const size_t smem1 = (size_t)(2 * S * V + Fp * V + 2 * D * S * V) * TW * sizeof(double);
+  set_smem(dev::k_adj_ns1<D, N>, smem1);
+  {
+    ProfScope ps(c, ZB_K_ADJ_VOL);
+    dev::k_adj_ns1<D, N><<<(unsigned)c.ntiles, NT, smem1, c.stream>>>(a, ops);
+    c.launches++;
+    CK(cudaGetLastError());
+  }
+  const size_t smem2 = (size_t)Fp * V * TW * sizeof(double);
+  set_smem(dev::k_adj_ns2<D, N>, smem2);
+  ProfScope ps(c, ZB_K_ADJ_TRACE);
+  dev::k_adj_ns2<D, N><<<(unsigned)c.ntiles, NT, smem2, c.stream>>>(a, ops);
+  c.launches++;
+  CK(cudaGetLastError());
+}
+
+void bind_vjp(Ctx &c)
+{
+  // the adjoint's shared memory fits hexahedra up to P3
+#define ZB_BIND(DD, NN) \
+  if (c.D == DD && c.N == NN) { c.launch_vjp = &launch_vjp_impl<DD, NN>; return; }
+  ZB_BIND(2, 2) ZB_BIND(2, 3) ZB_BIND(2, 4) ZB_BIND(2, 5) ZB_BIND(2, 6)
+  ZB_BIND(3, 2) ZB_BIND(3, 3) ZB_BIND(3, 4)
+#undef ZB_BIND
+  c.launch_vjp = nullptr;
+}
+
+}  // namespace zb

@@ -1,0 +1,985 @@
+// Adjoint (vector-Jacobian product) of the DFR residual, plain FP64 form.
+//
+// For a weight lam on the residual divF(U) of FRSolver::compute_residual
+// (src/solver.cpp:1494-1645) the kernels return Ubar = (d divF / d U)^T lam.
+// The reverse pass mirrors the forward kernels of dfr_kernels.cuh:
+//   - every line operator is applied transposed (Dm^T, Em^T, the surface
+//     lifting coefficients -Dbm / Dbp transposed into a flux point weight);
+//   - face coupling is gathered, never scattered: both elements of a face pair
+//     evaluate the vector-Jacobian product of the common flux with the summed
+//     weight of both sides and keep the part for their own trace, so no
+//     atomics are needed and the result is deterministic;
+//   - pointwise Jacobian-transpose products are hand-written reverse mode for
+//     the volume fluxes (flux_conv_vjp, flux_visc_vjp) and forward-mode dual
+//     numbers (dual.cuh) for the Riemann solvers, boundary ghost states and
+//     gradients, which run on flux points only.
+// Navier-Stokes needs three passes because the LDG common solution couples the
+// gradient of one element to the trace of its neighbour.
+#pragma once
+
+#include "dfr_kernels.cuh"
+#include "dual.cuh"
+
+namespace zb {
+namespace dev {
+
+// ---------------------------------------------------------------------------
+// Pointwise reverse mode (restating the forward functions of physics.cuh)
+// ---------------------------------------------------------------------------
+
+// Ub += (d F / d U)^T Fb for the inviscid flux F[var][dim] of flux_conv.
+template <int D>
+ZB_HD void flux_conv_vjp(const double U[D + 2], const double Fb[D + 2][D], double gamma, double Ub[D + 2])
+{
+  constexpr int V = D + 2;
+  const double ir = 1.0 / U[0];
+  double u[D], m2 = 0.0;
+  for (int k = 0; k < D; k++)
+  {
+    u[k] = U[k + 1] * ir;
+    m2 += U[k + 1] * U[k + 1];
+  }
+  const double q = 0.5 * m2 * ir;
+  const double P = (gamma - 1.0) * (U[V - 1] - q);
+  const double H = (U[V - 1] + P) * ir;
+  double mb[D], ub[D], Pb = 0.0, Hb = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    double s = Fb[0][d] + Fb[V - 1][d] * H;
+    for (int k = 0; k < D; k++) s += Fb[k + 1][d] * u[k];
+    mb[d] = s;
+    Hb += Fb[V - 1][d] * U[d + 1];
+    Pb += Fb[d + 1][d];
+  }
+  for (int k = 0; k < D; k++)
+  {
+    double s = 0.0;
+    for (int d = 0; d < D; d++) s += Fb[k + 1][d] * U[d + 1];
+    ub[k] = s;
+  }
+  double Eb = Hb * ir;
+  Pb += Hb * ir;
+  double irb = Hb * (U[V - 1] + P);
+  Eb += (gamma - 1.0) * Pb;
+  const double qb = -(gamma - 1.0) * Pb;
+  irb += qb * 0.5 * m2;
+  for (int k = 0; k < D; k++)
+  {
+    mb[k] += qb * u[k] + ub[k] * ir;
+    irb += ub[k] * U[k + 1];
+  }
+  Ub[0] += -irb * ir * ir;
+  for (int k = 0; k < D; k++) Ub[k + 1] += mb[k];
+  Ub[V - 1] += Eb;
+}
+
+// (Ub, dUb) += (d F / d (U, dU))^T Fb for the viscous contribution that
+// flux_visc_add adds to F (include/flux.hpp:71-202).
+template <int D>
+ZB_HD void flux_visc_vjp(const double U[D + 2], const double dU[D + 2][D], const double Fb[D + 2][D],
+                         const Phys<double> &ph, double Ub[D + 2], double dUb[D + 2][D])
+{
+  constexpr int V = D + 2;
+  const double g = ph.gamma;
+  // forward recomputation
+  const double ir = 1.0 / U[0];
+  double vel[D], vsq = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    vel[d] = U[d + 1] * ir;
+    vsq += vel[d] * vel[d];
+  }
+  const double e_int = U[V - 1] * ir - 0.5 * vsq;
+  double mu, rr = 0.0;
+  if (ph.fix_vis)
+    mu = ph.mu;
+  else
+  {
+    rr = (g - 1.0) * e_int / ph.rt;
+    mu = ph.mu * pow(rr, 1.5) * (1.0 + ph.c_sth) / (rr + ph.c_sth);
+  }
+  double dvel[D][D];
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++) dvel[i][j] = (dU[i + 1][j] - dU[0][j] * vel[i]) * ir;
+  double sj[D], dke[D], de[D];
+  for (int j = 0; j < D; j++)
+  {
+    double s = 0.0;
+    for (int i = 0; i < D; i++) s += vel[i] * dvel[i][j];
+    sj[j] = s;
+    dke[j] = 0.5 * vsq * dU[0][j] + U[0] * s;
+    de[j] = (dU[V - 1][j] - dke[j] - dU[0][j] * e_int) * ir;
+  }
+  double div = 0.0;
+  for (int d = 0; d < D; d++) div += dvel[d][d];
+  const double diag = div / 3.0;
+  double tau[D][D];
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++)
+      tau[i][j] = (i == j) ? 2.0 * mu * (dvel[i][i] - diag) : mu * (dvel[i][j] + dvel[j][i]);
+  const double kappa = (mu / ph.prandtl) * g;
+  // reverse
+  double taub[D][D], velb[D], dvelb[D][D], deb[D];
+  double mub = 0.0, kappab = 0.0, diagb = 0.0, irb = 0.0, rhob = 0.0, e_intb = 0.0, vsqb = 0.0;
+  for (int i = 0; i < D; i++)
+  {
+    velb[i] = 0.0;
+    for (int j = 0; j < D; j++)
+    {
+      taub[i][j] = -Fb[i + 1][j] - Fb[V - 1][j] * vel[i];
+      velb[i] -= Fb[V - 1][j] * tau[i][j];
+      dvelb[i][j] = 0.0;
+    }
+  }
+  for (int j = 0; j < D; j++)
+  {
+    kappab -= Fb[V - 1][j] * de[j];
+    deb[j] = -Fb[V - 1][j] * kappa;
+  }
+  mub += kappab * g / ph.prandtl;
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++)
+    {
+      if (i == j)
+      {
+        mub += taub[i][i] * 2.0 * (dvel[i][i] - diag);
+        dvelb[i][i] += 2.0 * mu * taub[i][i];
+        diagb -= 2.0 * mu * taub[i][i];
+      }
+      else
+      {
+        mub += taub[i][j] * (dvel[i][j] + dvel[j][i]);
+        dvelb[i][j] += mu * taub[i][j];
+        dvelb[j][i] += mu * taub[i][j];
+      }
+    }
+  for (int d = 0; d < D; d++) dvelb[d][d] += diagb / 3.0;
+  for (int j = 0; j < D; j++)
+  {
+    const double X = dU[V - 1][j] - dke[j] - dU[0][j] * e_int;
+    const double Xb = deb[j] * ir;
+    irb += deb[j] * X;
+    dUb[V - 1][j] += Xb;
+    const double dkeb = -Xb;
+    dUb[0][j] -= Xb * e_int;
+    e_intb -= Xb * dU[0][j];
+    vsqb += 0.5 * dkeb * dU[0][j];
+    dUb[0][j] += 0.5 * vsq * dkeb;
+    rhob += dkeb * sj[j];
+    const double sb = dkeb * U[0];
+    for (int i = 0; i < D; i++)
+    {
+      velb[i] += sb * dvel[i][j];
+      dvelb[i][j] += sb * vel[i];
+    }
+  }
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++)
+    {
+      const double Y = dU[i + 1][j] - dU[0][j] * vel[i];
+      const double Yb = dvelb[i][j] * ir;
+      irb += dvelb[i][j] * Y;
+      dUb[i + 1][j] += Yb;
+      dUb[0][j] -= Yb * vel[i];
+      velb[i] -= Yb * dU[0][j];
+    }
+  if (!ph.fix_vis)
+  {
+    // d mu / d r = mu (1.5 / r - 1 / (r + c))
+    const double rb = mub * mu * (1.5 / rr - 1.0 / (rr + ph.c_sth));
+    e_intb += rb * (g - 1.0) / ph.rt;
+  }
+  Ub[V - 1] += e_intb * ir;
+  irb += e_intb * U[V - 1];
+  vsqb -= 0.5 * e_intb;
+  for (int i = 0; i < D; i++)
+  {
+    velb[i] += 2.0 * vsqb * vel[i];
+    Ub[i + 1] += velb[i] * ir;
+    irb += velb[i] * U[i + 1];
+  }
+  rhob -= irb * ir * ir;
+  Ub[0] += rhob;
+}
+
+// Common convective flux of a face as a function of (UL, UR); boundary faces
+// (bc >= 0) take UR from the ghost state of UL.
+template <int D, typename X>
+ZB_HD void conv_face(int bc, const X UL[D + 2], const X URin[D + 2], const X n[D], X Fc[D + 2], const Phys<X> &ph)
+{
+  X UR[D + 2];
+  if (bc >= 0)
+  {
+    X UB[D + 2];
+    ghost_state<X, D>(bc, UL, n, UR, UB, ph);
+  }
+  else
+    for (int v = 0; v < D + 2; v++) UR[v] = URin[v];
+  if (ph.fconv == 2)
+    roe<X, D>(UL, UR, n, Fc, ph);
+  else
+    rusanov<X, D>(UL, UR, n, Fc, ph);
+}
+
+// Ub_own += (d Fc / d U_own)^T w for an interior face (own = left or right).
+template <int D>
+ZB_HD void conv_face_vjp_side(const double UL[D + 2], const double UR[D + 2], const double n[D], const double w[D + 2],
+                              bool own_left, const Phys<Dual<double>> &pd, double Ub[D + 2])
+{
+  constexpr int V = D + 2;
+  using DD = Dual<double>;
+  DD nd[D];
+  for (int d = 0; d < D; d++) nd[d] = DD(n[d]);
+  for (int k = 0; k < V; k++)
+  {
+    DD L[V], R[V], F[V];
+    for (int v = 0; v < V; v++)
+    {
+      L[v] = DD(UL[v], (own_left && v == k) ? 1.0 : 0.0);
+      R[v] = DD(UR[v], (!own_left && v == k) ? 1.0 : 0.0);
+    }
+    conv_face<D, DD>(-1, L, R, nd, F, pd);
+    double acc = 0.0;
+    for (int v = 0; v < V; v++) acc += w[v] * F[v].d;
+    Ub[k] += acc;
+  }
+}
+
+// Viscous normal flux of one trace (visc_normal) and its reverse:
+// (Ub, dUb) += (d (F_visc(U, dU) . n) / d (U, dU))^T w.
+template <int D>
+ZB_HD void visc_normal_vjp(const double U[D + 2], const double dU[D + 2][D], const double n[D], const double w[D + 2],
+                           const Phys<double> &ph, double Ub[D + 2], double dUb[D + 2][D])
+{
+  double Fb[D + 2][D];
+  for (int v = 0; v < D + 2; v++)
+    for (int d = 0; d < D; d++) Fb[v][d] = w[v] * n[d];
+  flux_visc_vjp<D>(U, dU, Fb, ph, Ub, dUb);
+}
+
+// Boundary face, everything the own trace (U, dU) feeds:
+//   convective common flux with the ghost state, plus for viscous runs
+//   F_visc(UB, ghost_grad(U, dU)) . n + tau (U - UB).
+template <int D, bool VISC>
+ZB_HD void bnd_face_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+                        const double w[D + 2], const Phys<Dual<double>> &pd, double Ub[D + 2], double dUb[D + 2][D])
+{
+  constexpr int V = D + 2;
+  using DD = Dual<double>;
+  constexpr int NI = VISC ? V + V * D : V;
+  DD nd[D];
+  for (int d = 0; d < D; d++) nd[d] = DD(n[d]);
+  for (int k = 0; k < NI; k++)
+  {
+    DD L[V], dL[V][D], F[V];
+    for (int v = 0; v < V; v++)
+    {
+      L[v] = DD(U[v], v == k ? 1.0 : 0.0);
+      for (int d = 0; d < D; d++) dL[v][d] = DD(dU[v][d], (k == V + v * D + d) ? 1.0 : 0.0);
+    }
+    conv_face<D, DD>(bc, L, L, nd, F, pd);
+    if (VISC)
+    {
+      DD UR[V], UB[V], dUB[V][D], Fn[V];
+      ghost_state<DD, D>(bc, L, nd, UR, UB, pd);
+      ghost_grad<DD, D>(bc, L, dL, nd, dUB);
+      visc_normal<DD, D>(UB, dUB, nd, Fn, pd);
+      for (int v = 0; v < V; v++) F[v] += Fn[v] + pd.ldg_tau * (L[v] - UB[v]);
+    }
+    double acc = 0.0;
+    for (int v = 0; v < V; v++) acc += w[v] * F[v].d;
+    if (k < V)
+      Ub[k] += acc;
+    else
+      dUb[(k - V) / D][(k - V) % D] += acc;
+  }
+}
+
+// Ub += (d UB / d U)^T w for the prescribed boundary state UB of the LDG
+// common solution.
+template <int D>
+ZB_HD void bnd_ucomm_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+                         const Phys<Dual<double>> &pd, double Ub[D + 2])
+{
+  constexpr int V = D + 2;
+  using DD = Dual<double>;
+  DD nd[D];
+  for (int d = 0; d < D; d++) nd[d] = DD(n[d]);
+  for (int k = 0; k < V; k++)
+  {
+    DD L[V], UR[V], UB[V];
+    for (int v = 0; v < V; v++) L[v] = DD(U[v], v == k ? 1.0 : 0.0);
+    ghost_state<DD, D>(bc, L, nd, UR, UB, pd);
+    double acc = 0.0;
+    for (int v = 0; v < V; v++) acc += w[v] * UB[v].d;
+    Ub[k] += acc;
+  }
+}
+
+// Free-stream parameters a boundary state depends on: k = 0 rho_fs,
+// 1..3 V_fs[k-1], 4 P_fs.  Only far-field (3) and characteristic (2) faces.
+ZB_HD bool bc_uses_freestream(int bc) { return bc == 2 || bc == 3; }
+
+ZB_HD void seed_param(Phys<Dual<double>> &q, int k)
+{
+  if (k == 0)
+    q.rho_fs.d = 1.0;
+  else if (k <= 3)
+    q.V_fs[k - 1].d = 1.0;
+  else
+    q.P_fs.d = 1.0;
+}
+
+// pb[k] += d (w . phi) / d param_k for the boundary face function of
+// bnd_face_vjp.
+template <int D, bool VISC>
+ZB_HD void bnd_face_param_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+                              const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
+{
+  constexpr int V = D + 2;
+  using DD = Dual<double>;
+  if (!bc_uses_freestream(bc)) return;
+  DD nd[D], L[V], dL[V][D];
+  for (int d = 0; d < D; d++) nd[d] = DD(n[d]);
+  for (int v = 0; v < V; v++)
+  {
+    L[v] = DD(U[v]);
+    for (int d = 0; d < D; d++) dL[v][d] = DD(dU[v][d]);
+  }
+  for (int k = 0; k < 5; k++)
+  {
+    if (k >= 1 && k <= 3 && k > D) continue;
+    Phys<DD> q = pd;
+    seed_param(q, k);
+    DD F[V];
+    conv_face<D, DD>(bc, L, L, nd, F, q);
+    if (VISC)
+    {
+      DD UR[V], UB[V], dUB[V][D], Fn[V];
+      ghost_state<DD, D>(bc, L, nd, UR, UB, q);
+      ghost_grad<DD, D>(bc, L, dL, nd, dUB);
+      visc_normal<DD, D>(UB, dUB, nd, Fn, q);
+      for (int v = 0; v < V; v++) F[v] += Fn[v] + q.ldg_tau * (L[v] - UB[v]);
+    }
+    double acc = 0.0;
+    for (int v = 0; v < V; v++) acc += w[v] * F[v].d;
+    pb[k] += acc;
+  }
+}
+
+// pb[k] += d (w . UB) / d param_k for the LDG boundary common solution.
+template <int D>
+ZB_HD void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+                               const Phys<Dual<double>> &pd, double pb[5])
+{
+  constexpr int V = D + 2;
+  using DD = Dual<double>;
+  if (!bc_uses_freestream(bc)) return;
+  DD nd[D], L[V];
+  for (int d = 0; d < D; d++) nd[d] = DD(n[d]);
+  for (int v = 0; v < V; v++) L[v] = DD(U[v]);
+  for (int k = 0; k < 5; k++)
+  {
+    if (k >= 1 && k <= 3 && k > D) continue;
+    Phys<DD> q = pd;
+    seed_param(q, k);
+    DD UR[V], UB[V];
+    ghost_state<DD, D>(bc, L, nd, UR, UB, q);
+    double acc = 0.0;
+    for (int v = 0; v < V; v++) acc += w[v] * UB[v].d;
+    pb[k] += acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+
+// Deterministic block sum of pb[5] into out[5] (fixed shuffle and warp order).
+__device__ __forceinline__ void block_sum5(double pb[5], double *out)
+{
+  __shared__ double red[32][5];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 5; k++)
+  {
+    double x = pb[k];
+    for (int o = 16; o > 0; o /= 2) x += __shfl_down_sync(0xffffffff, x, o);
+    if (lane == 0) red[warp][k] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 5)
+  {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w][threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+}
+
+struct AdjArgs
+{
+  const double *U;     // [tile][S][V][TW] state the residual is linearised at
+  const double *Ufp;   // [tile][Fp][V][TW] its extrapolation
+  const double *mets;  // [tile][S][NM][TW]
+  const double *fgeo;  // [tile][Fp][D+1][TW]
+  const int *nbr;      // [tile][Fp][TW]
+  const double *lam;   // [tile][S][V][TW] weight on the residual
+  double *Lfp;         // [tile][Fp][V][TW] weight on the own-side surface flux
+  double *Ubfp;        // [tile][Fp][V][TW] adjoint of the own trace U_fpts
+  double *dUbfp;       // NS: [tile][Fp][V][D][TW] adjoint of the own gradient trace
+  double *UCb;         // NS: [tile][Fp][V][TW] adjoint of the own common solution
+  double *Ubar;        // [tile][S][V][TW] result
+  double *pbar;        // [ntiles][5] per-tile free-stream adjoint (nullptr: off)
+  int64_t ntiles;
+  Phys<double> ph;
+};
+
+// Weight of the own surface flux point: the transpose of the surface
+// correction of finish_point, Lfp(f) = sum over the line of f of
+// (-Dbm | +Dbp)[m] lam(spt m).
+template <int D, int N>
+__global__ void __launch_bounds__(256) k_adj_lift(const __grid_constant__ AdjArgs a,
+                                                  const __grid_constant__ LineOpsT<double, N> ops)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V;
+  const int64_t total = a.ntiles * Fp * TW;
+  for (int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gid < total; gid += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int l = (int)(gid % TW);
+    const int f = (int)((gid / TW) % Fp);
+    const int64_t tile = gid / ((int64_t)TW * Fp);
+    int dim, side, base, stride;
+    fpt_line<D, N>(f, dim, side, base, stride);
+    const double *Lt = a.lam + tile * (int64_t)S * V * TW;
+    double *out = a.Lfp + (tile * Fp + f) * (int64_t)V * TW;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      double acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < N; m++)
+        acc += (side < 0 ? -ops.Dbm[m] : ops.Dbp[m]) * Lt[((base + m * stride) * V + v) * TW + l];
+      out[v * TW + l] = acc;
+    }
+  }
+}
+
+// Adjoint of the volume flux divergence at solution point s:
+// Fb[v][k] = sum_d adj[d][k] (Dm^T lam)_d[v].
+template <int D, int N>
+__device__ __forceinline__ void vol_weight(const AdjArgs &a, const LineOpsT<double, N> &ops, int64_t tile, int s, int l,
+                                           double Fb[D + 2][D])
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, V = G::V, NM = G::NM;
+  const double *Lt = a.lam + tile * (int64_t)S * V * TW;
+  double Ft[D][V];
+#pragma unroll
+  for (int d = 0; d < D; d++)
+  {
+    int i, fm, fp;
+    spt_ends<D, N>(s, d, i, fm, fp);
+    const int st = pow_n<N>(d);
+    const int b = s - i * st;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      double acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < N; m++) acc += ops.Dm[m * N + i] * Lt[((b + m * st) * V + v) * TW + l];
+      Ft[d][v] = acc;
+    }
+  }
+  const double *mt = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
+#pragma unroll
+  for (int v = 0; v < V; v++)
+#pragma unroll
+    for (int k = 0; k < D; k++)
+    {
+      double acc = 0.0;
+#pragma unroll
+      for (int d = 0; d < D; d++) acc += mt[(d * D + k) * TW] * Ft[d][v];
+      Fb[v][k] = acc;
+    }
+}
+
+// Summed weight on the common flux of the face of own flux point f (both
+// sides' surface terms) and the own-side bookkeeping.
+template <int D, int N>
+__device__ __forceinline__ void face_weight(const AdjArgs &a, int64_t tile, int f, int l, int code, double n[D],
+                                            double w[D + 2])
+{
+  using G = Shape<D, N>;
+  constexpr int Fp = G::Fp, V = G::V;
+  const double *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+  for (int d = 0; d < D; d++) n[d] = g[d * TW];
+  const double dA = g[D * TW];
+  double Lo[V];
+  const double *lo = a.Lfp + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+  for (int v = 0; v < V; v++) Lo[v] = lo[v * TW];
+  if (code < 0)
+  {
+#pragma unroll
+    for (int v = 0; v < V; v++) w[v] = dA * Lo[v];
+    return;
+  }
+  const int pidx = code >> 1;
+  const bool own_left = !(code & 1);
+  double Ln[V];
+  gather_fpt<double, double, V>(a.Lfp, pidx, Ln);
+  const double dAn = a.fgeo[((int64_t)(pidx / TW) * (D + 1) + D) * TW + pidx % TW];
+  const double so = own_left ? dA : -dA, sn = own_left ? -dAn : dAn;
+#pragma unroll
+  for (int v = 0; v < V; v++) w[v] = so * Lo[v] + sn * Ln[v];
+}
+
+// ---------------------------------------------------------------------------
+// Euler: one kernel after k_adj_lift
+// ---------------------------------------------------------------------------
+template <int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_constant__ AdjArgs a,
+                                                               const __grid_constant__ LineOpsT<double, N> ops)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sUb = reinterpret_cast<double *>(smem_raw);  // [S][V][TW]
+  double *sUbfp = sUb + S * V * TW;                     // [Fp][V][TW]
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  const Phys<Dual<double>> pd = dual_phys(a.ph);
+  double pb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    double Fb[V][D], U[V], Ub[V];
+    vol_weight<D, N>(a, ops, tile, s, l, Fb);
+    const double *ut = a.U + (tile * S + s) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      U[v] = ut[v * TW];
+      Ub[v] = 0.0;
+    }
+    flux_conv_vjp<D>(U, Fb, a.ph.gamma, Ub);
+#pragma unroll
+    for (int v = 0; v < V; v++) sUb[(s * V + v) * TW + l] = Ub[v];
+  }
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    const int code = a.nbr[(tile * Fp + f) * (int64_t)TW + l];
+    double n[D], w[V], Uo[V], Ub[V];
+    face_weight<D, N>(a, tile, f, l, code, n, w);
+    const double *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      Uo[v] = uo[v * TW];
+      Ub[v] = 0.0;
+    }
+    if (code >= 0)
+    {
+      double Un[V];
+      gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
+      const bool own_left = !(code & 1);
+      conv_face_vjp_side<D>(own_left ? Uo : Un, own_left ? Un : Uo, n, w, own_left, pd, Ub);
+    }
+    else
+    {
+      double dUz[V][D], dUbz[V][D];
+#pragma unroll
+      for (int v = 0; v < V; v++)
+#pragma unroll
+        for (int d = 0; d < D; d++) dUz[v][d] = dUbz[v][d] = 0.0;
+      bnd_face_vjp<D, false>(-code - 1, Uo, dUz, n, w, pd, Ub, dUbz);
+      if (a.pbar) bnd_face_param_vjp<D, false>(-code - 1, Uo, dUz, n, w, pd, pb);
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) sUbfp[(f * V + v) * TW + l] = Ub[v];
+  }
+  if (a.pbar) block_sum5(pb, a.pbar + tile * 5);
+  __syncthreads();
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    double acc[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) acc[v] = sUb[(s * V + v) * TW + l];
+#pragma unroll
+    for (int d = 0; d < D; d++)
+    {
+      int i, fm, fp;
+      spt_ends<D, N>(s, d, i, fm, fp);
+#pragma unroll
+      for (int v = 0; v < V; v++)
+        acc[v] += ops.Em[i] * sUbfp[(fm * V + v) * TW + l] + ops.Ep[i] * sUbfp[(fp * V + v) * TW + l];
+    }
+    double *out = a.Ubar + (tile * S + s) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) out[v * TW] = acc[v];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Navier-Stokes pass 1: recompute the common solution and gradient, adjoint of
+// the volume flux, of the face fluxes and of the gradient; writes the partial
+// solution-point result, the trace adjoint and the common-solution adjoint.
+// ---------------------------------------------------------------------------
+template <int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_constant__ AdjArgs a,
+                                                             const __grid_constant__ LineOpsT<double, N> ops)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V, NM = G::NM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sU = reinterpret_cast<double *>(smem_raw);  // [S][V][TW]
+  double *sUC = sU + S * V * TW;                       // [Fp][V][TW]
+  double *sUb = sUC + Fp * V * TW;                     // [S][V][TW]
+  double *sdU = sUb + S * V * TW;                      // [D][S][V][TW] physical gradient
+  double *sG = sdU + D * S * V * TW;                   // [D][S][V][TW] its adjoint, then tdU's
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  const Phys<Dual<double>> pd = dual_phys(a.ph);
+  const double beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
+  double pb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  {
+    const double *src = a.U + tile * (int64_t)S * V * TW;
+    for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
+  }
+  // common solution (as k_ns_grad)
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    const int code = a.nbr[(tile * Fp + f) * (int64_t)TW + l];
+    double Uo[V], UC[V];
+    const double *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
+    if (code >= 0)
+    {
+      double Un[V];
+      gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
+      const int slot = code & 1;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+      {
+        const double ul = slot ? Un[v] : Uo[v];
+        const double ur = slot ? Uo[v] : Un[v];
+        if (beta == 0.5)
+          UC[v] = ur;
+        else if (beta == -0.5)
+          UC[v] = ul;
+        else
+          UC[v] = 0.5 * (ul + ur) - beta * (ul - ur);
+      }
+    }
+    else
+    {
+      double n[D], UR[V];
+      const double *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+      for (int d = 0; d < D; d++) n[d] = g[d * TW];
+      ghost_state<double, D>(-code - 1, Uo, n, UR, UC, a.ph);
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) sUC[(f * V + v) * TW + l] = UC[v];
+  }
+  __syncthreads();
+  // physical gradient (as k_ns_grad)
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    double tdU[V][D];
+#pragma unroll
+    for (int d = 0; d < D; d++)
+    {
+      int i, fm, fp;
+      spt_ends<D, N>(s, d, i, fm, fp);
+      const int st = pow_n<N>(d);
+      const int b = s - i * st;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+      {
+        double acc = 0.0;
+#pragma unroll
+        for (int m = 0; m < N; m++) acc += ops.Dm[i * N + m] * sU[((b + m * st) * V + v) * TW + l];
+        const double cm = ops.Dbm[i] * sUC[(fm * V + v) * TW + l];
+        const double cp = ops.Dbp[i] * sUC[(fp * V + v) * TW + l];
+        tdU[v][d] = acc + ((fm < fp) ? (cm + cp) : (cp + cm));
+      }
+    }
+    const double *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
+    const double inv_det = 1.0 / m[D * D * TW];
+#pragma unroll
+    for (int v = 0; v < V; v++)
+#pragma unroll
+      for (int d1 = 0; d1 < D; d1++)
+      {
+        double g = tdU[v][0] * m[(0 * D + d1) * TW];
+#pragma unroll
+        for (int d2 = 1; d2 < D; d2++) g += tdU[v][d2] * m[(d2 * D + d1) * TW];
+        sdU[((d1 * S + s) * V + v) * TW + l] = g * inv_det;
+      }
+  }
+  __syncthreads();
+  // adjoint of the volume flux: U and gradient parts
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    double Fb[V][D], U[V], dU[V][D], Ub[V], dUb[V][D];
+    vol_weight<D, N>(a, ops, tile, s, l, Fb);
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      U[v] = sU[(s * V + v) * TW + l];
+      Ub[v] = 0.0;
+#pragma unroll
+      for (int d = 0; d < D; d++)
+      {
+        dU[v][d] = sdU[((d * S + s) * V + v) * TW + l];
+        dUb[v][d] = 0.0;
+      }
+    }
+    flux_conv_vjp<D>(U, Fb, a.ph.gamma, Ub);
+    flux_visc_vjp<D>(U, dU, Fb, a.ph, Ub, dUb);
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      sUb[(s * V + v) * TW + l] = Ub[v];
+#pragma unroll
+      for (int d = 0; d < D; d++) sG[((d * S + s) * V + v) * TW + l] = dUb[v][d];
+    }
+  }
+  // adjoint of the face fluxes at own flux points
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    const int code = a.nbr[(tile * Fp + f) * (int64_t)TW + l];
+    double n[D], w[V], Uo[V], dUo[V][D], Ub[V], dUb[V][D];
+    face_weight<D, N>(a, tile, f, l, code, n, w);
+    const double *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
+    SOps<double, N> o(reinterpret_cast<const double *>(&ops));
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      Uo[v] = uo[v * TW];
+      Ub[v] = 0.0;
+#pragma unroll
+      for (int d = 0; d < D; d++)
+      {
+        dUo[v][d] = extrap_smem<double, D, N>(sdU + d * S * V * TW, o, f, v, l, V);
+        dUb[v][d] = 0.0;
+      }
+    }
+    if (code >= 0)
+    {
+      double Un[V];
+      gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
+      const bool own_left = !(code & 1);
+      conv_face_vjp_side<D>(own_left ? Uo : Un, own_left ? Un : Uo, n, w, own_left, pd, Ub);
+      // LDG: (1/2 + beta) FnL + (1/2 - beta) FnR + tau (UL - UR)
+      const double c = own_left ? 0.5 + beta : 0.5 - beta;
+      if (c != 0.0)
+      {
+        double wc[V];
+#pragma unroll
+        for (int v = 0; v < V; v++) wc[v] = c * w[v];
+        visc_normal_vjp<D>(Uo, dUo, n, wc, a.ph, Ub, dUb);
+      }
+#pragma unroll
+      for (int v = 0; v < V; v++) Ub[v] += own_left ? tau * w[v] : -tau * w[v];
+    }
+    else
+    {
+      bnd_face_vjp<D, true>(-code - 1, Uo, dUo, n, w, pd, Ub, dUb);
+      if (a.pbar) bnd_face_param_vjp<D, true>(-code - 1, Uo, dUo, n, w, pd, pb);
+    }
+    double *ub = a.Ubfp + (tile * Fp + f) * (int64_t)V * TW + l;
+    double *dub = a.dUbfp + (tile * Fp + f) * (int64_t)V * D * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      ub[v * TW] = Ub[v];
+#pragma unroll
+      for (int d = 0; d < D; d++) dub[(v * D + d) * TW] = dUb[v][d];
+    }
+  }
+  __syncthreads();
+  // gradient adjoint: add the transposed trace extrapolation, then map to
+  // the reference gradient: tdUb[v][d2] = sum_d1 adj[d2][d1] dUb[v][d1] / |J|
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    double g[V][D];
+#pragma unroll
+    for (int v = 0; v < V; v++)
+#pragma unroll
+      for (int d = 0; d < D; d++) g[v][d] = sG[((d * S + s) * V + v) * TW + l];
+#pragma unroll
+    for (int dl = 0; dl < D; dl++)
+    {
+      int i, fm, fp;
+      spt_ends<D, N>(s, dl, i, fm, fp);
+      const double *bm = a.dUbfp + (tile * Fp + fm) * (int64_t)V * D * TW + l;
+      const double *bp = a.dUbfp + (tile * Fp + fp) * (int64_t)V * D * TW + l;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+#pragma unroll
+        for (int d = 0; d < D; d++) g[v][d] += ops.Em[i] * bm[(v * D + d) * TW] + ops.Ep[i] * bp[(v * D + d) * TW];
+    }
+    const double *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
+    const double inv_det = 1.0 / m[D * D * TW];
+#pragma unroll
+    for (int v = 0; v < V; v++)
+#pragma unroll
+      for (int d2 = 0; d2 < D; d2++)
+      {
+        double acc = 0.0;
+#pragma unroll
+        for (int d1 = 0; d1 < D; d1++) acc += m[(d2 * D + d1) * TW] * g[v][d1];
+        sG[((d2 * S + s) * V + v) * TW + l] = acc * inv_det;
+      }
+  }
+  __syncthreads();
+  // U part of the reference gradient: Ub += Dm^T tdUb along each line
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    double acc[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) acc[v] = sUb[(s * V + v) * TW + l];
+#pragma unroll
+    for (int d = 0; d < D; d++)
+    {
+      int i, fm, fp;
+      spt_ends<D, N>(s, d, i, fm, fp);
+      const int st = pow_n<N>(d);
+      const int b = s - i * st;
+#pragma unroll
+      for (int m = 0; m < N; m++)
+      {
+        const double c = ops.Dm[m * N + i];
+#pragma unroll
+        for (int v = 0; v < V; v++) acc[v] += c * sG[((d * S + b + m * st) * V + v) * TW + l];
+      }
+    }
+    double *out = a.Ubar + (tile * S + s) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) out[v * TW] = acc[v];
+  }
+  // common solution part: UCb(f) = sum over the line of (Dbm | Dbp)[m] tdUb
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    int dim, side, base, stride;
+    fpt_line<D, N>(f, dim, side, base, stride);
+    double ucb[V];
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      double acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < N; m++)
+        acc += (side < 0 ? ops.Dbm[m] : ops.Dbp[m]) * sG[((dim * S + base + m * stride) * V + v) * TW + l];
+      ucb[v] = acc;
+    }
+    const int code = a.nbr[(tile * Fp + f) * (int64_t)TW + l];
+    if (code >= 0)
+    {
+      double *out = a.UCb + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+      for (int v = 0; v < V; v++) out[v * TW] = ucb[v];
+    }
+    else
+    {
+      double n[D], Uo[V], Ub[V];
+      const double *g = a.fgeo + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+      for (int d = 0; d < D; d++) n[d] = g[d * TW];
+      const double *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
+      double *ub = a.Ubfp + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+      {
+        Uo[v] = uo[v * TW];
+        Ub[v] = 0.0;
+      }
+      bnd_ucomm_vjp<D>(-code - 1, Uo, n, ucb, pd, Ub);
+      if (a.pbar) bnd_ucomm_param_vjp<D>(-code - 1, Uo, n, ucb, pd, pb);
+#pragma unroll
+      for (int v = 0; v < V; v++) ub[v * TW] += Ub[v];
+    }
+  }
+  if (a.pbar) block_sum5(pb, a.pbar + tile * 5);
+}
+
+// ---------------------------------------------------------------------------
+// Navier-Stokes pass 2: both sides' common-solution adjoints reach the own
+// trace, then the transposed extrapolation finishes Ubar.
+// ---------------------------------------------------------------------------
+template <int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns2(const __grid_constant__ AdjArgs a,
+                                                             const __grid_constant__ LineOpsT<double, N> ops)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sUbfp = reinterpret_cast<double *>(smem_raw);  // [Fp][V][TW]
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  const double beta = a.ph.ldg_b;
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    const int f = it / TW, l = it % TW;
+    const int code = a.nbr[(tile * Fp + f) * (int64_t)TW + l];
+    const double *ub = a.Ubfp + (tile * Fp + f) * (int64_t)V * TW + l;
+    double Ub[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) Ub[v] = ub[v * TW];
+    if (code >= 0)
+    {
+      // UC = (1/2 - beta) UL + (1/2 + beta) UR, shared by both sides
+      const bool own_left = !(code & 1);
+      const double c = own_left ? 0.5 - beta : 0.5 + beta;
+      if (c != 0.0)
+      {
+        double Co[V], Cn[V];
+        const double *co = a.UCb + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+        for (int v = 0; v < V; v++) Co[v] = co[v * TW];
+        gather_fpt<double, double, V>(a.UCb, code >> 1, Cn);
+#pragma unroll
+        for (int v = 0; v < V; v++) Ub[v] += c * (Co[v] + Cn[v]);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) sUbfp[(f * V + v) * TW + l] = Ub[v];
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  {
+    const int s = it / TW, l = it % TW;
+    double *out = a.Ubar + (tile * S + s) * (int64_t)V * TW + l;
+    double acc[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) acc[v] = out[v * TW];
+#pragma unroll
+    for (int d = 0; d < D; d++)
+    {
+      int i, fm, fp;
+      spt_ends<D, N>(s, d, i, fm, fp);
+#pragma unroll
+      for (int v = 0; v < V; v++)
+        acc[v] += ops.Em[i] * sUbfp[(fm * V + v) * TW + l] + ops.Ep[i] * sUbfp[(fp * V + v) * TW + l];
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) out[v * TW] = acc[v];
+  }
+}
+
+}  // namespace dev
+}  // namespace zb

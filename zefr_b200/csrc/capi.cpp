@@ -321,6 +321,24 @@ zb_status zb_functionals(zb_ctx *ctx, double *out)
   })
 }
 
+zb_status zb_set_freestream(zb_ctx *ctx, double rho_fs, const double *V_fs, double P_fs)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && V_fs, "null argument");
+    zb::ctx_set_freestream(ctx->impl, rho_fs, V_fs, P_fs);
+  })
+}
+
+zb_status zb_vjp(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride, int64_t var_stride,
+                 int64_t ele_stride, int where, double *param_bar)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && lam && Ubar, "null argument");
+    ZB_REQUIRE(where == ZB_HOST || where == ZB_DEVICE, "where must be ZB_HOST or ZB_DEVICE");
+    zb::ctx_vjp(ctx->impl, lam, Ubar, spt_stride, var_stride, ele_stride, where, param_bar);
+  })
+}
+
 zb_status zb_synchronize(zb_ctx *ctx)
 {
   ZB_GUARD({
@@ -358,7 +376,8 @@ zb_status zb_compute_residual_noalloc(const zb_plan *plan, const double *U, doub
 const char *zb_kernel_name(int id)
 {
   static const char *names[ZB_NKERNELS] = {"k_extrap", "k_euler", "k_ns_grad", "k_ns_face",
-                                           "k_to_tiles", "k_from_tiles", "k_norms", "unused"};
+                                           "k_to_tiles", "k_from_tiles", "k_norms", "k_adj_lift",
+                                           "k_adj_vol", "k_adj_trace", "k_functionals"};
   return (id >= 0 && id < ZB_NKERNELS) ? names[id] : "unknown";
 }
 

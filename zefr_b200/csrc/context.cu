@@ -1,10 +1,6 @@
 // Device context: buffers in the tile-major layout, layout conversion, kernel
 // dispatch over (dimension, order, precision) and explicit RK44 stepping.
-#include <cstring>
-#include <cmath>
-#include <mutex>
-
-#include "context.hpp"
+#include "ctx_impl.cuh"
 #include "hex_kernels.cuh"
 
 namespace zb {
@@ -14,104 +10,6 @@ using dev::LineOpsT;
 using dev::Shape;
 using dev::TW;
 
-#define CK(x)                                                                                  \
-  do                                                                                           \
-  {                                                                                            \
-    cudaError_t e_ = (x);                                                                      \
-    if (e_ != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-struct StageCfg
-{
-  unsigned stage;
-  int rk_mode;      // 0 none, 1 stage update, 2 final combination
-  int save_ini;
-  int extrap_next;
-  int want_dU = 0;     // write the physical gradient (NS)
-  int grad_only = 0;   // NS: stop after the gradient kernel
-};
-
-// RK44 tables (src/solver.cpp:722-735)
-static const double kRkAlpha[3] = {0.5, 0.5, 1.0};
-static const double kRkBeta[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
-
-struct Ctx
-{
-  Plan plan;
-  int dev = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  int prec = ZB_FP64;
-  size_t tsz = 8;  // storage type size
-  size_t asz = 8;  // arithmetic type size
-  int D = 0, N = 0, S = 0, Fp = 0, V = 0, nstages = 4;
-  int64_t ntiles = 0;
-  void *U = nullptr, *U_ini = nullptr, *divF[4] = {nullptr, nullptr, nullptr, nullptr};
-  void *divF_vol = nullptr, *Ufp[2] = {nullptr, nullptr}, *Fvn = nullptr, *mets = nullptr, *fgeo = nullptr;
-  void *Ucomp = nullptr;
-  int *nbr = nullptr;
-  double *dtmp = nullptr;
-  size_t dtmp_bytes = 0;
-  double *dred = nullptr;
-  int cur = 0;
-  bool ufp_valid = false;
-  double dt = 0.0;
-  // mixed form: reference state (FP32-representable values) the stored state
-  // deviates from; zero for the FP64 form
-  double uref[5] = {0, 0, 0, 0, 0};
-  double *dref = nullptr;  // device copy for the conversion kernels
-  void *dU = nullptr;          // physical gradient side output (functionals)
-  double *dweights = nullptr;  // quadrature weights of the solution points
-  double *dfun = nullptr;      // functional reduction buffer
-  int64_t launches = 0;
-  // per-kernel CUDA-event timing (zb_profile_*)
-  bool profiling = false;
-  struct Rec { int kid; cudaEvent_t a, b; };
-  std::vector<Rec> recs;
-  std::vector<cudaEvent_t> pool;
-  double prof_ms[ZB_NKERNELS] = {0};
-  int64_t prof_n[ZB_NKERNELS] = {0};
-  void (*launch_extrap)(Ctx &) = nullptr;
-  void (*launch_stage)(Ctx &, const StageCfg &) = nullptr;
-};
-
-static cudaEvent_t take_event(Ctx &c)
-{
-  if (!c.pool.empty())
-  {
-    cudaEvent_t e = c.pool.back();
-    c.pool.pop_back();
-    return e;
-  }
-  cudaEvent_t e;
-  CK(cudaEventCreate(&e));
-  return e;
-}
-
-// Brackets one kernel launch with events when profiling is on.
-struct ProfScope
-{
-  Ctx &c;
-  int kid;
-  cudaEvent_t a = nullptr;
-  ProfScope(Ctx &cc, int k) : c(cc), kid(k)
-  {
-    if (c.profiling)
-    {
-      a = take_event(c);
-      CK(cudaEventRecord(a, c.stream));
-    }
-  }
-  ~ProfScope()
-  {
-    if (c.profiling && a)
-    {
-      cudaEvent_t b = take_event(c);
-      cudaEventRecord(b, c.stream);
-      c.recs.push_back({kid, a, b});
-    }
-  }
-};
 
 // ---------------------------------------------------------------------------
 // layout conversion kernels
@@ -312,69 +210,6 @@ __global__ void k_functionals(const T *__restrict__ U, const T *__restrict__ dU,
 // dispatch
 // ---------------------------------------------------------------------------
 
-template <typename T, int N>
-static LineOpsT<T, N> line_ops(const Plan &p)
-{
-  LineOpsT<T, N> o;
-  for (int i = 0; i < N * N; i++) o.Dm[i] = (T)p.ops.D[i];
-  for (int i = 0; i < N; i++)
-  {
-    o.Em[i] = (T)p.ops.Em[i];
-    o.Ep[i] = (T)p.ops.Ep[i];
-    o.Dbm[i] = (T)p.ops.Dbm[i];
-    o.Dbp[i] = (T)p.ops.Dbp[i];
-  }
-  return o;
-}
-
-template <typename T>
-static dev::Phys<T> phys_of(const zb_params &p, const double *uref, int ndims, bool deviations)
-{
-  dev::Phys<T> ph;
-  std::memset(&ph, 0, sizeof(ph));
-  ph.dev = deviations ? 1 : 0;
-  // perturbation-form constants of the reference state (FP64, then rounded)
-  const int V = ndims + 2;
-  double m2 = 0.0;
-  for (int d = 0; d < ndims; d++) m2 += uref[d + 1] * uref[d + 1];
-  for (int v = 0; v < V; v++) ph.Ur[v] = (T)uref[v];
-  if (uref[0] != 0.0)
-  {
-    const double Pr = (p.gamma - 1.0) * (uref[V - 1] - 0.5 * m2 / uref[0]);
-    ph.Pr = (T)Pr;
-    ph.er = (T)(uref[V - 1] + Pr);
-    ph.inv_rr = (T)(1.0 / uref[0]);
-    ph.mr2 = (T)m2;
-  }
-  ph.gamma = (T)p.gamma;
-  ph.prandtl = (T)p.prandtl;
-  ph.mu = (T)p.mu;
-  ph.rt = (T)p.rt;
-  ph.c_sth = (T)p.c_sth;
-  ph.rus_k = (T)p.rus_k;
-  ph.ldg_b = (T)p.ldg_b;
-  ph.ldg_tau = (T)p.ldg_tau;
-  ph.rho_fs = (T)p.rho_fs;
-  ph.P_fs = (T)p.P_fs;
-  ph.T_wall = (T)p.T_wall;
-  ph.R_ref = (T)p.R_ref;
-  for (int d = 0; d < 3; d++)
-  {
-    ph.V_fs[d] = (T)p.V_fs[d];
-    ph.V_wall[d] = (T)p.V_wall[d];
-  }
-  ph.fix_vis = p.fix_vis;
-  ph.fconv = p.fconv;
-  return ph;
-}
-
-static int grid_for(int64_t work, int threads)
-{
-  int64_t b = (work + threads - 1) / threads;
-  if (b > 148 * 64) b = 148 * 64;
-  if (b < 1) b = 1;
-  return (int)b;
-}
 
 template <typename T, typename A, int D, int N>
 static void launch_extrap_impl(Ctx &c)
@@ -392,11 +227,6 @@ static void launch_extrap_impl(Ctx &c)
   CK(cudaGetLastError());
 }
 
-template <typename K>
-static void set_smem(K kernel, size_t bytes)
-{
-  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-}
 
 template <typename T, typename A, int D, int N>
 static void launch_stage_impl(Ctx &c, const StageCfg &sc)
@@ -499,6 +329,7 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
   if (sc.extrap_next) c.cur ^= 1;
 }
 
+
 template <typename T, typename A, int D, int N>
 static void bind(Ctx &c)
 {
@@ -538,7 +369,7 @@ static void free_all(Ctx *c)
 {
   void *bufs[] = {c->U, c->U_ini, c->divF[0], c->divF[1], c->divF[2], c->divF[3], c->divF_vol, c->Ufp[0],
                   c->Ufp[1], c->Fvn, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
-                  c->dU, c->dweights, c->dfun};
+                  c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubar, c->pbar};
   for (void *b : bufs)
     if (b) cudaFree(b);
   for (auto &r : c->recs)
@@ -626,7 +457,10 @@ Ctx *ctx_create(const Plan &plan)
   c->dt = plan.params.dt;
   if (plan.tile != TW) ZB_THROW(ZB_ERR_INTERNAL, "plan tile width does not match kernels");
   if (c->prec == ZB_FP64)
+  {
     bind_t<double, double>(*c);
+    bind_vjp(*c);
+  }
   else
     bind_t<float, float>(*c);
   try
@@ -704,6 +538,14 @@ void ctx_set_stream(Ctx *c, void *stream)
 }
 
 void ctx_set_dt(Ctx *c, double dt) { c->dt = dt; }
+
+void ctx_set_freestream(Ctx *c, double rho_fs, const double *V_fs, double P_fs)
+{
+  // launches read the parameters by value, so queued work keeps the old ones
+  c->plan.params.rho_fs = rho_fs;
+  for (int d = 0; d < 3; d++) c->plan.params.V_fs[d] = V_fs[d];
+  c->plan.params.P_fs = P_fs;
+}
 
 static const double *stage_in(Ctx *c, const double *src, size_t extent_elems, int where)
 {
@@ -934,6 +776,55 @@ void ctx_functionals(Ctx *c, double *out)
   out[0] = h[0];
   out[1] = grad ? h[1] : 0.0;
   out[2] = h[2];
+}
+
+void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, int64_t es, int where,
+             double *param_bar)
+{
+  if (c->prec != ZB_FP64) ZB_THROW(ZB_ERR_UNSUPPORTED, "the adjoint is built for the plain FP64 form only");
+  if (!c->launch_vjp)
+    ZB_THROW(ZB_ERR_UNSUPPORTED, "no adjoint kernels for ndims=" + std::to_string(c->D) + " P=" + std::to_string(c->N - 1));
+  if (!lam || !Ubar) ZB_THROW(ZB_ERR_ARG, "null adjoint buffer");
+  const size_t nU = (size_t)c->ntiles * c->S * c->V * TW;
+  const size_t nF = (size_t)c->ntiles * c->Fp * c->V * TW;
+  if (!c->lam)
+  {
+    c->lam = (double *)dalloc(nU * sizeof(double));
+    c->Ubar = (double *)dalloc(nU * sizeof(double));
+    c->Lfp = (double *)dalloc(nF * sizeof(double));
+    c->Ubfp = (double *)dalloc(nF * sizeof(double));
+    c->pbar = (double *)dalloc((size_t)c->ntiles * 5 * sizeof(double));
+    if (c->plan.params.viscous)
+    {
+      c->dUbfp = (double *)dalloc(nF * c->D * sizeof(double));
+      c->UCb = (double *)dalloc(nF * sizeof(double));
+    }
+  }
+  const size_t ext = extent(c, ss, vs, es, c->S);
+  const double *src = stage_in(c, lam, ext, where);
+  {
+    const int64_t work = c->ntiles * c->S * c->V * TW;
+    ProfScope ps(*c, ZB_K_TO_TILES);
+    k_to_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>(src, c->lam, nullptr, nullptr, c->plan.neles,
+                                                                     c->ntiles, c->S, c->V, ss, vs, es);
+    c->launches++;
+    CK(cudaGetLastError());
+  }
+  // linearisation point: the current state and its traces
+  c->ufp_valid = false;
+  ensure_ufp(c);
+  c->launch_vjp(*c, param_bar != nullptr);
+  from_tiles(c, c->Ubar, nullptr, nullptr, Ubar, ss, vs, es, where);
+  if (param_bar)
+  {
+    std::vector<double> h((size_t)c->ntiles * 5);
+    CK(cudaMemcpyAsync(h.data(), c->pbar, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    // fixed-order sum over tiles of the real elements (padded lanes repeat element 0)
+    for (int k = 0; k < 5; k++) param_bar[k] = 0.0;
+    for (int64_t t = 0; t < c->ntiles; t++)
+      for (int k = 0; k < 5; k++) param_bar[k] += h[(size_t)t * 5 + k];
+  }
 }
 
 void ctx_profile_enable(Ctx *c, int on)

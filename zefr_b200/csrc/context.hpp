@@ -21,6 +21,7 @@ void ctx_destroy(Ctx *c);
 void ctx_info(const Ctx *c, zb_info *out);
 void ctx_set_stream(Ctx *c, void *stream);
 void ctx_set_dt(Ctx *c, double dt);
+void ctx_set_freestream(Ctx *c, double rho_fs, const double *V_fs, double P_fs);
 void ctx_set_state(Ctx *c, const double *U, int64_t ss, int64_t vs, int64_t es, int where);
 void ctx_get_state(Ctx *c, double *U, int64_t ss, int64_t vs, int64_t es, int where);
 void ctx_compute_residual(Ctx *c, unsigned stage);
@@ -32,6 +33,8 @@ void ctx_sync(Ctx *c);
 int64_t ctx_launches(const Ctx *c);
 void ctx_profile_enable(Ctx *c, int on);
 void ctx_functionals(Ctx *c, double *out);
+void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, int64_t es, int where,
+             double *param_bar);
 void ctx_profile_read(Ctx *c, double *ms, int64_t *count);
 void noalloc_residual(const Plan &p, const double *U, double *divF, cudaStream_t st);
 

@@ -1,0 +1,195 @@
+// Device context shared by the forward (context.cu) and adjoint (adjoint.cu)
+// translation units: buffers, launch helpers and profiling scopes.
+#pragma once
+#include <cstring>
+#include <cmath>
+#include <mutex>
+#include <type_traits>
+
+#include "context.hpp"
+#include "dfr_kernels.cuh"
+
+namespace zb {
+
+using dev::Args;
+using dev::LineOpsT;
+using dev::Shape;
+using dev::TW;
+
+#define CK(x)                                                                                  \
+  do                                                                                           \
+  {                                                                                            \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct StageCfg
+{
+  unsigned stage;
+  int rk_mode;      // 0 none, 1 stage update, 2 final combination
+  int save_ini;
+  int extrap_next;
+  int want_dU = 0;     // write the physical gradient (NS)
+  int grad_only = 0;   // NS: stop after the gradient kernel
+};
+
+// RK44 tables (src/solver.cpp:722-735)
+static const double kRkAlpha[3] = {0.5, 0.5, 1.0};
+static const double kRkBeta[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+
+struct Ctx
+{
+  Plan plan;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int prec = ZB_FP64;
+  size_t tsz = 8;  // storage type size
+  size_t asz = 8;  // arithmetic type size
+  int D = 0, N = 0, S = 0, Fp = 0, V = 0, nstages = 4;
+  int64_t ntiles = 0;
+  void *U = nullptr, *U_ini = nullptr, *divF[4] = {nullptr, nullptr, nullptr, nullptr};
+  void *divF_vol = nullptr, *Ufp[2] = {nullptr, nullptr}, *Fvn = nullptr, *mets = nullptr, *fgeo = nullptr;
+  void *Ucomp = nullptr;
+  int *nbr = nullptr;
+  double *dtmp = nullptr;
+  size_t dtmp_bytes = 0;
+  double *dred = nullptr;
+  int cur = 0;
+  bool ufp_valid = false;
+  double dt = 0.0;
+  // mixed form: reference state (FP32-representable values) the stored state
+  // deviates from; zero for the FP64 form
+  double uref[5] = {0, 0, 0, 0, 0};
+  double *dref = nullptr;  // device copy for the conversion kernels
+  void *dU = nullptr;          // physical gradient side output (functionals)
+  double *dweights = nullptr;  // quadrature weights of the solution points
+  double *dfun = nullptr;      // functional reduction buffer
+  int64_t launches = 0;
+  // per-kernel CUDA-event timing (zb_profile_*)
+  bool profiling = false;
+  struct Rec { int kid; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  double prof_ms[ZB_NKERNELS] = {0};
+  int64_t prof_n[ZB_NKERNELS] = {0};
+  // adjoint (plain FP64 form), allocated on first use
+  double *lam = nullptr, *Lfp = nullptr, *Ubfp = nullptr, *dUbfp = nullptr, *UCb = nullptr, *Ubar = nullptr;
+  double *pbar = nullptr;
+  void (*launch_extrap)(Ctx &) = nullptr;
+  void (*launch_stage)(Ctx &, const StageCfg &) = nullptr;
+  void (*launch_vjp)(Ctx &, bool) = nullptr;
+};
+
+static cudaEvent_t take_event(Ctx &c)
+{
+  if (!c.pool.empty())
+  {
+    cudaEvent_t e = c.pool.back();
+    c.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CK(cudaEventCreate(&e));
+  return e;
+}
+
+// Brackets one kernel launch with events when profiling is on.
+struct ProfScope
+{
+  Ctx &c;
+  int kid;
+  cudaEvent_t a = nullptr;
+  ProfScope(Ctx &cc, int k) : c(cc), kid(k)
+  {
+    if (c.profiling)
+    {
+      a = take_event(c);
+      CK(cudaEventRecord(a, c.stream));
+    }
+  }
+  ~ProfScope()
+  {
+    if (c.profiling && a)
+    {
+      cudaEvent_t b = take_event(c);
+      cudaEventRecord(b, c.stream);
+      c.recs.push_back({kid, a, b});
+    }
+  }
+};
+
+template <typename T, int N>
+static LineOpsT<T, N> line_ops(const Plan &p)
+{
+  LineOpsT<T, N> o;
+  for (int i = 0; i < N * N; i++) o.Dm[i] = (T)p.ops.D[i];
+  for (int i = 0; i < N; i++)
+  {
+    o.Em[i] = (T)p.ops.Em[i];
+    o.Ep[i] = (T)p.ops.Ep[i];
+    o.Dbm[i] = (T)p.ops.Dbm[i];
+    o.Dbp[i] = (T)p.ops.Dbp[i];
+  }
+  return o;
+}
+
+template <typename T>
+static dev::Phys<T> phys_of(const zb_params &p, const double *uref, int ndims, bool deviations)
+{
+  dev::Phys<T> ph;
+  std::memset(&ph, 0, sizeof(ph));
+  ph.dev = deviations ? 1 : 0;
+  // perturbation-form constants of the reference state (FP64, then rounded)
+  const int V = ndims + 2;
+  double m2 = 0.0;
+  for (int d = 0; d < ndims; d++) m2 += uref[d + 1] * uref[d + 1];
+  for (int v = 0; v < V; v++) ph.Ur[v] = (T)uref[v];
+  if (uref[0] != 0.0)
+  {
+    const double Pr = (p.gamma - 1.0) * (uref[V - 1] - 0.5 * m2 / uref[0]);
+    ph.Pr = (T)Pr;
+    ph.er = (T)(uref[V - 1] + Pr);
+    ph.inv_rr = (T)(1.0 / uref[0]);
+    ph.mr2 = (T)m2;
+  }
+  ph.gamma = (T)p.gamma;
+  ph.prandtl = (T)p.prandtl;
+  ph.mu = (T)p.mu;
+  ph.rt = (T)p.rt;
+  ph.c_sth = (T)p.c_sth;
+  ph.rus_k = (T)p.rus_k;
+  ph.ldg_b = (T)p.ldg_b;
+  ph.ldg_tau = (T)p.ldg_tau;
+  ph.rho_fs = (T)p.rho_fs;
+  ph.P_fs = (T)p.P_fs;
+  ph.T_wall = (T)p.T_wall;
+  ph.R_ref = (T)p.R_ref;
+  for (int d = 0; d < 3; d++)
+  {
+    ph.V_fs[d] = (T)p.V_fs[d];
+    ph.V_wall[d] = (T)p.V_wall[d];
+  }
+  ph.fix_vis = p.fix_vis;
+  ph.fconv = p.fconv;
+  return ph;
+}
+
+static int grid_for(int64_t work, int threads)
+{
+  int64_t b = (work + threads - 1) / threads;
+  if (b > 148 * 64) b = 148 * 64;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+template <typename K>
+static void set_smem(K kernel, size_t bytes)
+{
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// selects the adjoint kernels of the context (plain FP64 form; adjoint.cu)
+void bind_vjp(Ctx &c);
+
+}  // namespace zb

@@ -25,30 +25,31 @@ struct Dual
   __host__ __device__ constexpr Dual(T x, T dx) : v(x), d(dx) {}
 };
 
-template <typename T> __device__ __forceinline__ Dual<T> operator+(Dual<T> a, Dual<T> b) { return {a.v + b.v, a.d + b.d}; }
-template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a, Dual<T> b) { return {a.v - b.v, a.d - b.d}; }
-template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a) { return {-a.v, -a.d}; }
-template <typename T> __device__ __forceinline__ Dual<T> operator*(Dual<T> a, Dual<T> b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
-template <typename T> __device__ __forceinline__ Dual<T> operator/(Dual<T> a, Dual<T> b)
+template <typename T> ZB_HD Dual<T> operator+(Dual<T> a, Dual<T> b) { return {a.v + b.v, a.d + b.d}; }
+template <typename T> ZB_HD Dual<T> operator-(Dual<T> a, Dual<T> b) { return {a.v - b.v, a.d - b.d}; }
+template <typename T> ZB_HD Dual<T> operator-(Dual<T> a) { return {-a.v, -a.d}; }
+template <typename T> ZB_HD Dual<T> operator*(Dual<T> a, Dual<T> b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+template <typename T> ZB_HD Dual<T> operator/(Dual<T> a, Dual<T> b)
 {
   const T q = a.v / b.v;
   return {q, (a.d - q * b.d) / b.v};
 }
-template <typename T> __device__ __forceinline__ Dual<T> &operator+=(Dual<T> &a, Dual<T> b) { a = a + b; return a; }
-template <typename T> __device__ __forceinline__ Dual<T> &operator-=(Dual<T> &a, Dual<T> b) { a = a - b; return a; }
-template <typename T> __device__ __forceinline__ Dual<T> &operator*=(Dual<T> &a, Dual<T> b) { a = a * b; return a; }
-template <typename T> __device__ __forceinline__ bool operator<(Dual<T> a, Dual<T> b) { return a.v < b.v; }
-template <typename T> __device__ __forceinline__ bool operator>(Dual<T> a, Dual<T> b) { return a.v > b.v; }
-template <typename T> __device__ __forceinline__ bool operator<=(Dual<T> a, Dual<T> b) { return a.v <= b.v; }
-template <typename T> __device__ __forceinline__ bool operator>=(Dual<T> a, Dual<T> b) { return a.v >= b.v; }
-template <typename T> __device__ __forceinline__ bool operator==(Dual<T> a, Dual<T> b) { return a.v == b.v; }
+template <typename T> ZB_HD Dual<T> &operator+=(Dual<T> &a, Dual<T> b) { a = a + b; return a; }
+template <typename T> ZB_HD Dual<T> &operator-=(Dual<T> &a, Dual<T> b) { a = a - b; return a; }
+template <typename T> ZB_HD Dual<T> &operator*=(Dual<T> &a, Dual<T> b) { a = a * b; return a; }
+template <typename T> ZB_HD Dual<T> &operator/=(Dual<T> &a, Dual<T> b) { a = a / b; return a; }
+template <typename T> ZB_HD bool operator<(Dual<T> a, Dual<T> b) { return a.v < b.v; }
+template <typename T> ZB_HD bool operator>(Dual<T> a, Dual<T> b) { return a.v > b.v; }
+template <typename T> ZB_HD bool operator<=(Dual<T> a, Dual<T> b) { return a.v <= b.v; }
+template <typename T> ZB_HD bool operator>=(Dual<T> a, Dual<T> b) { return a.v >= b.v; }
+template <typename T> ZB_HD bool operator==(Dual<T> a, Dual<T> b) { return a.v == b.v; }
 
-template <> __device__ __forceinline__ Dual<double> dsqrt<Dual<double>>(Dual<double> x)
+template <> ZB_HD Dual<double> dsqrt<Dual<double>>(Dual<double> x)
 {
   const double s = sqrt(x.v);
   return {s, x.d / (2.0 * s)};
 }
-template <> __device__ __forceinline__ Dual<double> dpow<Dual<double>>(Dual<double> x, Dual<double> y)
+template <> ZB_HD Dual<double> dpow<Dual<double>>(Dual<double> x, Dual<double> y)
 {
   // y is a constant exponent in every use (1.5, gamma, 1/(gamma-1))
   const double p = pow(x.v, y.v);
@@ -56,7 +57,7 @@ template <> __device__ __forceinline__ Dual<double> dpow<Dual<double>>(Dual<doub
 }
 
 template <typename T>
-__device__ __forceinline__ Phys<Dual<T>> dual_phys(const Phys<T> &p)
+ZB_HD Phys<Dual<T>> dual_phys(const Phys<T> &p)
 {
   Phys<Dual<T>> q;
   q.gamma = p.gamma;
@@ -89,7 +90,7 @@ __device__ __forceinline__ Phys<Dual<T>> dual_phys(const Phys<T> &p)
 
 // g = J^T lam for y = f(x), x in R^NI, y in R^NO; f(const Dual* x, Dual* y).
 template <int NI, int NO, typename F>
-__device__ __forceinline__ void vjp_local(F &&f, const double x[NI], const double lam[NO], double g[NI])
+ZB_HD void vjp_local(F &&f, const double x[NI], const double lam[NO], double g[NI])
 {
 #pragma unroll 1
   for (int k = 0; k < NI; k++)

@@ -6,6 +6,14 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
+
+// Pointwise functions compile for the host too (unit tests of the adjoint
+// algebra run them on the CPU).
+#ifndef ZB_HD
+#define ZB_HD __host__ __device__ __forceinline__
+#endif
+
 namespace zb {
 namespace dev {
 
@@ -27,18 +35,18 @@ struct Phys
 template <typename T> struct Pert { static constexpr bool on = false; };
 template <> struct Pert<float> { static constexpr bool on = true; };
 
-template <typename T> __device__ __forceinline__ T dsqrt(T x);
-template <> __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
-template <typename T> __device__ __forceinline__ T dpow(T x, T y);
-template <> __device__ __forceinline__ double dpow<double>(double x, double y) { return pow(x, y); }
-template <> __device__ __forceinline__ float dpow<float>(float x, float y) { return powf(x, y); }
-template <typename T> __device__ __forceinline__ T dabs(T x) { return x < T(0) ? -x : x; }
-template <typename T> __device__ __forceinline__ T dmax(T a, T b) { return a > b ? a : b; }
+template <typename T> ZB_HD T dsqrt(T x);
+template <> ZB_HD double dsqrt<double>(double x) { return sqrt(x); }
+template <> ZB_HD float dsqrt<float>(float x) { return sqrtf(x); }
+template <typename T> ZB_HD T dpow(T x, T y);
+template <> ZB_HD double dpow<double>(double x, double y) { return pow(x, y); }
+template <> ZB_HD float dpow<float>(float x, float y) { return powf(x, y); }
+template <typename T> ZB_HD T dabs(T x) { return x < T(0) ? -x : x; }
+template <typename T> ZB_HD T dmax(T a, T b) { return a > b ? a : b; }
 
 // Inviscid flux F[var][dim] and pressure (include/flux.hpp:11-63, Vg = 0).
 template <typename T, int D>
-__device__ __forceinline__ void flux_conv(const T U[D + 2], T F[D + 2][D], T &P, T gamma)
+ZB_HD void flux_conv(const T U[D + 2], T F[D + 2][D], T &P, T gamma)
 {
   const T invrho = T(1) / U[0];
   T momF = U[1] * U[1];
@@ -66,7 +74,7 @@ __device__ __forceinline__ void flux_conv(const T U[D + 2], T F[D + 2][D], T &P,
 //   m_d e/rho - mr_d er/rho_r = (m'_d er + mr_d e' + m'_d e')/rho - mr_d er rho'/(rho rho_r)
 // with e = E + P the total enthalpy per volume.
 template <typename T, int D>
-__device__ __forceinline__ void flux_conv_pert(const T Up[D + 2], T F[D + 2][D], T &P, T &Pp, const Phys<T> &ph)
+ZB_HD void flux_conv_pert(const T Up[D + 2], T F[D + 2][D], T &P, T &Pp, const Phys<T> &ph)
 {
   const T *Ur = ph.Ur;
   const T rho = Ur[0] + Up[0];
@@ -97,14 +105,14 @@ __device__ __forceinline__ void flux_conv_pert(const T Up[D + 2], T F[D + 2][D],
 
 // absolute state from a stored one (identity outside the perturbation form)
 template <typename T, int D>
-__device__ __forceinline__ void to_abs(const T Us[D + 2], T Ua[D + 2], const Phys<T> &ph)
+ZB_HD void to_abs(const T Us[D + 2], T Ua[D + 2], const Phys<T> &ph)
 {
 #pragma unroll
   for (int v = 0; v < D + 2; v++) Ua[v] = ph.dev ? ph.Ur[v] + Us[v] : Us[v];
 }
 
 template <typename T, int D>
-__device__ __forceinline__ void to_stored(const T Ua[D + 2], T Us[D + 2], const Phys<T> &ph)
+ZB_HD void to_stored(const T Ua[D + 2], T Us[D + 2], const Phys<T> &ph)
 {
 #pragma unroll
   for (int v = 0; v < D + 2; v++) Us[v] = ph.dev ? Ua[v] - ph.Ur[v] : Ua[v];
@@ -113,7 +121,7 @@ __device__ __forceinline__ void to_stored(const T Ua[D + 2], T Us[D + 2], const 
 // Inviscid flux of a stored state (deviation from Ur in the perturbation form)
 // and the absolute pressure.
 template <typename T, int D>
-__device__ __forceinline__ void flux_conv_stored(const T Us[D + 2], T F[D + 2][D], T &P, T &Pp, const Phys<T> &ph)
+ZB_HD void flux_conv_stored(const T Us[D + 2], T F[D + 2][D], T &P, T &Pp, const Phys<T> &ph)
 {
   if constexpr (Pert<T>::on)
     flux_conv_pert<T, D>(Us, F, P, Pp, ph);
@@ -129,7 +137,7 @@ __device__ __forceinline__ void flux_conv_stored(const T Us[D + 2], T F[D + 2][D
 
 // Viscous flux added to F (include/flux.hpp:71-202): F -= tau / heat flux.
 template <typename T, int D>
-__device__ __forceinline__ void flux_visc_add(const T U[D + 2], const T dU[D + 2][D], T F[D + 2][D],
+ZB_HD void flux_visc_add(const T U[D + 2], const T dU[D + 2][D], T F[D + 2][D],
                                               const Phys<T> &ph)
 {
   const T invrho = T(1) / U[0];
@@ -189,7 +197,7 @@ __device__ __forceinline__ void flux_visc_add(const T U[D + 2], const T dU[D + 2
 
 // Normal viscous flux from one side: (F_visc(U, dU)) . n
 template <typename T, int D>
-__device__ __forceinline__ void visc_normal(const T U[D + 2], const T dU[D + 2][D], const T n[D],
+ZB_HD void visc_normal(const T U[D + 2], const T dU[D + 2][D], const T n[D],
                                             T Fn[D + 2], const Phys<T> &ph)
 {
   T F[D + 2][D];
@@ -212,7 +220,7 @@ __device__ __forceinline__ void visc_normal(const T U[D + 2], const T dU[D + 2][
 // UL, UR are stored states (deviations from Ur in the perturbation form); the
 // result is the common flux of the stored form (minus F(Ur).n).
 template <typename T, int D>
-__device__ __forceinline__ void rusanov(const T UL[D + 2], const T UR[D + 2], const T n[D], T Fc[D + 2],
+ZB_HD void rusanov(const T UL[D + 2], const T UR[D + 2], const T n[D], T Fc[D + 2],
                                         const Phys<T> &ph)
 {
   T FL[D + 2][D], FR[D + 2][D], PL, PR, QL, QR;
@@ -252,7 +260,7 @@ __device__ __forceinline__ void rusanov(const T UL[D + 2], const T UR[D + 2], co
 // |l| below delta = 0.1 * (|u_n| + a) of the Roe state is replaced by
 // (l^2 + delta^2) / (2 delta).  No reference counterpart.
 template <typename T, int D>
-__device__ __forceinline__ void roe(const T SL[D + 2], const T SR[D + 2], const T n[D], T Fc[D + 2],
+ZB_HD void roe(const T SL[D + 2], const T SR[D + 2], const T n[D], T Fc[D + 2],
                                     const Phys<T> &ph)
 {
   const T g = ph.gamma;
@@ -334,7 +342,7 @@ __device__ __forceinline__ void roe(const T SL[D + 2], const T SR[D + 2], const 
 // rus_bias = 0: Rusanov uses the ghost state UR, LDG the prescribed state UB).
 // Returns false for a boundary code with no ghost state.
 template <typename T, int D>
-__device__ __forceinline__ void ghost_state(int bc, const T UL[D + 2], const T n[D], T UR[D + 2], T UB[D + 2],
+ZB_HD void ghost_state(int bc, const T UL[D + 2], const T n[D], T UR[D + 2], T UB[D + 2],
                                             const Phys<T> &ph)
 {
   const T g = ph.gamma;
@@ -489,7 +497,7 @@ __device__ __forceinline__ void ghost_state(int bc, const T UL[D + 2], const T n
 // Boundary gradient (src/faces.cpp:508-710): copy, except adiabatic walls
 // remove the wall-normal temperature gradient from the energy gradient.
 template <typename T, int D>
-__device__ __forceinline__ void ghost_grad(int bc, const T UL[D + 2], const T dUL[D + 2][D], const T n[D],
+ZB_HD void ghost_grad(int bc, const T UL[D + 2], const T dUL[D + 2][D], const T n[D],
                                            T dUR[D + 2][D])
 {
 #pragma unroll

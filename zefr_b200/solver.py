@@ -176,10 +176,18 @@ class FRSolver:
         return (self.nvars * E, E, 1)
 
     # -- state --
+    @staticmethod
+    def _torch_ready():
+        """The library runs on its own stream: wait for torch's queued work
+        on a tensor before the library reads it."""
+        import torch
+        torch.cuda.current_stream().synchronize()
+
     def set_state(self, U) -> None:
         if hasattr(U, "is_cuda") and U.is_cuda:
             import torch
             U = U.to(torch.float64).contiguous()
+            self._torch_ready()
             assert tuple(U.shape) == self.state_shape
             check(lib().zb_set_state(self.h, ctypes.cast(U.data_ptr(), _DP), *self._strides(), _lib.ZB_DEVICE))
             self._keep = U
@@ -195,8 +203,10 @@ class FRSolver:
         return out
 
     def get_state_device(self, out) -> None:
-        """Copy the state into a contiguous float64 CUDA tensor of state_shape."""
+        """Copy the state into a contiguous float64 CUDA tensor of state_shape
+        (complete on return)."""
         check(lib().zb_get_state(self.h, ctypes.cast(out.data_ptr(), _DP), *self._strides(), _lib.ZB_DEVICE))
+        self.synchronize()
 
     # -- residual --
     def compute_residual(self, stage: int = 0) -> None:
@@ -211,8 +221,11 @@ class FRSolver:
         return out
 
     def get_residual_device(self, out, stage: int = 0) -> None:
+        """Copy a residual register into a contiguous float64 CUDA tensor
+        (complete on return)."""
         check(lib().zb_get_residual(self.h, stage, ctypes.cast(out.data_ptr(), _DP), *self._strides(),
                                     _lib.ZB_DEVICE))
+        self.synchronize()
 
     def residual(self, U, stage: int = 0) -> np.ndarray:
         self.set_state(U)
@@ -232,6 +245,12 @@ class FRSolver:
     def set_dt(self, dt: float) -> None:
         check(lib().zb_set_dt(self.h, dt))
 
+    def set_freestream(self, rho_fs: float, V_fs, P_fs: float) -> None:
+        """Free-stream state of the far-field / characteristic boundaries."""
+        v = np.zeros(3)
+        v[:len(V_fs)] = V_fs
+        check(lib().zb_set_freestream(self.h, float(rho_fs), v.ctypes.data_as(_DP), float(P_fs)))
+
     def residual_norms(self) -> Dict[str, np.ndarray]:
         out = np.zeros(3 * self.nvars)
         check(lib().zb_residual_norms(self.h, out.ctypes.data_as(_DP)))
@@ -244,6 +263,32 @@ class FRSolver:
         out = np.zeros(4)
         check(lib().zb_functionals(self.h, out.ctypes.data_as(_DP)))
         return {"ke": float(out[0]), "enstrophy": float(out[1]), "volume": float(out[2])}
+
+    # -- adjoint --
+    def vjp(self, lam, params: bool = False):
+        """Adjoint of the residual at the current state (plain FP64 form):
+        returns Ubar = (d divF / d U)^T lam in state_shape, and with
+        ``params`` also d(lam . divF)/d(rho_fs, V_fs[0..2], P_fs).  ``lam``
+        is a numpy array or a CUDA tensor (then Ubar is a CUDA tensor)."""
+        pbar = np.zeros(5) if params else None
+        pptr = pbar.ctypes.data_as(_DP) if params else None
+        if hasattr(lam, "is_cuda") and lam.is_cuda:
+            import torch
+            lam = lam.to(torch.float64).contiguous()
+            assert tuple(lam.shape) == self.state_shape
+            out = torch.empty_like(lam)
+            self._torch_ready()
+            check(lib().zb_vjp(self.h, ctypes.cast(lam.data_ptr(), _DP), ctypes.cast(out.data_ptr(), _DP),
+                               *self._strides(), _lib.ZB_DEVICE, pptr))
+            self.synchronize()
+        else:
+            lam = np.ascontiguousarray(lam, dtype=np.float64)
+            if lam.shape != self.state_shape:
+                raise ValueError(f"lam shape {lam.shape} != {self.state_shape}")
+            out = np.zeros(self.state_shape)
+            check(lib().zb_vjp(self.h, lam.ctypes.data_as(_DP), out.ctypes.data_as(_DP), *self._strides(),
+                               _lib.ZB_HOST, pptr))
+        return (out, pbar) if params else out
 
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().zb_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
