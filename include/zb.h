@@ -123,6 +123,9 @@ typedef struct zb_params {
   double rho_fs, V_fs[3], P_fs;
   double T_wall, R_ref, V_wall[3];
   double dt;          /* RK time step */
+  int tri_volume_div; /* triangles: 0 = the reference's operators, whose oppDiv
+                         lacks the volume-divergence term (src/elements.cpp:
+                         609-623 builds it for quads/hexes only); 1 = include it */
 } zb_params;
 
 /* Deck-style inputs for zb_params_from_deck (reference keys, src/input.cpp). */

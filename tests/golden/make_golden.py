@@ -53,6 +53,9 @@ def _cases():
     def shear(X, g):
         return ics.double_shear_layer(X * 0.1 + 0.5, mach=0.2, gamma=g)
 
+    def shear_unit(X, g):
+        return ics.double_shear_layer(X, mach=0.2, gamma=g)
+
     per = {"PERIODIC": "periodic"}
     return {
         "quad_p3_euler_vortex": (lambda: meshgen.box_quads(8, 8), 2, 3, False, per, eul, vortex, 3),
@@ -75,6 +78,14 @@ def _cases():
                                    {"WALL": "wall_slip", "FARFIELD": "char"}, dict(eul, mach_fs=0.2), cyl_state, 2),
         "cyl_p2_euler_supin_sym": (lambda: meshgen.cylinder_omesh(3, 8, r1=4.0), 2, 2, False,
                                    {"WALL": "symmetry", "FARFIELD": "farfield"}, dict(eul, mach_fs=0.2), cyl_state, 2),
+        # triangles (FR with Williams-Shunn points and the 'M3' correction)
+        "tri_p4_ns_jitter": (lambda: meshgen.box_tris(4, seed=3), 2, 4, True, per,
+                             dict(cyl_deck, Re_fs=1000, prandtl=0.71), shear_unit, 2),
+        "tri_p2_euler_vortex": (lambda: meshgen.box_tris(5, -5.0, 5.0, seed=1), 2, 2, False, per, eul, vortex, 2),
+        "tri_p3_euler_char": (lambda: meshgen.box_tris(4, -2.0, 2.0, seed=2, bnd="FARFIELD"), 2, 3, False,
+                              {"FARFIELD": "char"}, dict(eul, mach_fs=0.2), cyl_state, 2),
+        "tri_p1_ns_adi": (lambda: meshgen.box_tris(4, 0.0, 1.0, seed=4, bnd="WALL"), 2, 1, True,
+                          {"WALL": "wall_ns_adi"}, cyl_deck, shear_unit, 2),
     }
 
 

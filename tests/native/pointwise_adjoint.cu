@@ -115,6 +115,61 @@ static void check_point(std::mt19937_64 &rng, bool sutherland)
   }
 }
 
+// Riemann solvers: hand reverse (both sides) against dual numbers.  near0
+// puts the normal velocity near zero so Roe's entropy fix is active.
+template <int D>
+static void check_riemann(std::mt19937_64 &rng, int fconv, bool near0)
+{
+  constexpr int V = D + 2;
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  double UL[V], UR[V], n[D], w[V];
+  double nn = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    n[d] = u(rng);
+    nn += n[d] * n[d];
+  }
+  for (int d = 0; d < D; d++) n[d] /= std::sqrt(nn);
+  for (double *U : {UL, UR})
+  {
+    U[0] = 1.0 + 0.3 * u(rng);
+    double m2 = 0.0;
+    for (int d = 0; d < D; d++)
+    {
+      U[d + 1] = (near0 ? 0.02 : 0.6) * u(rng);
+      m2 += U[d + 1] * U[d + 1];
+    }
+    U[V - 1] = 2.5 + 0.5 * m2 / U[0] + 0.2 * u(rng);
+  }
+  for (int v = 0; v < V; v++) w[v] = u(rng);
+  Phys<double> ph = phys(false);
+  ph.fconv = fconv;
+  ph.rus_k = 0.0;
+  const Phys<DD> pd = dual_phys(ph);
+  double bL[V] = {0}, bR[V] = {0};
+  if (fconv == 2)
+    roe_vjp<D>(UL, UR, n, w, ph, bL, bR);
+  else
+    rusanov_vjp<D>(UL, UR, n, w, ph, bL, bR);
+  for (int k = 0; k < 2 * V; k++)
+  {
+    DD L[V], R[V], F[V], nd[D];
+    for (int d = 0; d < D; d++) nd[d] = DD(n[d]);
+    for (int v = 0; v < V; v++)
+    {
+      L[v] = DD(UL[v], k == v ? 1.0 : 0.0);
+      R[v] = DD(UR[v], k == V + v ? 1.0 : 0.0);
+    }
+    if (fconv == 2)
+      roe<DD, D>(L, R, nd, F, pd);
+    else
+      rusanov<DD, D>(L, R, nd, F, pd);
+    double s = 0.0;
+    for (int v = 0; v < V; v++) s += w[v] * F[v].d;
+    record(fconv == 2 ? "roe" : "rusanov", k < V ? bL[k] : bR[k - V], s);
+  }
+}
+
 int main()
 {
   std::mt19937_64 rng(20261203);
@@ -124,6 +179,12 @@ int main()
     check_point<2>(rng, true);
     check_point<3>(rng, false);
     check_point<3>(rng, true);
+    for (int fc : {0, 2})
+      for (bool z : {false, true})
+      {
+        check_riemann<2>(rng, fc, z);
+        check_riemann<3>(rng, fc, z);
+      }
   }
   std::printf("worst relative error %.3e\n", g_worst);
   return g_worst > 1e-12 ? 1 : 0;

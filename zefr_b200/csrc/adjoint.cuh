@@ -10,15 +10,19 @@
 //     weight of both sides and keep the part for their own trace, so no
 //     atomics are needed and the result is deterministic;
 //   - pointwise Jacobian-transpose products are hand-written reverse mode for
-//     the volume fluxes (flux_conv_vjp, flux_visc_vjp) and forward-mode dual
-//     numbers (dual.cuh) for the Riemann solvers, boundary ghost states and
-//     gradients, which run on flux points only.
+//     the fluxes and Riemann solvers (flux_conv_vjp, flux_visc_vjp,
+//     rusanov_vjp, roe_vjp) and forward-mode dual numbers (dual.cuh) for the
+//     boundary ghost states and gradients, which run on boundary faces only.
 // Navier-Stokes needs three passes because the LDG common solution couples the
 // gradient of one element to the trace of its neighbour.
 #pragma once
 
 #include "dfr_kernels.cuh"
 #include "dual.cuh"
+
+// Boundary-face functions run on few flux points and hold many dual numbers:
+// out of line, so their registers do not weigh on the interior path.
+#define ZB_HD_COLD __host__ __device__ __noinline__
 
 namespace zb {
 namespace dev {
@@ -202,6 +206,274 @@ ZB_HD void flux_visc_vjp(const double U[D + 2], const double dU[D + 2][D], const
   Ub[0] += rhob;
 }
 
+// Ub += (dP/dU)^T Pb for the pressure P = (gamma-1)(E - |m|^2 / 2 rho).
+template <int D>
+ZB_HD void pressure_vjp(const double U[D + 2], double Pb, double gamma, double Ub[D + 2])
+{
+  const double g1 = (gamma - 1.0) * Pb, ir = 1.0 / U[0];
+  double m2 = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    m2 += U[d + 1] * U[d + 1];
+    Ub[d + 1] -= g1 * U[d + 1] * ir;
+  }
+  Ub[0] += g1 * 0.5 * m2 * ir * ir;
+  Ub[D + 1] += g1;
+}
+
+// (UbL, UbR) += (d Fc / d (UL, UR))^T w for the Rusanov flux of physics.cuh
+// (absolute FP64 states).  The wave-speed max and |Vn| take the derivative of
+// the branch the forward evaluation takes.
+template <int D>
+ZB_HD void rusanov_vjp(const double UL[D + 2], const double UR[D + 2], const double n[D], const double w[D + 2],
+                       const Phys<double> &ph, double UbL[D + 2], double UbR[D + 2])
+{
+  constexpr int V = D + 2;
+  const double g = ph.gamma;
+  double m2L = 0.0, m2R = 0.0, VnL = 0.0, VnR = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    m2L += UL[d + 1] * UL[d + 1];
+    m2R += UR[d + 1] * UR[d + 1];
+    VnL += UL[d + 1] / UL[0] * n[d];
+    VnR += UR[d + 1] / UR[0] * n[d];
+  }
+  const double PL = (g - 1.0) * (UL[V - 1] - 0.5 * m2L / UL[0]);
+  const double PR = (g - 1.0) * (UR[V - 1] - 0.5 * m2R / UR[0]);
+  const double aL = sqrt(g * PL / UL[0]), aR = sqrt(g * PR / UR[0]);
+  const double sL = fabs(VnL) + aL, sR = fabs(VnR) + aR;
+  const double eig = sL > sR ? sL : sR;
+  const double diss = 0.5 * eig * (1.0 - ph.rus_k);
+  double FbL[V][D], FbR[V][D], dissb = 0.0;
+  for (int v = 0; v < V; v++)
+  {
+    for (int d = 0; d < D; d++) FbL[v][d] = FbR[v][d] = 0.5 * w[v] * n[d];
+    UbR[v] -= diss * w[v];
+    UbL[v] += diss * w[v];
+    dissb -= w[v] * (UR[v] - UL[v]);
+  }
+  flux_conv_vjp<D>(UL, FbL, g, UbL);
+  flux_conv_vjp<D>(UR, FbR, g, UbR);
+  const double eigb = 0.5 * (1.0 - ph.rus_k) * dissb;
+  const bool left = sL > sR;
+  const double *U = left ? UL : UR;
+  double *Ub = left ? UbL : UbR;
+  const double Vn = left ? VnL : VnR, a = left ? aL : aR, P = left ? PL : PR;
+  // |Vn| + a
+  const double Vnb = (Vn < 0.0) ? -eigb : eigb;
+  const double qb = eigb / (2.0 * a);  // a = sqrt(q), q = g P / rho
+  const double ir = 1.0 / U[0];
+  pressure_vjp<D>(U, qb * g * ir, g, Ub);
+  Ub[0] -= qb * g * P * ir * ir;
+  for (int d = 0; d < D; d++) Ub[d + 1] += Vnb * n[d] * ir;
+  Ub[0] -= Vnb * Vn * ir;
+}
+
+// (UbL, UbR) += (d Fc / d (UL, UR))^T w for the Roe flux with Harten's
+// entropy fix of physics.cuh (absolute FP64 states).
+template <int D>
+ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double n[D], const double w[D + 2],
+                   const Phys<double> &ph, double UbL[D + 2], double UbR[D + 2])
+{
+  constexpr int V = D + 2;
+  const double g = ph.gamma;
+  // ---- forward recomputation ----
+  const double rL = UL[0], rR = UR[0];
+  double m2L = 0.0, m2R = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    m2L += UL[d + 1] * UL[d + 1];
+    m2R += UR[d + 1] * UR[d + 1];
+  }
+  const double PL = (g - 1.0) * (UL[V - 1] - 0.5 * m2L / rL);
+  const double PR = (g - 1.0) * (UR[V - 1] - 0.5 * m2R / rR);
+  const double sL = sqrt(rL), sR = sqrt(rR);
+  const double inv = 1.0 / (sL + sR);
+  double uL[D], uR[D], u[D], unL = 0.0, unR = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    uL[d] = UL[d + 1] / rL;
+    uR[d] = UR[d + 1] / rR;
+    u[d] = (sL * uL[d] + sR * uR[d]) * inv;
+    unL += uL[d] * n[d];
+    unR += uR[d] * n[d];
+  }
+  const double HL = (UL[V - 1] + PL) / rL, HR = (UR[V - 1] + PR) / rR;
+  const double H = (sL * HL + sR * HR) * inv;
+  double q2 = 0.0, un = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    q2 += u[d] * u[d];
+    un += u[d] * n[d];
+  }
+  double c2 = (g - 1.0) * (H - 0.5 * q2);
+  const bool clamped = !(c2 > 1e-30);
+  if (clamped) c2 = 1e-30;
+  const double a = sqrt(c2);
+  const double rho = sL * sR;
+  const double dp = PR - PL, dr = rR - rL, dun = unR - unL;
+  const double t2 = 1.0 / (2.0 * c2);
+  const double a1 = (dp - rho * a * dun) * t2;
+  const double a3 = (dp + rho * a * dun) * t2;
+  const double a2w = dr - dp / c2;
+  const double x[3] = {un - a, un, un + a};
+  const double delta = 0.1 * (fabs(un) + a);
+  double l[3];
+  bool fixed[3];
+  for (int i = 0; i < 3; i++)
+  {
+    const double ax = fabs(x[i]);
+    fixed[i] = ax < delta;
+    l[i] = fixed[i] ? (ax * ax + delta * delta) / (2.0 * delta) : ax;
+  }
+  double dvt[D], udvt = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    dvt[d] = (uR[d] - uL[d]) - dun * n[d];
+    udvt += u[d] * dvt[d];
+  }
+  // ---- reverse ----
+  double FbL[V][D], FbR[V][D], dsb[V];
+  for (int v = 0; v < V; v++)
+  {
+    for (int d = 0; d < D; d++) FbL[v][d] = FbR[v][d] = 0.5 * w[v] * n[d];
+    dsb[v] = -0.5 * w[v];
+  }
+  flux_conv_vjp<D>(UL, FbL, g, UbL);
+  flux_conv_vjp<D>(UR, FbR, g, UbR);
+  double lb[3] = {0.0, 0.0, 0.0};
+  double a1b = 0.0, a3b = 0.0, a2wb = 0.0, Hb = 0.0, ab = 0.0, unb = 0.0, q2b = 0.0, rhob = 0.0, udvtb = 0.0;
+  double ub[D], dvtb[D];
+  for (int d = 0; d < D; d++) ub[d] = dvtb[d] = 0.0;
+  {
+    const double X = dsb[V - 1];
+    lb[0] += X * a1 * (H - a * un);
+    a1b += X * l[0] * (H - a * un);
+    Hb += X * (l[0] * a1 + l[2] * a3);
+    ab += X * (-l[0] * a1 * un + l[2] * a3 * un);
+    unb += X * (-l[0] * a1 * a + l[2] * a3 * a);
+    lb[1] += X * (a2w * 0.5 * q2 + rho * udvt);
+    a2wb += X * l[1] * 0.5 * q2;
+    q2b += X * l[1] * a2w * 0.5;
+    rhob += X * l[1] * udvt;
+    udvtb += X * l[1] * rho;
+    lb[2] += X * a3 * (H + a * un);
+    a3b += X * l[2] * (H + a * un);
+  }
+  for (int d = 0; d < D; d++)
+  {
+    ub[d] += udvtb * dvt[d];
+    dvtb[d] += udvtb * u[d];
+    const double X = dsb[d + 1];
+    lb[0] += X * a1 * (u[d] - a * n[d]);
+    a1b += X * l[0] * (u[d] - a * n[d]);
+    ub[d] += X * (l[0] * a1 + l[1] * a2w + l[2] * a3);
+    ab += X * (-l[0] * a1 * n[d] + l[2] * a3 * n[d]);
+    lb[1] += X * (a2w * u[d] + rho * dvt[d]);
+    a2wb += X * l[1] * u[d];
+    rhob += X * l[1] * dvt[d];
+    dvtb[d] += X * l[1] * rho;
+    lb[2] += X * a3 * (u[d] + a * n[d]);
+    a3b += X * l[2] * (u[d] + a * n[d]);
+  }
+  {
+    const double X = dsb[0];
+    lb[0] += X * a1;
+    a1b += X * l[0];
+    lb[1] += X * a2w;
+    a2wb += X * l[1];
+    lb[2] += X * a3;
+    a3b += X * l[2];
+  }
+  double uLb[D], uRb[D], dunb = 0.0;
+  for (int d = 0; d < D; d++)
+  {
+    uRb[d] = dvtb[d];
+    uLb[d] = -dvtb[d];
+    dunb -= dvtb[d] * n[d];
+  }
+  // entropy fix and |x|
+  double deltab = 0.0;
+  for (int i = 0; i < 3; i++)
+  {
+    const double ax = fabs(x[i]);
+    double axb = lb[i];
+    if (fixed[i])
+    {
+      axb = lb[i] * ax / delta;
+      deltab += lb[i] * (delta * delta - ax * ax) / (2.0 * delta * delta);
+    }
+    const double xb = (x[i] < 0.0) ? -axb : axb;
+    unb += xb;
+    if (i == 0) ab -= xb;
+    if (i == 2) ab += xb;
+  }
+  unb += 0.1 * deltab * ((un < 0.0) ? -1.0 : 1.0);
+  ab += 0.1 * deltab;
+  // wave strengths
+  double dpb = 0.0, drb = 0.0, c2b = 0.0;
+  dpb += a1b * t2;
+  rhob -= a1b * a * dun * t2;
+  ab -= a1b * rho * dun * t2;
+  dunb -= a1b * rho * a * t2;
+  c2b -= a1b * a1 / c2;
+  dpb += a3b * t2;
+  rhob += a3b * a * dun * t2;
+  ab += a3b * rho * dun * t2;
+  dunb += a3b * rho * a * t2;
+  c2b -= a3b * a3 / c2;
+  drb += a2wb;
+  dpb -= a2wb / c2;
+  c2b += a2wb * dp / (c2 * c2);
+  c2b += ab / (2.0 * a);
+  if (!clamped)
+  {
+    Hb += (g - 1.0) * c2b;
+    q2b -= 0.5 * (g - 1.0) * c2b;
+  }
+  double sLb = rhob * sR, sRb = rhob * sL;
+  double PLb = -dpb, PRb = dpb;
+  double rLb = -drb, rRb = drb;
+  double unLb = -dunb, unRb = dunb;
+  for (int d = 0; d < D; d++) ub[d] += 2.0 * q2b * u[d] + unb * n[d];
+  double invb = 0.0;
+  {
+    const double HLb = Hb * sL * inv, HRb = Hb * sR * inv;
+    sLb += Hb * HL * inv;
+    sRb += Hb * HR * inv;
+    invb += Hb * (sL * HL + sR * HR);
+    UbL[V - 1] += HLb / rL;
+    PLb += HLb / rL;
+    rLb -= HLb * HL / rL;
+    UbR[V - 1] += HRb / rR;
+    PRb += HRb / rR;
+    rRb -= HRb * HR / rR;
+  }
+  for (int d = 0; d < D; d++)
+  {
+    uLb[d] += ub[d] * sL * inv + unLb * n[d];
+    uRb[d] += ub[d] * sR * inv + unRb * n[d];
+    sLb += ub[d] * uL[d] * inv;
+    sRb += ub[d] * uR[d] * inv;
+    invb += ub[d] * (sL * uL[d] + sR * uR[d]);
+  }
+  sLb -= invb * inv * inv;
+  sRb -= invb * inv * inv;
+  for (int d = 0; d < D; d++)
+  {
+    UbL[d + 1] += uLb[d] / rL;
+    rLb -= uLb[d] * uL[d] / rL;
+    UbR[d + 1] += uRb[d] / rR;
+    rRb -= uRb[d] * uR[d] / rR;
+  }
+  rLb += sLb / (2.0 * sL);
+  rRb += sRb / (2.0 * sR);
+  UbL[0] += rLb;
+  UbR[0] += rRb;
+  pressure_vjp<D>(UL, PLb, g, UbL);
+  pressure_vjp<D>(UR, PRb, g, UbR);
+}
+
 // Common convective flux of a face as a function of (UL, UR); boundary faces
 // (bc >= 0) take UR from the ghost state of UL.
 template <int D, typename X>
@@ -221,28 +493,20 @@ ZB_HD void conv_face(int bc, const X UL[D + 2], const X URin[D + 2], const X n[D
     rusanov<X, D>(UL, UR, n, Fc, ph);
 }
 
-// Ub_own += (d Fc / d U_own)^T w for an interior face (own = left or right).
+// Ub_own += (d Fc / d U_own)^T w for an interior face (own = left or right),
+// by the hand-written reverse of the Riemann solver.
 template <int D>
 ZB_HD void conv_face_vjp_side(const double UL[D + 2], const double UR[D + 2], const double n[D], const double w[D + 2],
-                              bool own_left, const Phys<Dual<double>> &pd, double Ub[D + 2])
+                              bool own_left, const Phys<double> &ph, double Ub[D + 2])
 {
   constexpr int V = D + 2;
-  using DD = Dual<double>;
-  DD nd[D];
-  for (int d = 0; d < D; d++) nd[d] = DD(n[d]);
-  for (int k = 0; k < V; k++)
-  {
-    DD L[V], R[V], F[V];
-    for (int v = 0; v < V; v++)
-    {
-      L[v] = DD(UL[v], (own_left && v == k) ? 1.0 : 0.0);
-      R[v] = DD(UR[v], (!own_left && v == k) ? 1.0 : 0.0);
-    }
-    conv_face<D, DD>(-1, L, R, nd, F, pd);
-    double acc = 0.0;
-    for (int v = 0; v < V; v++) acc += w[v] * F[v].d;
-    Ub[k] += acc;
-  }
+  double bL[V], bR[V];
+  for (int v = 0; v < V; v++) bL[v] = bR[v] = 0.0;
+  if (ph.fconv == 2)
+    roe_vjp<D>(UL, UR, n, w, ph, bL, bR);
+  else
+    rusanov_vjp<D>(UL, UR, n, w, ph, bL, bR);
+  for (int v = 0; v < V; v++) Ub[v] += own_left ? bL[v] : bR[v];
 }
 
 // Viscous normal flux of one trace (visc_normal) and its reverse:
@@ -261,7 +525,7 @@ ZB_HD void visc_normal_vjp(const double U[D + 2], const double dU[D + 2][D], con
 //   convective common flux with the ghost state, plus for viscous runs
 //   F_visc(UB, ghost_grad(U, dU)) . n + tau (U - UB).
 template <int D, bool VISC>
-ZB_HD void bnd_face_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+ZB_HD_COLD void bnd_face_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
                         const double w[D + 2], const Phys<Dual<double>> &pd, double Ub[D + 2], double dUb[D + 2][D])
 {
   constexpr int V = D + 2;
@@ -298,7 +562,7 @@ ZB_HD void bnd_face_vjp(int bc, const double U[D + 2], const double dU[D + 2][D]
 // Ub += (d UB / d U)^T w for the prescribed boundary state UB of the LDG
 // common solution.
 template <int D>
-ZB_HD void bnd_ucomm_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+ZB_HD_COLD void bnd_ucomm_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
                          const Phys<Dual<double>> &pd, double Ub[D + 2])
 {
   constexpr int V = D + 2;
@@ -333,7 +597,7 @@ ZB_HD void seed_param(Phys<Dual<double>> &q, int k)
 // pb[k] += d (w . phi) / d param_k for the boundary face function of
 // bnd_face_vjp.
 template <int D, bool VISC>
-ZB_HD void bnd_face_param_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+ZB_HD_COLD void bnd_face_param_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
                               const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
 {
   constexpr int V = D + 2;
@@ -369,7 +633,7 @@ ZB_HD void bnd_face_param_vjp(int bc, const double U[D + 2], const double dU[D +
 
 // pb[k] += d (w . UB) / d param_k for the LDG boundary common solution.
 template <int D>
-ZB_HD void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+ZB_HD_COLD void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
                                const Phys<Dual<double>> &pd, double pb[5])
 {
   constexpr int V = D + 2;
@@ -550,7 +814,6 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_cons
   double *sUbfp = sUb + S * V * TW;                     // [Fp][V][TW]
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
-  const Phys<Dual<double>> pd = dual_phys(a.ph);
   double pb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
   {
@@ -586,7 +849,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_cons
       double Un[V];
       gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
       const bool own_left = !(code & 1);
-      conv_face_vjp_side<D>(own_left ? Uo : Un, own_left ? Un : Uo, n, w, own_left, pd, Ub);
+      conv_face_vjp_side<D>(own_left ? Uo : Un, own_left ? Un : Uo, n, w, own_left, a.ph, Ub);
     }
     else
     {
@@ -595,8 +858,8 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_cons
       for (int v = 0; v < V; v++)
 #pragma unroll
         for (int d = 0; d < D; d++) dUz[v][d] = dUbz[v][d] = 0.0;
-      bnd_face_vjp<D, false>(-code - 1, Uo, dUz, n, w, pd, Ub, dUbz);
-      if (a.pbar) bnd_face_param_vjp<D, false>(-code - 1, Uo, dUz, n, w, pd, pb);
+      bnd_face_vjp<D, false>(-code - 1, Uo, dUz, n, w, dual_phys(a.ph), Ub, dUbz);
+      if (a.pbar) bnd_face_param_vjp<D, false>(-code - 1, Uo, dUz, n, w, dual_phys(a.ph), pb);
     }
 #pragma unroll
     for (int v = 0; v < V; v++) sUbfp[(f * V + v) * TW + l] = Ub[v];
@@ -643,7 +906,6 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
   double *sG = sdU + D * S * V * TW;                   // [D][S][V][TW] its adjoint, then tdU's
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
-  const Phys<Dual<double>> pd = dual_phys(a.ph);
   const double beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
   double pb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   {
@@ -780,7 +1042,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
       double Un[V];
       gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
       const bool own_left = !(code & 1);
-      conv_face_vjp_side<D>(own_left ? Uo : Un, own_left ? Un : Uo, n, w, own_left, pd, Ub);
+      conv_face_vjp_side<D>(own_left ? Uo : Un, own_left ? Un : Uo, n, w, own_left, a.ph, Ub);
       // LDG: (1/2 + beta) FnL + (1/2 - beta) FnR + tau (UL - UR)
       const double c = own_left ? 0.5 + beta : 0.5 - beta;
       if (c != 0.0)
@@ -795,8 +1057,8 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
     }
     else
     {
-      bnd_face_vjp<D, true>(-code - 1, Uo, dUo, n, w, pd, Ub, dUb);
-      if (a.pbar) bnd_face_param_vjp<D, true>(-code - 1, Uo, dUo, n, w, pd, pb);
+      bnd_face_vjp<D, true>(-code - 1, Uo, dUo, n, w, dual_phys(a.ph), Ub, dUb);
+      if (a.pbar) bnd_face_param_vjp<D, true>(-code - 1, Uo, dUo, n, w, dual_phys(a.ph), pb);
     }
     double *ub = a.Ubfp + (tile * Fp + f) * (int64_t)V * TW + l;
     double *dub = a.dUbfp + (tile * Fp + f) * (int64_t)V * D * TW + l;
@@ -908,8 +1170,8 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
         Uo[v] = uo[v * TW];
         Ub[v] = 0.0;
       }
-      bnd_ucomm_vjp<D>(-code - 1, Uo, n, ucb, pd, Ub);
-      if (a.pbar) bnd_ucomm_param_vjp<D>(-code - 1, Uo, n, ucb, pd, pb);
+      bnd_ucomm_vjp<D>(-code - 1, Uo, n, ucb, dual_phys(a.ph), Ub);
+      if (a.pbar) bnd_ucomm_param_vjp<D>(-code - 1, Uo, n, ucb, dual_phys(a.ph), pb);
 #pragma unroll
       for (int v = 0; v < V; v++) ub[v * TW] += Ub[v];
     }

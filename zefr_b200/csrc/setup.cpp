@@ -353,6 +353,28 @@ static Shape tensor_shape(int gmsh_type, int D, const std::vector<double> &loc, 
   return s;
 }
 
+// triangle shape functions at npts reference points (tri_setup.cpp)
+static Shape simplex_shape(int nn, const std::vector<double> &loc, int npts)
+{
+  Shape s;
+  s.nn = nn;
+  s.D = 2;
+  s.val.assign((size_t)npts * nn, 0.0);
+  s.dval.assign((size_t)2 * npts * nn, 0.0);
+  std::vector<double> v(nn), dv(2 * nn);
+  for (int pt = 0; pt < npts; pt++)
+  {
+    tri_shape(nn, &loc[(size_t)pt * 2], v.data(), dv.data());
+    for (int g = 0; g < nn; g++)
+    {
+      s.val[(size_t)pt * nn + g] = v[g];
+      s.dval[((size_t)0 * npts + pt) * nn + g] = dv[g];
+      s.dval[((size_t)1 * npts + pt) * nn + g] = dv[nn + g];
+    }
+  }
+  return s;
+}
+
 // ---------------------------------------------------------------------------
 // Metrics
 // ---------------------------------------------------------------------------
@@ -422,28 +444,43 @@ void build_plan(const zb_mesh &mesh, const zb_params &params, Plan &p)
     p.etype = ET_QUAD;
   else if (mesh.gmsh_type == 5 && mesh.nodes_per_ele == 8)
     p.etype = ET_HEX;
+  else if ((mesh.gmsh_type == 2 && mesh.nodes_per_ele == 3) || (mesh.gmsh_type == 9 && mesh.nodes_per_ele == 6))
+    p.etype = ET_TRI;
   else
     ZB_THROW(ZB_ERR_UNSUPPORTED, "element type not built: gmsh type " + std::to_string(mesh.gmsh_type));
-  if ((p.etype == ET_QUAD && p.ndims != 2) || (p.etype == ET_HEX && p.ndims != 3))
+  if ((p.etype != ET_HEX && p.ndims != 2) || (p.etype == ET_HEX && p.ndims != 3))
     ZB_THROW(ZB_ERR_MESH, "element type does not match ndims");
 
   const int D = p.ndims;
   p.order = params.order;
   p.N = params.order + 1;
   p.nvars = D + 2;
-  p.nfaces = (D == 2) ? 4 : 6;
-  p.nfpts_face = (D == 2) ? p.N : p.N * p.N;
-  p.nspts = (D == 2) ? p.N * p.N : p.N * p.N * p.N;
-  p.nfpts = p.nfaces * p.nfpts_face;
   p.neles = mesh.n_eles;
   p.tile = 8;
   p.ntiles = (p.neles + p.tile - 1) / p.tile;
   p.neles_pad = p.ntiles * p.tile;
-  p.ops = make_line_ops(p.N);
-  if (D == 2)
-    quad_tables(p);
+  if (p.etype == ET_TRI)
+  {
+    // flux reconstruction on triangles (src/tris.cpp:24-43)
+    p.nfaces = 3;
+    p.nfpts_face = p.N;
+    p.nspts = p.N * (p.N + 1) / 2;
+    p.nfpts = 3 * p.N;
+    p.ops.N = p.N;
+    tri_tables(p);
+  }
   else
-    hex_tables(p);
+  {
+    p.nfaces = (D == 2) ? 4 : 6;
+    p.nfpts_face = (D == 2) ? p.N : p.N * p.N;
+    p.nspts = (D == 2) ? p.N * p.N : p.N * p.N * p.N;
+    p.nfpts = p.nfaces * p.nfpts_face;
+    p.ops = make_line_ops(p.N);
+    if (D == 2)
+      quad_tables(p);
+    else
+      hex_tables(p);
+  }
 
   const int64_t E = p.neles;
   const int S = p.nspts, Fp = p.nfpts, nn = p.nnodes_ele;
@@ -461,8 +498,8 @@ void build_plan(const zb_mesh &mesh, const zb_params &params, Plan &p)
       for (int d = 0; d < D; d++)
         p.nodes[((size_t)n * D + d) * E + e] = mesh.coords[mesh.ele2nodes[e * nn + n] * 3 + d];
 
-  Shape shs = tensor_shape(mesh.gmsh_type, D, p.loc_spts, S);
-  Shape shf = tensor_shape(mesh.gmsh_type, D, p.loc_fpts, Fp);
+  Shape shs = (p.etype == ET_TRI) ? simplex_shape(nn, p.loc_spts, S) : tensor_shape(mesh.gmsh_type, D, p.loc_spts, S);
+  Shape shf = (p.etype == ET_TRI) ? simplex_shape(nn, p.loc_fpts, Fp) : tensor_shape(mesh.gmsh_type, D, p.loc_fpts, Fp);
 
   p.coord_spts.assign((size_t)S * D * E, 0.0);
   p.coord_fpts.assign((size_t)Fp * D * E, 0.0);
@@ -739,6 +776,15 @@ void Plan::dense_operators(std::vector<double> &oppE, std::vector<double> &oppD,
                            std::vector<double> &oppDiv_fpts) const
 {
   const int S = nspts, Fp = nfpts, D = ndims, Nn = N;
+  if (etype == ET_TRI)
+  {
+    oppE = tri_oppE;
+    oppD = tri_oppD;
+    oppD_fpts = tri_oppD_fpts;
+    oppDiv = tri_oppDiv;
+    oppDiv_fpts = tri_oppDiv_fpts;
+    return;
+  }
   oppE.assign((size_t)Fp * S, 0.0);
   oppD.assign((size_t)D * S * S, 0.0);
   oppD_fpts.assign((size_t)D * S * Fp, 0.0);

@@ -76,7 +76,14 @@ struct Plan
   std::vector<double> fnorm;     // [Fp][D][E]: left element's unit normal of the face
   std::vector<double> fdA;       // [Fp][E]: this side's dA
 
-  // Dense operators assembled from the line operators (set-up checks only)
+  // Triangles: dense FR operators in the reference layouts
+  std::vector<double> tri_oppE;        // [Fp][S]
+  std::vector<double> tri_oppD;        // [D][S][S]
+  std::vector<double> tri_oppD_fpts;   // [D][S][Fp]
+  std::vector<double> tri_oppDiv;      // [S][D][S]
+  std::vector<double> tri_oppDiv_fpts; // [S][Fp]
+
+  // Dense operators (assembled from the line operators for quads and hexes)
   void dense_operators(std::vector<double> &oppE, std::vector<double> &oppD,
                        std::vector<double> &oppD_fpts, std::vector<double> &oppDiv,
                        std::vector<double> &oppDiv_fpts) const;
@@ -88,6 +95,8 @@ void build_plan(const zb_mesh &mesh, const zb_params &params, Plan &plan);
 void read_gmsh(const std::string &path, int ndims, const std::vector<std::string> &names,
                const std::vector<int> &bcs, MeshData &out);
 void params_from_deck(const zb_deck &deck, zb_params &out);
+void tri_tables(Plan &plan);
+void tri_shape(int nn, const double *loc, double *val, double *dval);
 
 // Polynomials restated from reference include/polynomials.hpp:16-76
 double lagrange(const std::vector<double> &grid, int mode, double x);
