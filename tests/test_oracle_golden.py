@@ -17,8 +17,9 @@ def test_fixtures_present():
 def test_oracle_residual_matches_reference(name):
     g = gc.load(name)
     R = dfr_numpy.residual(g.setup(), g.U0, g.params, g.viscous)
-    # same arithmetic as the reference up to summation order: 1e-13 per variable scale
-    assert gc.rel_err(R, g.R0) < 1e-13
+    # same arithmetic as the reference up to summation order (and, on triangles,
+    # the dense 'M3' operators' rounding): 1e-12 per variable scale
+    assert gc.rel_err(R, g.R0) < 1e-12
 
 
 @pytest.mark.parametrize("name", [n for n in CASES if gc.load(n).meta["nsteps"] <= 2])
@@ -28,7 +29,7 @@ def test_oracle_rk44_matches_reference(name):
     U = g.U0
     for _ in range(g.meta["nsteps"]):
         U = dfr_numpy.rk44_step(st, U, g.params, g.viscous, g.meta["dt"])
-    assert gc.rel_err(U, g.Un) < 1e-13
+    assert gc.rel_err(U, g.Un) < 1e-12
 
 
 def test_oracle_detects_planted_error():
