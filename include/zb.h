@@ -223,12 +223,50 @@ zb_status zb_residual_norms(zb_ctx *ctx, double *out);
  * |V_fs|^2). */
 zb_status zb_functionals(zb_ctx *ctx, double *out);
 
+/* Force and moment on the wall boundaries (slip, isothermal and adiabatic
+ * walls) of FRSolver::compute_moments (src/solver.cpp:7600-7811), FP64
+ * device reduction over the current state: out[0..2] force, out[3..5]
+ * moment about the origin.  Per wall flux point w (P n - tau n) dA with the
+ * element's own trace and extrapolated corrected gradient; in 3D each flux
+ * point's own state is used where the reference reads flux point 0's
+ * (src/solver.cpp:7716-7720). */
+zb_status zb_wall_force(zb_ctx *ctx, double *out);
+
 /* Replace the free-stream state the far-field and characteristic boundaries
  * prescribe (input rho_fs, V_fs, P_fs of the reference, src/input.cpp:463-539
  * after non-dimensionalisation); takes effect from the next launch.  Used to
  * differentiate with respect to the free-stream conditions.  No reference
  * counterpart (the reference fixes them at set-up). */
 zb_status zb_set_freestream(zb_ctx *ctx, double rho_fs, const double *V_fs, double P_fs);
+
+/* ---- Batched stepping of independent cases ----
+ * Many Euler cases on quadrilaterals (each its own context: mesh, order
+ * P1-P5, state, dt) advance together: one persistent launch per RK stage
+ * covers every tile of every case, and the four stages of a step replay as
+ * one CUDA graph.  The contexts stay owned by the caller and must outlive the
+ * batch; do not use them while batched work is queued (zb_batch_synchronize
+ * first).  No reference counterpart (the reference steps one mesh). */
+typedef struct zb_batch zb_batch;
+typedef struct zb_batch_config {
+  int threads;        /* threads per CTA: 128 or 256 */
+  int blocks_per_sm;  /* persistent CTAs per SM */
+  int order;          /* work order: 0 by polynomial order (costliest first), 1 case-major */
+  double ms_per_step; /* autotuner: measured time of one RK44 step */
+} zb_batch_config;
+
+zb_status zb_batch_create(zb_ctx *const *ctxs, int n, zb_batch **out);
+void zb_batch_destroy(zb_batch *batch);
+/* Time every launch shape on `steps` steps from the current states (which are
+ * restored afterwards) and keep the fastest; *chosen may be NULL. */
+zb_status zb_batch_autotune(zb_batch *batch, int steps, zb_batch_config *chosen);
+zb_status zb_batch_set_config(zb_batch *batch, const zb_batch_config *cfg);
+/* nsteps RK44 steps of every case; use_graph = 1 replays the captured graph,
+ * 0 launches the four stages directly.  Returns once queued. */
+zb_status zb_batch_step(zb_batch *batch, int nsteps, int use_graph);
+/* One RK stage of every case (completes before returning). */
+zb_status zb_batch_stage(zb_batch *batch, unsigned stage);
+zb_status zb_batch_synchronize(zb_batch *batch);
+int64_t zb_batch_launch_count(const zb_batch *batch);
 
 /* Adjoint (vector-Jacobian product) of the residual at the current state:
  * Ubar = (d divF / d U)^T lam, both in the strided layout of zb_set_state,

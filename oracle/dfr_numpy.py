@@ -471,6 +471,65 @@ def functionals(st: Setup, U: np.ndarray, weights: np.ndarray, p: Dict[str, floa
     return {"ke": ke, "enstrophy": en, "volume": float(jw.sum())}
 
 
+WALL_BCS = (BC_SLIP, BC_ISO, BC_ADI, BC_ISO_MOVE, BC_ADI_MOVE)
+
+
+def wall_force(st: Setup, U: np.ndarray, wfpt: np.ndarray, coord_fpts: np.ndarray, p: Dict[str, float],
+               viscous: bool):
+    """Force and moment (about the origin) on wall boundaries of
+    FRSolver::compute_moments (src/solver.cpp:7600-7811): per wall flux point
+    w * (P n - tau n) * dA from the element's own trace and its extrapolated
+    corrected gradient.  In 3D the reference reads the state of flux point 0
+    for the viscous stress (src/solver.cpp:7716-7720); this restatement uses
+    each flux point's own state.  wfpt [Fp] face quadrature weights,
+    coord_fpts [Fp, D, E]."""
+    S, V, E = U.shape
+    D = st.ndims
+    g = p["gamma"]
+    Ufp = np.einsum("fs,sve->fve", st.oppE, U)
+    bc = np.where(st.partner < 0, -1 - st.partner, 0)
+    wall = np.isin(bc, WALL_BCS)
+    rho = Ufp[:, 0]
+    vel = [Ufp[:, d + 1] / rho for d in range(D)]
+    P = (g - 1.0) * (Ufp[:, D + 1] - 0.5 * rho * sum(v * v for v in vel))
+    w = wfpt[:, None] * st.dA
+    force = np.zeros(3)
+    moment = np.zeros(3)
+    fx = np.zeros((3,) + P.shape)
+    for d in range(D):
+        fx[d] = w * P * st.norm[:, d]
+    if viscous:
+        dUs = physical_gradient(st, U, p)                     # [D, S, V, E]
+        dUf = np.einsum("fs,dsve->dfve", st.oppE, dUs)         # [D, Fp, V, E]
+        if p["fix_vis"]:
+            mu = np.full_like(rho, p["mu"])
+        else:
+            e_int = Ufp[:, D + 1] / rho - 0.5 * sum(v * v for v in vel)
+            rt = (g - 1.0) * e_int / p["rt"]
+            mu = p["mu"] * rt ** 1.5 * (1.0 + p["c_sth"]) / (rt + p["c_sth"])
+        gv = [[(dUf[j, :, i + 1] - dUf[j, :, 0] * vel[i]) / rho for j in range(D)] for i in range(D)]
+        diag = sum(gv[i][i] for i in range(D)) / 3.0
+        tau = [[None] * D for _ in range(D)]
+        for i in range(D):
+            for j in range(D):
+                tau[i][j] = 2.0 * mu * (gv[i][i] - diag) if i == j else mu * (gv[i][j] + gv[j][i])
+        for i in range(D):
+            taun = sum(tau[i][j] * st.norm[:, j] for j in range(D))
+            fx[i] = fx[i] - w * taun
+    for d in range(D):
+        force[d] = float(fx[d][wall].sum())
+    x = coord_fpts[:, 0]
+    y = coord_fpts[:, 1]
+    if D == 2:
+        moment[2] = float((x * fx[1] - y * fx[0])[wall].sum())
+    else:
+        z = coord_fpts[:, 2]
+        moment[0] = float((y * fx[2] - z * fx[1])[wall].sum())
+        moment[1] = float((z * fx[0] - x * fx[2])[wall].sum())
+        moment[2] = float((x * fx[1] - y * fx[0])[wall].sum())
+    return force, moment
+
+
 def rk44_step(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, dt: float) -> np.ndarray:
     """One explicit RK44 step (FRSolver::step_RK, src/solver.cpp:2864-3097)."""
     alpha = [0.5, 0.5, 1.0]

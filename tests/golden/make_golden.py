@@ -14,6 +14,7 @@ Usage:  python tests/golden/make_golden.py  (needs oracle/_ref/libzefr_ref.so)
 from __future__ import annotations
 
 import json
+import math
 import os
 import sys
 import tempfile
@@ -53,6 +54,10 @@ def _cases():
     def shear(X, g):
         return ics.double_shear_layer(X * 0.1 + 0.5, mach=0.2, gamma=g)
 
+    def angled_state(X, g):
+        c = 0.2 * np.sqrt(g)
+        return ics.uniform(X, 1.0, (c * math.cos(math.pi / 6), c * math.sin(math.pi / 6)), 1.0, g)
+
     def shear_unit(X, g):
         return ics.double_shear_layer(X, mach=0.2, gamma=g)
 
@@ -82,8 +87,13 @@ def _cases():
         "tri_p4_ns_jitter": (lambda: meshgen.box_tris(4, seed=3), 2, 4, True, per,
                              dict(cyl_deck, Re_fs=1000, prandtl=0.71), shear_unit, 2),
         "tri_p2_euler_vortex": (lambda: meshgen.box_tris(5, -5.0, 5.0, seed=1), 2, 2, False, per, eul, vortex, 2),
+        # free stream at 30 degrees: no boundary of the box is tangent to the
+        # flow, where the characteristic condition's inflow/outflow switch
+        # would follow the rounding of the normal
         "tri_p3_euler_char": (lambda: meshgen.box_tris(4, -2.0, 2.0, seed=2, bnd="FARFIELD"), 2, 3, False,
-                              {"FARFIELD": "char"}, dict(eul, mach_fs=0.2), cyl_state, 2),
+                              {"FARFIELD": "char"},
+                              dict(eul, mach_fs=0.2, nx_fs=math.cos(math.pi / 6), ny_fs=math.sin(math.pi / 6)),
+                              angled_state, 2),
         "tri_p1_ns_adi": (lambda: meshgen.box_tris(4, 0.0, 1.0, seed=4, bnd="WALL"), 2, 1, True,
                           {"WALL": "wall_ns_adi"}, cyl_deck, shear_unit, 2),
     }
@@ -139,7 +149,11 @@ def make_case(name, spec, tmp):
         U0 = ics.uniform(X, p["rho_fs"], (p["V_fs0"], p["V_fs1"], p["V_fs2"]), p["P_fs"], g)
     else:
         U0 = state_fn(X, g)
-    U0 = ics.perturb(U0, 1e-3, seed=zlib.crc32(name.encode()))
+    # Triangles: 5% perturbations, so residuals are not a 1e-3 difference of
+    # O(1) fluxes; their dense operators come out of a Vandermonde inverse
+    # that agrees with the reference's (Eigen LU) only to rounding.
+    amp = 5e-2 if name.startswith("tri_") else 1e-3
+    U0 = ics.perturb(U0, amp, seed=zlib.crc32(name.encode()))
     R0 = r.residual(U0, 0)
     r.set_state(U0)
     r.update(nsteps)

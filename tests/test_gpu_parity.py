@@ -63,7 +63,8 @@ def _ref_params(viscous, mu=0.0, ldg_b=0.5, ldg_tau=0.1, V_fs=(0.3, 0.0, 0.0)):
             "viscous": float(viscous)}
 
 
-@pytest.mark.parametrize("case", ["quad32_p3_euler", "hex6_p3_ns", "cyl_12x24_p3_ns", "quad_jitter_p4_ns"])
+@pytest.mark.parametrize("case", ["quad32_p3_euler", "hex6_p3_ns", "cyl_12x24_p3_ns", "quad_jitter_p4_ns",
+                                  "tri32_p4_ns"])
 def test_residual_matches_oracle_larger(case):
     if case == "quad32_p3_euler":
         mesh, order, visc, bounds = meshgen.box_quads(32, 32), 3, False, {"PERIODIC": "periodic"}
@@ -79,6 +80,12 @@ def test_residual_matches_oracle_larger(case):
         bounds = {"WALL": "wall_ns_adi", "FARFIELD": "char"}
         p = _ref_params(True, mu=0.2 * np.sqrt(1.4) / 100.0, V_fs=(0.2 * np.sqrt(1.4), 0.0, 0.0))
         mk = lambda X: ics.uniform(X, 1.0, (0.2 * np.sqrt(1.4), 0.0), 1.0)
+    elif case == "tri32_p4_ns":
+        # the triangle workload's shape at 32 x 32 (2048 triangles), jittered 15%
+        mesh, order, visc = meshgen.box_tris(32, seed=5), 4, True
+        bounds = {"PERIODIC": "periodic"}
+        p = _ref_params(True, mu=0.2 * np.sqrt(1.4) / 1000.0, ldg_tau=0.1)
+        mk = lambda X: ics.double_shear_layer(X, mach=0.2)
     else:
         mesh = meshgen.jitter_interior(meshgen.box_quads(10, 9, 0.0, 1.0, 0.0, 1.0), 0.02, 3)
         order, visc, bounds = 4, True, {"PERIODIC": "periodic"}
@@ -95,7 +102,8 @@ def test_residual_matches_oracle_larger(case):
 
 
 @pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "hex_p3_ns_tgv", "cyl_p3_ns_char_adi", "quad_p2_ns_jitter",
-                                  "hex_p2_euler_jitter", "cyl_p2_ns_iso_farfield_b03"])
+                                  "hex_p2_euler_jitter", "cyl_p2_ns_iso_farfield_b03", "tri_p4_ns_jitter",
+                                  "tri_p3_euler_char"])
 def test_mixed_precision_error(name):
     g = gc.load(name)
     s = solver_for(g, precision="mixed")
@@ -148,7 +156,8 @@ def test_mixed_tgv_kinetic_energy_history():
     assert np.abs(eps32 - eps64).max() / np.abs(eps64).max() < 1e-3
 
 
-@pytest.mark.parametrize("name", ["hex_p3_ns_tgv", "quad_p2_ns_jitter", "cyl_p3_ns_char_adi", "quad_p3_euler_vortex"])
+@pytest.mark.parametrize("name", ["hex_p3_ns_tgv", "quad_p2_ns_jitter", "cyl_p3_ns_char_adi", "quad_p3_euler_vortex",
+                                  "tri_p4_ns_jitter"])
 def test_functionals_match_oracle(name):
     g = gc.load(name)
     s = solver_for(g)
@@ -196,7 +205,8 @@ def test_free_stream_preservation(fconv):
     assert np.abs(R).max() < 1e-11
 
 
-@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "hex_p3_ns_tgv", "cyl_p3_ns_char_adi", "hex_p2_euler_jitter"])
+@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "hex_p3_ns_tgv", "cyl_p3_ns_char_adi", "hex_p2_euler_jitter",
+                                  "tri_p4_ns_jitter", "tri_p3_euler_char"])
 def test_roe_matches_numpy_restatement(name):
     """Roe has no reference counterpart: the CUDA Roe residual is checked
     against the numpy restatement of the same published method (1e-12)."""
@@ -204,6 +214,35 @@ def test_roe_matches_numpy_restatement(name):
     R = solver_for(g, fconv="roe").residual(g.U0, 0)
     Ro = dfr_numpy.residual(g.setup(), g.U0, g.params, g.viscous, fconv="roe")
     assert gc.rel_err(R, Ro) < TOL_FP64
+
+
+@pytest.mark.parametrize("fconv", ["rusanov", "roe"])
+def test_free_stream_preservation_triangles(fconv):
+    """Uniform flow on jittered triangles: the common flux equals the
+    extrapolated normal flux, so the 'M3' correction cancels it."""
+    mesh = meshgen.box_tris(8, seed=2)
+    s = FRSolver(mesh, make_params(4, True, mu=1e-3, fconv=fconv), {"PERIODIC": "periodic"})
+    X = s.plan.get("coord_spts").reshape(s.nspts, 2, s.neles)
+    R = s.residual(ics.uniform(X, 1.2, (0.3, -0.2), 0.9), 0)
+    assert np.abs(R).max() < 1e-11
+
+
+def test_triangle_volume_divergence_option():
+    """tri_volume_div = 1 adds the volume divergence the reference's triangle
+    oppDiv lacks: a linear pressure field then gives d p/dx per unit volume."""
+    mesh = meshgen.box_tris(6, -1.0, 1.0, seed=1, jitter=0.0)
+    p = make_params(3, False)
+    p.tri_volume_div = 1
+    s = FRSolver(mesh, p, {"PERIODIC": "periodic"})
+    X = s.plan.get("coord_spts").reshape(s.nspts, 2, s.neles)
+    det = s.plan.get("jaco_det_spts").reshape(s.nspts, s.neles)
+    U = np.zeros(s.state_shape)
+    U[:, 0] = 1.0
+    U[:, 3] = (1.0 + 0.01 * X[:, 0]) / 0.4
+    R = s.residual(U, 0)
+    cx, cy = X[:, 0].mean(0), X[:, 1].mean(0)
+    inner = (np.abs(cx) < 0.6) & (np.abs(cy) < 0.6)
+    assert np.allclose(R[:, 1, inner] / det[:, inner], 0.01, rtol=1e-10, atol=1e-12)
 
 
 def test_device_pointer_state_roundtrip():
@@ -254,3 +293,23 @@ def test_kernels_launched():
     s.step(1)
     # viscous RK44 step: two kernels per stage, extrapolation fused into the second
     assert s.launch_count() - n0 == 8
+
+
+@pytest.mark.parametrize("name", ["cyl_p3_ns_char_adi", "cyl_p2_ns_iso_farfield_b03", "cyl_p3_euler_slip_char",
+                                  "tri_p1_ns_adi"])
+def test_wall_force_matches_oracle(name):
+    g = gc.load(name)
+    s = solver_for(g)
+    s.set_state(g.U0)
+    out = s.wall_force()
+    st = g.setup()
+    w1 = np.polynomial.legendre.leggauss(g.order + 1)[1]
+    Fp = st.oppE.shape[0]
+    wf = np.array([w1[f % (g.order + 1)] for f in range(Fp)])
+    S, V, E = g.U0.shape
+    cfp = s.plan.get("coord_fpts").reshape(Fp, g.meta["ndims"], E)
+    F, M = dfr_numpy.wall_force(st, g.U0, wf, cfp, g.params, g.viscous)
+    scale = np.abs(F).max()
+    assert scale > 0
+    assert np.abs(out["force"] - F).max() <= 1e-12 * scale
+    assert np.abs(out["moment"] - M).max() <= 1e-12 * max(np.abs(M).max(), scale)

@@ -33,7 +33,9 @@ EXPORTED = [
     "zb_destroy", "zb_info_get", "zb_set_stream", "zb_set_dt", "zb_set_state", "zb_get_state",
     "zb_compute_residual", "zb_get_residual", "zb_rk_stage", "zb_step", "zb_residual_norms",
     "zb_synchronize", "zb_launch_count", "zb_profile_enable", "zb_profile_read", "zb_kernel_name",
-    "zb_compute_residual_noalloc", "zb_functionals", "zb_vjp", "zb_set_freestream",
+    "zb_compute_residual_noalloc", "zb_functionals", "zb_vjp", "zb_set_freestream", "zb_wall_force",
+    "zb_batch_create", "zb_batch_destroy", "zb_batch_autotune", "zb_batch_set_config", "zb_batch_step",
+    "zb_batch_stage", "zb_batch_synchronize", "zb_batch_launch_count",
 ]
 ZB_NKERNELS = 11
 
@@ -58,6 +60,11 @@ class ZbParams(ctypes.Structure):
         ("R_ref", ctypes.c_double), ("V_wall", ctypes.c_double * 3), ("dt", ctypes.c_double),
         ("tri_volume_div", ctypes.c_int),
     ]
+
+
+class ZbBatchConfig(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_int), ("blocks_per_sm", ctypes.c_int), ("order", ctypes.c_int),
+                ("ms_per_step", ctypes.c_double)]
 
 
 class ZbDeck(ctypes.Structure):
@@ -128,6 +135,17 @@ def lib() -> ctypes.CDLL:
         L.zb_kernel_name.argtypes = [ctypes.c_int]
         L.zb_compute_residual_noalloc.argtypes = [vp, dp, dp, vp]
         L.zb_functionals.argtypes = [vp, dp]
+        L.zb_wall_force.argtypes = [vp, dp]
+        L.zb_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
+        L.zb_batch_destroy.argtypes = [vp]
+        L.zb_batch_destroy.restype = None
+        L.zb_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ZbBatchConfig)]
+        L.zb_batch_set_config.argtypes = [vp, ctypes.POINTER(ZbBatchConfig)]
+        L.zb_batch_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.zb_batch_stage.argtypes = [vp, ctypes.c_uint]
+        L.zb_batch_synchronize.argtypes = [vp]
+        L.zb_batch_launch_count.argtypes = [vp]
+        L.zb_batch_launch_count.restype = i64
         L.zb_set_freestream.argtypes = [vp, ctypes.c_double, dp, ctypes.c_double]
         L.zb_vjp.argtypes = [vp, dp, dp, i64, i64, i64, ctypes.c_int, dp]
         _lib = L

@@ -67,6 +67,8 @@ static void launch_vjp_impl(Ctx &c, bool params)
 
 void bind_vjp(Ctx &c)
 {
+  c.launch_vjp = nullptr;
+  if (c.plan.etype == ET_TRI) return;  // tensor-product elements only
   // the adjoint's shared memory fits hexahedra up to P3
 #define ZB_BIND(DD, NN) \
   if (c.D == DD && c.N == NN) { c.launch_vjp = &launch_vjp_impl<DD, NN>; return; }

@@ -1,0 +1,394 @@
+// Batched RK stepping of many independent Euler cases on quadrilaterals: one
+// persistent launch per RK stage covers every tile of every case, the four
+// stages of a step are captured once as a CUDA graph, and a small autotuner
+// picks the launch shape.
+//
+// Each case is an ordinary context (its own mesh, order 1-5, state, time
+// step and reference state); the batch only builds per-stage descriptors of
+// their buffers.  A work item is one tile (8 elements) of one case; a CTA
+// walks the item list with a grid stride and runs the tile with the kernel
+// body of its order (euler_tile, the body of the single-case k_euler), so a
+// stage of the batch computes exactly what the cases' own stages compute.
+// Reference: FRSolver::step_RK (src/solver.cpp:2864-3097) per case.
+#include <algorithm>
+#include <chrono>
+
+#include "ctx_impl.cuh"
+
+namespace zb {
+
+using dev::Args;
+using dev::LineOpsT;
+using dev::Shape;
+using dev::TW;
+
+constexpr int kBatchMaxN = 6;
+
+template <typename T, typename A>
+struct BatchCase
+{
+  Args<T, A> a;
+  int N;
+  int pad;
+  A ops[kBatchMaxN * kBatchMaxN + 4 * kBatchMaxN];  // LineOpsT<A, N> laid out flat
+};
+
+template <typename T, typename A>
+__global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__restrict__ cases,
+                                                     const int2 *__restrict__ items, int nitems)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x)
+  {
+    const int2 w = items[it];
+    const BatchCase<T, A> &bc = cases[w.x];
+    switch (bc.N)
+    {
+#define ZB_BATCH_N(NN)                                                                                         \
+  case NN:                                                                                                     \
+    dev::euler_tile<T, A, 2, NN>(bc.a, *reinterpret_cast<const LineOpsT<A, NN> *>(bc.ops), w.y, smem_raw); \
+    break;
+      ZB_BATCH_N(2) ZB_BATCH_N(3) ZB_BATCH_N(4) ZB_BATCH_N(5) ZB_BATCH_N(6)
+#undef ZB_BATCH_N
+      default: break;
+    }
+    __syncthreads();
+  }
+}
+
+static size_t euler_smem_bytes(int N, size_t asz)
+{
+  switch (N)
+  {
+    case 2: return dev::euler_smem_elems<2, 2>() * asz;
+    case 3: return dev::euler_smem_elems<2, 3>() * asz;
+    case 4: return dev::euler_smem_elems<2, 4>() * asz;
+    case 5: return dev::euler_smem_elems<2, 5>() * asz;
+    default: return dev::euler_smem_elems<2, 6>() * asz;
+  }
+}
+
+struct Batch
+{
+  std::vector<Ctx *> ctx;
+  int prec = ZB_FP64;
+  size_t asz = 8;
+  cudaStream_t stream = nullptr;
+  void *cases[4] = {nullptr, nullptr, nullptr, nullptr};  // BatchCase arrays, one per stage
+  int2 *items = nullptr;
+  int nitems = 0;
+  std::vector<int> parity;  // Ufp parity of every case the descriptors assume
+  size_t smem = 0;
+  int sms = 148;
+  zb_batch_config cfg{256, 4, 0, 0.0};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches = 0;
+};
+
+template <typename T, typename A>
+static void build_cases(Batch &b)
+{
+  const size_t n = b.ctx.size();
+  std::vector<BatchCase<T, A>> h(n);
+  for (unsigned st = 0; st < 4; st++)
+  {
+    for (size_t i = 0; i < n; i++)
+    {
+      Ctx &c = *b.ctx[i];
+      StageCfg sc;
+      sc.stage = st;
+      sc.rk_mode = (st + 1 < 4) ? 1 : 2;
+      sc.save_ini = (st == 0);
+      sc.extrap_next = 1;
+      const int cur0 = c.cur;
+      c.cur = b.parity[i] ^ (int)(st & 1);
+      std::memset(&h[i], 0, sizeof(h[i]));
+      h[i].a = make_args<T, A>(c, sc);
+      c.cur = cur0;
+      h[i].N = c.N;
+      const Plan &p = c.plan;
+      const int N = c.N;
+      A *o = h[i].ops;
+      for (int k = 0; k < N * N; k++) o[k] = (A)p.ops.D[k];
+      for (int k = 0; k < N; k++)
+      {
+        o[N * N + k] = (A)p.ops.Em[k];
+        o[N * N + N + k] = (A)p.ops.Ep[k];
+        o[N * N + 2 * N + k] = (A)p.ops.Dbm[k];
+        o[N * N + 3 * N + k] = (A)p.ops.Dbp[k];
+      }
+    }
+    if (!b.cases[st])
+    {
+      cudaError_t e = cudaMalloc(&b.cases[st], n * sizeof(BatchCase<T, A>));
+      if (e != cudaSuccess) ZB_THROW(ZB_ERR_NOMEM, "batch descriptors");
+    }
+    CK(cudaMemcpy(b.cases[st], h.data(), n * sizeof(BatchCase<T, A>), cudaMemcpyHostToDevice));
+  }
+}
+
+// Work order 0: items sorted by order (costliest first), cases interleaved
+// within an order; order 1: case-major.
+static void build_items(Batch &b, int order)
+{
+  std::vector<int2> it;
+  const int n = (int)b.ctx.size();
+  if (order == 1)
+  {
+    for (int i = 0; i < n; i++)
+      for (int64_t t = 0; t < b.ctx[i]->ntiles; t++) it.push_back(make_int2(i, (int)t));
+  }
+  else
+  {
+    for (int N = kBatchMaxN; N >= 2; N--)
+    {
+      int64_t maxt = 0;
+      for (int i = 0; i < n; i++)
+        if (b.ctx[i]->N == N) maxt = std::max(maxt, b.ctx[i]->ntiles);
+      for (int64_t t = 0; t < maxt; t++)
+        for (int i = 0; i < n; i++)
+          if (b.ctx[i]->N == N && t < b.ctx[i]->ntiles) it.push_back(make_int2(i, (int)t));
+    }
+  }
+  if (it.size() > (size_t)INT32_MAX) ZB_THROW(ZB_ERR_UNSUPPORTED, "batch too large");
+  if (b.items) cudaFree(b.items);
+  b.items = nullptr;
+  CK(cudaMalloc(&b.items, it.size() * sizeof(int2)));
+  CK(cudaMemcpy(b.items, it.data(), it.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  b.nitems = (int)it.size();
+}
+
+template <typename T, typename A>
+static void launch_stage_t(Batch &b, unsigned st)
+{
+  const int blocks = std::max(1, std::min(b.nitems, b.cfg.blocks_per_sm * b.sms));
+  k_batch_euler<T, A><<<blocks, b.cfg.threads, b.smem, b.stream>>>((const BatchCase<T, A> *)b.cases[st], b.items,
+                                                                    b.nitems);
+  b.launches++;
+  CK(cudaGetLastError());
+}
+
+static void launch_stage(Batch &b, unsigned st)
+{
+  if (b.prec == ZB_FP64)
+    launch_stage_t<double, double>(b, st);
+  else
+    launch_stage_t<float, float>(b, st);
+}
+
+static void drop_graph(Batch &b)
+{
+  if (b.exec) cudaGraphExecDestroy(b.exec);
+  if (b.graph) cudaGraphDestroy(b.graph);
+  b.exec = nullptr;
+  b.graph = nullptr;
+}
+
+static void build_graph(Batch &b)
+{
+  drop_graph(b);
+  CK(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
+  for (unsigned st = 0; st < 4; st++)
+  {
+    const int blocks = std::max(1, std::min(b.nitems, b.cfg.blocks_per_sm * b.sms));
+    if (b.prec == ZB_FP64)
+      k_batch_euler<double, double><<<blocks, b.cfg.threads, b.smem, b.stream>>>(
+          (const BatchCase<double, double> *)b.cases[st], b.items, b.nitems);
+    else
+      k_batch_euler<float, float><<<blocks, b.cfg.threads, b.smem, b.stream>>>(
+          (const BatchCase<float, float> *)b.cases[st], b.items, b.nitems);
+  }
+  cudaError_t e = cudaStreamEndCapture(b.stream, &b.graph);
+  if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  CK(cudaGraphInstantiate(&b.exec, b.graph, 0));
+}
+
+// Make every case ready for batched stages from stage `first`: its own
+// queued work done, its traces current, and the descriptors built for the
+// trace parity its stage 0 had (parity flips once per stage).
+static void prepare(Batch &b, unsigned first)
+{
+  bool stale = b.parity.empty();
+  for (size_t i = 0; i < b.ctx.size(); i++)
+  {
+    Ctx &c = *b.ctx[i];
+    if (!c.ufp_valid)
+    {
+      c.launch_extrap(c);
+      c.ufp_valid = true;
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    if (!stale && b.parity[i] != (c.cur ^ (int)(first & 1))) stale = true;
+  }
+  if (!stale) return;
+  b.parity.resize(b.ctx.size());
+  for (size_t i = 0; i < b.ctx.size(); i++) b.parity[i] = b.ctx[i]->cur ^ (int)(first & 1);
+  if (b.prec == ZB_FP64)
+    build_cases<double, double>(b);
+  else
+    build_cases<float, float>(b);
+  drop_graph(b);
+}
+
+Batch *batch_create(Ctx *const *ctxs, int n)
+{
+  if (n <= 0 || !ctxs) ZB_THROW(ZB_ERR_ARG, "empty batch");
+  std::unique_ptr<Batch> b(new Batch());
+  int dev0 = -1;
+  for (int i = 0; i < n; i++)
+  {
+    Ctx *c = ctxs[i];
+    if (!c) ZB_THROW(ZB_ERR_ARG, "null context in batch");
+    if (c->plan.etype != ET_QUAD || c->plan.params.viscous)
+      ZB_THROW(ZB_ERR_UNSUPPORTED, "the batched stage is built for Euler on quadrilaterals");
+    if (c->N < 2 || c->N > kBatchMaxN) ZB_THROW(ZB_ERR_UNSUPPORTED, "batched orders are P1-P5");
+    if (i == 0)
+    {
+      b->prec = c->prec;
+      dev0 = c->dev;
+    }
+    else if (c->prec != b->prec || c->dev != dev0)
+      ZB_THROW(ZB_ERR_ARG, "batched contexts must share precision and device");
+    b->ctx.push_back(c);
+  }
+  b->asz = (b->prec == ZB_FP64) ? sizeof(double) : sizeof(float);
+  int maxN = 2;
+  for (Ctx *c : b->ctx) maxN = std::max(maxN, c->N);
+  b->smem = euler_smem_bytes(maxN, b->asz);
+  CK(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev0));
+  CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  if (b->prec == ZB_FP64)
+    CK(cudaFuncSetAttribute(k_batch_euler<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+  else
+    CK(cudaFuncSetAttribute(k_batch_euler<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+  build_items(*b, b->cfg.order);
+  return b.release();
+}
+
+void batch_destroy(Batch *b)
+{
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  drop_graph(*b);
+  for (void *p : b->cases)
+    if (p) cudaFree(p);
+  if (b->items) cudaFree(b->items);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+void batch_stage(Batch *b, unsigned stage)
+{
+  if (stage > 3) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  prepare(*b, stage);
+  // a lone stage flips every case's trace parity
+  launch_stage(*b, stage);
+  CK(cudaStreamSynchronize(b->stream));
+  for (Ctx *c : b->ctx) c->cur ^= 1;
+}
+
+void batch_step(Batch *b, int nsteps, int use_graph)
+{
+  if (nsteps < 0) ZB_THROW(ZB_ERR_ARG, "negative step count");
+  prepare(*b, 0);
+  if (use_graph && !b->exec) build_graph(*b);
+  for (int i = 0; i < nsteps; i++)
+  {
+    if (use_graph)
+    {
+      CK(cudaGraphLaunch(b->exec, b->stream));
+      b->launches += 4;
+    }
+    else
+      for (unsigned st = 0; st < 4; st++) launch_stage(*b, st);
+  }
+}
+
+void batch_sync(Batch *b) { CK(cudaStreamSynchronize(b->stream)); }
+
+int64_t batch_launches(const Batch *b) { return b->launches; }
+
+// Time each candidate launch shape on a few graph-replayed steps from the
+// current state, restore the state, keep the fastest.
+void batch_autotune(Batch *b, int steps, zb_batch_config *out)
+{
+  if (steps < 1) steps = 1;
+  prepare(*b, 0);
+  // save the states (and compensated remainders) the trials overwrite
+  std::vector<void *> saveU(b->ctx.size(), nullptr), saveC(b->ctx.size(), nullptr);
+  for (size_t i = 0; i < b->ctx.size(); i++)
+  {
+    Ctx &c = *b->ctx[i];
+    const size_t bytes = (size_t)c.ntiles * c.S * c.V * TW * c.tsz;
+    CK(cudaMalloc(&saveU[i], bytes));
+    CK(cudaMemcpyAsync(saveU[i], c.U, bytes, cudaMemcpyDeviceToDevice, b->stream));
+    if (c.Ucomp)
+    {
+      CK(cudaMalloc(&saveC[i], bytes));
+      CK(cudaMemcpyAsync(saveC[i], c.Ucomp, bytes, cudaMemcpyDeviceToDevice, b->stream));
+    }
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int threads[] = {128, 256};
+  const int bps[] = {2, 4, 8, 16};
+  const int orders[] = {0, 1};
+  zb_batch_config best{0, 0, 0, 1e300};
+  for (int order : orders)
+  {
+    build_items(*b, order);
+    for (int th : threads)
+      for (int bp : bps)
+      {
+        b->cfg.threads = th;
+        b->cfg.blocks_per_sm = bp;
+        b->cfg.order = order;
+        build_graph(*b);
+        CK(cudaGraphLaunch(b->exec, b->stream));  // warm-up
+        CK(cudaEventRecord(e0, b->stream));
+        for (int s = 0; s < steps; s++) CK(cudaGraphLaunch(b->exec, b->stream));
+        CK(cudaEventRecord(e1, b->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        const double per = ms / steps;
+        if (per < best.ms_per_step) best = zb_batch_config{th, bp, order, per};
+      }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (size_t i = 0; i < b->ctx.size(); i++)
+  {
+    Ctx &c = *b->ctx[i];
+    const size_t bytes = (size_t)c.ntiles * c.S * c.V * TW * c.tsz;
+    CK(cudaMemcpyAsync(c.U, saveU[i], bytes, cudaMemcpyDeviceToDevice, b->stream));
+    if (saveC[i]) CK(cudaMemcpyAsync(c.Ucomp, saveC[i], bytes, cudaMemcpyDeviceToDevice, b->stream));
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  for (size_t i = 0; i < b->ctx.size(); i++)
+  {
+    cudaFree(saveU[i]);
+    if (saveC[i]) cudaFree(saveC[i]);
+    b->ctx[i]->ufp_valid = false;  // traces of the restored state are recomputed
+  }
+  b->cfg = best;
+  build_items(*b, best.order);
+  drop_graph(*b);
+  b->parity.clear();
+  if (out) *out = best;
+}
+
+void batch_config(Batch *b, const zb_batch_config *cfg)
+{
+  if (cfg->threads != 128 && cfg->threads != 256) ZB_THROW(ZB_ERR_ARG, "threads must be 128 or 256");
+  if (cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 64) ZB_THROW(ZB_ERR_ARG, "blocks_per_sm out of range");
+  if (cfg->order != 0 && cfg->order != 1) ZB_THROW(ZB_ERR_ARG, "order must be 0 or 1");
+  CK(cudaStreamSynchronize(b->stream));
+  b->cfg = *cfg;
+  build_items(*b, cfg->order);
+  drop_graph(*b);
+}
+
+}  // namespace zb

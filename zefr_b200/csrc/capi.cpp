@@ -3,6 +3,8 @@
 // thread-local message, the C-ABI analogue of the reference's ThrowException
 // (include/macros.hpp:52-54).
 #include <cstring>
+#include <memory>
+#include <vector>
 #include <string>
 
 #include "context.hpp"
@@ -321,6 +323,76 @@ zb_status zb_functionals(zb_ctx *ctx, double *out)
   })
 }
 
+zb_status zb_batch_create(zb_ctx *const *ctxs, int n, zb_batch **out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctxs && out && n > 0, "null argument or empty batch");
+    std::vector<zb::Ctx *> v((size_t)n);
+    for (int i = 0; i < n; i++)
+    {
+      ZB_REQUIRE(ctxs[i], "null context in batch");
+      v[(size_t)i] = ctxs[i]->impl;
+    }
+    std::unique_ptr<zb_batch> b(new zb_batch{zb::batch_create(v.data(), n)});
+    *out = b.release();
+  })
+}
+
+void zb_batch_destroy(zb_batch *batch)
+{
+  if (!batch) return;
+  try
+  {
+    zb::batch_destroy(batch->impl);
+  }
+  catch (...)
+  {
+  }
+  delete batch;
+}
+
+zb_status zb_batch_autotune(zb_batch *batch, int steps, zb_batch_config *chosen)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(batch, "null batch");
+    zb::batch_autotune(batch->impl, steps, chosen);
+  })
+}
+
+zb_status zb_batch_set_config(zb_batch *batch, const zb_batch_config *cfg)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(batch && cfg, "null argument");
+    zb::batch_config(batch->impl, cfg);
+  })
+}
+
+zb_status zb_batch_step(zb_batch *batch, int nsteps, int use_graph)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(batch, "null batch");
+    zb::batch_step(batch->impl, nsteps, use_graph);
+  })
+}
+
+zb_status zb_batch_stage(zb_batch *batch, unsigned stage)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(batch, "null batch");
+    zb::batch_stage(batch->impl, stage);
+  })
+}
+
+zb_status zb_batch_synchronize(zb_batch *batch)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(batch, "null batch");
+    zb::batch_sync(batch->impl);
+  })
+}
+
+int64_t zb_batch_launch_count(const zb_batch *batch) { return batch ? zb::batch_launches(batch->impl) : -1; }
+
 zb_status zb_set_freestream(zb_ctx *ctx, double rho_fs, const double *V_fs, double P_fs)
 {
   ZB_GUARD({
@@ -336,6 +408,14 @@ zb_status zb_vjp(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_strid
     ZB_REQUIRE(ctx && lam && Ubar, "null argument");
     ZB_REQUIRE(where == ZB_HOST || where == ZB_DEVICE, "where must be ZB_HOST or ZB_DEVICE");
     zb::ctx_vjp(ctx->impl, lam, Ubar, spt_stride, var_stride, ele_stride, where, param_bar);
+  })
+}
+
+zb_status zb_wall_force(zb_ctx *ctx, double *out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && out, "null argument");
+    zb::ctx_wall_force(ctx->impl, out);
   })
 }
 

@@ -2,6 +2,7 @@
 // dispatch over (dimension, order, precision) and explicit RK44 stepping.
 #include "ctx_impl.cuh"
 #include "hex_kernels.cuh"
+#include "tri_kernels.cuh"
 
 namespace zb {
 
@@ -206,6 +207,103 @@ __global__ void k_functionals(const T *__restrict__ U, const T *__restrict__ dU,
   }
 }
 
+// FP64 force and moment (about the origin) on wall boundaries of
+// FRSolver::compute_moments (src/solver.cpp:7600-7811): per wall flux point
+// w (P n - tau n) dA from the element's own trace and its extrapolated
+// corrected gradient.  The reference's 3D branch reads flux point 0's state
+// for the stress (src/solver.cpp:7716-7720); this uses each point's own.
+struct WallArgs
+{
+  double gamma, mu, rt, c_sth;
+  int fix_vis, viscous, D, S, Fp;
+  int64_t ntiles, neles;
+};
+
+template <typename T>
+__global__ void k_wall_force(const T *__restrict__ Ufp, const T *__restrict__ dU, const T *__restrict__ fgeo,
+                             const int *__restrict__ nbr, const double *__restrict__ dE, const double *__restrict__ fw,
+                             const double *__restrict__ cfp, const double *__restrict__ ref, const WallArgs w,
+                             double *out)
+{
+  const int D = w.D, V = D + 2, S = w.S, Fp = w.Fp;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const int64_t total = w.ntiles * Fp * TW;
+  for (int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gid < total; gid += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int l = (int)(gid % TW);
+    const int f = (int)((gid / TW) % Fp);
+    const int64_t t = gid / ((int64_t)TW * Fp);
+    const int64_t e = t * TW + l;
+    if (e >= w.neles) continue;
+    const int code = nbr[(t * Fp + f) * TW + l];
+    if (code >= 0) continue;
+    const int bc = -code - 1;
+    if (bc != 5 && bc != 6 && bc != 7 && bc != 8 && bc != 9) continue;
+    double u[5], n[3] = {0, 0, 0};
+    for (int v = 0; v < V; v++) u[v] = (double)Ufp[((t * Fp + f) * V + v) * TW + l] + (ref ? ref[v] : 0.0);
+    for (int d = 0; d < D; d++) n[d] = (double)fgeo[((t * Fp + f) * (D + 1) + d) * TW + l];
+    const double dA = (double)fgeo[((t * Fp + f) * (D + 1) + D) * TW + l];
+    const double rho = u[0];
+    double vel[3] = {0, 0, 0}, q2 = 0.0;
+    for (int d = 0; d < D; d++)
+    {
+      vel[d] = u[d + 1] / rho;
+      q2 += vel[d] * vel[d];
+    }
+    const double P = (w.gamma - 1.0) * (u[V - 1] - 0.5 * rho * q2);
+    const double wt = fw[f] * dA;
+    double F[3] = {0, 0, 0};
+    for (int d = 0; d < D; d++) F[d] = wt * P * n[d];
+    if (w.viscous)
+    {
+      double g[3][3];  // g[i][j] = d u_i / d x_j at the flux point
+      for (int j = 0; j < D; j++)
+      {
+        double dr = 0.0, dm[3] = {0, 0, 0};
+        for (int sp = 0; sp < S; sp++)
+        {
+          const double c = dE[(size_t)f * S + sp];
+          dr += c * (double)dU[(((t * D + j) * S + sp) * V + 0) * TW + l];
+          for (int i = 0; i < D; i++) dm[i] += c * (double)dU[(((t * D + j) * S + sp) * V + i + 1) * TW + l];
+        }
+        for (int i = 0; i < D; i++) g[i][j] = (dm[i] - dr * vel[i]) / rho;
+      }
+      double mu = w.mu;
+      if (!w.fix_vis)
+      {
+        const double e_int = u[V - 1] / rho - 0.5 * q2;
+        const double rr = (w.gamma - 1.0) * e_int / w.rt;
+        mu = w.mu * pow(rr, 1.5) * (1.0 + w.c_sth) / (rr + w.c_sth);
+      }
+      double diag = 0.0;
+      for (int d = 0; d < D; d++) diag += g[d][d];
+      diag /= 3.0;
+      for (int i = 0; i < D; i++)
+      {
+        double taun = 0.0;
+        for (int j = 0; j < D; j++)
+          taun += ((i == j) ? 2.0 * mu * (g[i][i] - diag) : mu * (g[i][j] + g[j][i])) * n[j];
+        F[i] -= wt * taun;
+      }
+    }
+    double x[3] = {0, 0, 0};
+    for (int d = 0; d < D; d++) x[d] = cfp[((size_t)f * D + d) * w.neles + e];
+    for (int d = 0; d < D; d++) acc[d] += F[d];
+    if (D == 3)
+    {
+      acc[3] += x[1] * F[2] - x[2] * F[1];
+      acc[4] += x[2] * F[0] - x[0] * F[2];
+    }
+    acc[5] += x[0] * F[1] - x[1] * F[0];
+  }
+  for (int k = 0; k < 6; k++)
+  {
+    double a = acc[k];
+    for (int o = 16; o > 0; o /= 2) a += __shfl_down_sync(0xffffffff, a, o);
+    if ((threadIdx.x & 31) == 0 && a != 0.0) atomicAdd(&out[k], a);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
@@ -233,36 +331,7 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, NT = G::NT;
-  Args<T, A> a;
-  std::memset(&a, 0, sizeof(a));
-  a.U = (const T *)c.U;
-  a.Ufp = (const T *)c.Ufp[c.cur];
-  a.Ufp_next = (T *)c.Ufp[c.cur ^ 1];
-  a.mets = (const T *)c.mets;
-  a.fgeo = (const T *)c.fgeo;
-  a.nbr = c.nbr;
-  a.divF = (T *)c.divF[sc.stage];
-  a.divF_vol = (A *)c.divF_vol;
-  a.Fvn = (T *)c.Fvn;
-  a.rk_mode = sc.rk_mode;
-  a.save_ini = sc.save_ini;
-  a.extrap_next = sc.extrap_next;
-  a.Uout = (T *)c.U;
-  a.U_ini = (T *)c.U_ini;
-  a.Ucomp = nullptr;
-  a.dt = (A)c.dt;
-  a.ntiles = c.ntiles;
-  a.dU_out = sc.want_dU ? (T *)c.dU : nullptr;
-  a.ph = phys_of<A>(c.plan.params, c.uref, c.D, sizeof(T) < sizeof(double));
-  if (sc.rk_mode == 1)
-    a.rk_coef[0] = (A)kRkAlpha[sc.stage];
-  else if (sc.rk_mode == 2)
-  {
-    a.nprev = (int)sc.stage;
-    for (unsigned s = 0; s <= sc.stage; s++) a.rk_coef[s] = (A)kRkBeta[s];
-    for (unsigned s = 0; s < sc.stage; s++) a.divF_prev[s] = (const T *)c.divF[s];
-    if (c.Ucomp) a.Ucomp = (T *)c.Ucomp;
-  }
+  const Args<T, A> a = make_args<T, A>(c, sc);
   const LineOpsT<A, N> ops = line_ops<A, N>(c.plan);
   const size_t ops_bytes = sizeof(LineOpsT<A, N>);
   if constexpr (D == 3)
@@ -330,6 +399,55 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
 }
 
 
+// Triangles: dense-operator kernels (tri_kernels.cuh)
+template <typename T, typename A, int N>
+static void launch_extrap_tri(Ctx &c)
+{
+  using G = dev::TriShape<N>;
+  ProfScope ps(c, ZB_K_EXTRAP);
+  dev::k_tri_extrap<T, A, N><<<grid_for(c.ntiles * G::Fp * TW, 128), 128, 0, c.stream>>>(
+      (const T *)c.U, (T *)c.Ufp[c.cur], c.ntiles, (const A *)c.dops);
+  c.launches++;
+  CK(cudaGetLastError());
+}
+
+template <typename T, typename A, int N>
+static void launch_stage_tri(Ctx &c, const StageCfg &sc)
+{
+  using G = dev::TriShape<N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V, D = 2;
+  const Args<T, A> a = make_args<T, A>(c, sc);
+  const size_t ops = (size_t)((G::NOPS + 1) / 2) * 2;
+  if (!c.plan.params.viscous)
+  {
+    const size_t smem = (ops + (size_t)(S * V + D * S * V + Fp * V) * TW) * sizeof(A);
+    set_smem(dev::k_tri_euler<T, A, N>, smem);
+    ProfScope ps(c, ZB_K_EULER);
+    dev::k_tri_euler<T, A, N><<<(unsigned)c.ntiles, 128, smem, c.stream>>>(a);
+    c.launches++;
+    CK(cudaGetLastError());
+  }
+  else
+  {
+    const size_t smem1 = (ops + (size_t)(S * V + Fp * V + D * S * V) * TW) * sizeof(A);
+    set_smem(dev::k_tri_ns_grad<T, A, N>, smem1);
+    {
+      ProfScope ps(c, ZB_K_NS_GRAD);
+      dev::k_tri_ns_grad<T, A, N><<<(unsigned)c.ntiles, 128, smem1, c.stream>>>(a);
+      c.launches++;
+      CK(cudaGetLastError());
+    }
+    if (sc.grad_only) return;
+    const size_t smem2 = (ops + (size_t)(Fp * V + S * V) * TW) * sizeof(A);
+    set_smem(dev::k_tri_ns_face<T, A, N>, smem2);
+    ProfScope ps(c, ZB_K_NS_FACE);
+    dev::k_tri_ns_face<T, A, N><<<(unsigned)c.ntiles, 128, smem2, c.stream>>>(a);
+    c.launches++;
+    CK(cudaGetLastError());
+  }
+  if (sc.extrap_next) c.cur ^= 1;
+}
+
 template <typename T, typename A, int D, int N>
 static void bind(Ctx &c)
 {
@@ -341,6 +459,19 @@ template <typename T, typename A>
 static void bind_t(Ctx &c)
 {
   const int D = c.D, N = c.N;
+  if (c.plan.etype == ET_TRI)
+  {
+#define ZB_BIND_TRI(NN)                                   \
+  if (N == NN)                                            \
+  {                                                       \
+    c.launch_extrap = &launch_extrap_tri<T, A, NN>;       \
+    c.launch_stage = &launch_stage_tri<T, A, NN>;         \
+    return;                                               \
+  }
+    ZB_BIND_TRI(2) ZB_BIND_TRI(3) ZB_BIND_TRI(4) ZB_BIND_TRI(5)
+#undef ZB_BIND_TRI
+    ZB_THROW(ZB_ERR_UNSUPPORTED, "no triangle kernels for P=" + std::to_string(N - 1));
+  }
 #define ZB_BIND(DD, NN) \
   if (D == DD && N == NN) { bind<T, A, DD, NN>(c); return; }
   ZB_BIND(2, 2) ZB_BIND(2, 3) ZB_BIND(2, 4) ZB_BIND(2, 5) ZB_BIND(2, 6)
@@ -369,7 +500,7 @@ static void free_all(Ctx *c)
 {
   void *bufs[] = {c->U, c->U_ini, c->divF[0], c->divF[1], c->divF[2], c->divF[3], c->divF_vol, c->Ufp[0],
                   c->Ufp[1], c->Fvn, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
-                  c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubar, c->pbar};
+                  c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubar, c->pbar, c->dops, c->dwall};
   for (void *b : bufs)
     if (b) cudaFree(b);
   for (auto &r : c->recs)
@@ -488,6 +619,22 @@ Ctx *ctx_create(const Plan &plan)
       upload_static<double>(*c);
     else
       upload_static<float>(*c);
+    if (plan.etype == ET_TRI)
+    {
+      // oppE, oppD, oppD_fpts, oppDiv, oppDiv_fpts back to back (TriShape)
+      std::vector<double> ops;
+      for (const auto *v : {&plan.tri_oppE, &plan.tri_oppD, &plan.tri_oppD_fpts, &plan.tri_oppDiv,
+                            &plan.tri_oppDiv_fpts})
+        ops.insert(ops.end(), v->begin(), v->end());
+      c->dops = dalloc(ops.size() * c->asz);
+      if (c->asz == sizeof(double))
+        CK(cudaMemcpy(c->dops, ops.data(), ops.size() * sizeof(double), cudaMemcpyHostToDevice));
+      else
+      {
+        std::vector<float> f(ops.begin(), ops.end());
+        CK(cudaMemcpy(c->dops, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+      }
+    }
     // zero the state so a residual before set_state is well defined (all zeros)
     CK(cudaMemsetAsync(c->U, 0, nU * c->tsz, c->stream));
     if (c->Ucomp) CK(cudaMemsetAsync(c->Ucomp, 0, nU * c->tsz, c->stream));
@@ -741,7 +888,7 @@ void ctx_functionals(Ctx *c, double *out)
   if (!c->dweights)
   {
     c->dweights = (double *)dalloc(c->S * sizeof(double));
-    c->dfun = (double *)dalloc(4 * sizeof(double));
+    if (!c->dfun) c->dfun = (double *)dalloc(8 * sizeof(double));
     CK(cudaMemcpyAsync(c->dweights, c->plan.weights_spts.data(), c->S * sizeof(double), cudaMemcpyHostToDevice,
                        c->stream));
   }
@@ -825,6 +972,81 @@ void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, in
     for (int64_t t = 0; t < c->ntiles; t++)
       for (int k = 0; k < 5; k++) param_bar[k] += h[(size_t)t * 5 + k];
   }
+}
+
+void ctx_wall_force(Ctx *c, double *out)
+{
+  const Plan &p = c->plan;
+  const int S = c->S, Fp = c->Fp, D = c->D;
+  if (!c->dwall)
+  {
+    // dense extrapolation (FP64), face quadrature weights, flux point coordinates
+    std::vector<double> oppE, oD, oDf, oDv, oDvf;
+    p.dense_operators(oppE, oD, oDf, oDv, oDvf);
+    std::vector<double> fw((size_t)Fp);
+    const std::vector<double> w1 = gauss_legendre_weights(c->N);
+    for (int f = 0; f < Fp; f++)
+    {
+      if (p.etype == ET_HEX)
+      {
+        const int r = f % (c->N * c->N);
+        fw[f] = w1[r / c->N] * w1[r % c->N];
+      }
+      else
+        fw[f] = w1[f % c->N];
+    }
+    const size_t nE = oppE.size(), nC = p.coord_fpts.size();
+    c->dwall = (double *)dalloc((nE + Fp + nC + 8) * sizeof(double));
+    CK(cudaMemcpy(c->dwall, oppE.data(), nE * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->dwall + nE, fw.data(), Fp * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->dwall + nE + Fp, p.coord_fpts.data(), nC * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (!c->dfun) c->dfun = (double *)dalloc(8 * sizeof(double));
+  const bool visc = p.params.viscous != 0;
+  const size_t nU = (size_t)c->ntiles * S * c->V * TW;
+  if (visc)
+  {
+    if (!c->dU) c->dU = dalloc(nU * D * c->tsz);
+    c->ufp_valid = false;
+    ensure_ufp(c);
+    StageCfg sc{0, 0, 0, 0};
+    sc.want_dU = 1;
+    sc.grad_only = 1;
+    c->launch_stage(*c, sc);
+  }
+  else
+    ensure_ufp(c);
+  CK(cudaMemsetAsync(c->dfun, 0, 8 * sizeof(double), c->stream));
+  WallArgs w;
+  w.gamma = p.params.gamma;
+  w.mu = p.params.mu;
+  w.rt = p.params.rt;
+  w.c_sth = p.params.c_sth;
+  w.fix_vis = p.params.fix_vis;
+  w.viscous = visc ? 1 : 0;
+  w.D = D;
+  w.S = S;
+  w.Fp = Fp;
+  w.ntiles = c->ntiles;
+  w.neles = p.neles;
+  const double *dE = c->dwall, *fw = c->dwall + (size_t)Fp * S, *cfp = fw + Fp;
+  const double *ref = c->prec == ZB_FP64 ? nullptr : c->dref;
+  const int blocks = grid_for(c->ntiles * Fp * TW, 256);
+  {
+    ProfScope ps(*c, ZB_K_FUNCTIONALS);
+    if (c->prec == ZB_FP64)
+      k_wall_force<double><<<blocks, 256, 0, c->stream>>>((const double *)c->Ufp[c->cur], (const double *)c->dU,
+                                                          (const double *)c->fgeo, c->nbr, dE, fw, cfp, ref, w, c->dfun);
+    else
+      k_wall_force<float><<<blocks, 256, 0, c->stream>>>((const float *)c->Ufp[c->cur], (const float *)c->dU,
+                                                         (const float *)c->fgeo, c->nbr, dE, fw, cfp, ref, w, c->dfun);
+    c->launches++;
+    CK(cudaGetLastError());
+  }
+  double h[8];
+  CK(cudaMemcpyAsync(h, c->dfun, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 6; k++) out[k] = h[k];
 }
 
 void ctx_profile_enable(Ctx *c, int on)

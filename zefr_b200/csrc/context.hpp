@@ -33,14 +33,30 @@ void ctx_sync(Ctx *c);
 int64_t ctx_launches(const Ctx *c);
 void ctx_profile_enable(Ctx *c, int on);
 void ctx_functionals(Ctx *c, double *out);
+void ctx_wall_force(Ctx *c, double *out);
 void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, int64_t es, int where,
              double *param_bar);
 void ctx_profile_read(Ctx *c, double *ms, int64_t *count);
 void noalloc_residual(const Plan &p, const double *U, double *divF, cudaStream_t st);
+
+struct Batch;
+Batch *batch_create(Ctx *const *ctxs, int n);
+void batch_destroy(Batch *b);
+void batch_autotune(Batch *b, int steps, zb_batch_config *out);
+void batch_config(Batch *b, const zb_batch_config *cfg);
+void batch_step(Batch *b, int nsteps, int use_graph);
+void batch_stage(Batch *b, unsigned stage);
+void batch_sync(Batch *b);
+int64_t batch_launches(const Batch *b);
 
 }  // namespace zb
 
 struct zb_ctx
 {
   zb::Ctx *impl;
+};
+
+struct zb_batch
+{
+  zb::Batch *impl;
 };

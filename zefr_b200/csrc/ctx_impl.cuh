@@ -51,6 +51,8 @@ struct Ctx
   void *U = nullptr, *U_ini = nullptr, *divF[4] = {nullptr, nullptr, nullptr, nullptr};
   void *divF_vol = nullptr, *Ufp[2] = {nullptr, nullptr}, *Fvn = nullptr, *mets = nullptr, *fgeo = nullptr;
   void *Ucomp = nullptr;
+  void *dops = nullptr;  // triangles: dense operators in the arithmetic type
+  double *dwall = nullptr;  // wall force: FP64 oppE, face weights, flux point coordinates
   int *nbr = nullptr;
   double *dtmp = nullptr;
   size_t dtmp_bytes = 0;
@@ -187,6 +189,44 @@ template <typename K>
 static void set_smem(K kernel, size_t bytes)
 {
   CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// kernel arguments of one stage of a context
+template <typename T, typename A>
+static Args<T, A> make_args(Ctx &c, const StageCfg &sc)
+{
+  Args<T, A> a;
+  std::memset(&a, 0, sizeof(a));
+  a.U = (const T *)c.U;
+  a.Ufp = (const T *)c.Ufp[c.cur];
+  a.Ufp_next = (T *)c.Ufp[c.cur ^ 1];
+  a.mets = (const T *)c.mets;
+  a.fgeo = (const T *)c.fgeo;
+  a.nbr = c.nbr;
+  a.divF = (T *)c.divF[sc.stage];
+  a.divF_vol = (A *)c.divF_vol;
+  a.Fvn = (T *)c.Fvn;
+  a.rk_mode = sc.rk_mode;
+  a.save_ini = sc.save_ini;
+  a.extrap_next = sc.extrap_next;
+  a.Uout = (T *)c.U;
+  a.U_ini = (T *)c.U_ini;
+  a.Ucomp = nullptr;
+  a.dt = (A)c.dt;
+  a.ntiles = c.ntiles;
+  a.dU_out = sc.want_dU ? (T *)c.dU : nullptr;
+  a.dops = (const A *)c.dops;
+  a.ph = phys_of<A>(c.plan.params, c.uref, c.D, sizeof(T) < sizeof(double));
+  if (sc.rk_mode == 1)
+    a.rk_coef[0] = (A)kRkAlpha[sc.stage];
+  else if (sc.rk_mode == 2)
+  {
+    a.nprev = (int)sc.stage;
+    for (unsigned s = 0; s <= sc.stage; s++) a.rk_coef[s] = (A)kRkBeta[s];
+    for (unsigned s = 0; s < sc.stage; s++) a.divF_prev[s] = (const T *)c.divF[s];
+    if (c.Ucomp) a.Ucomp = (T *)c.Ucomp;
+  }
+  return a;
 }
 
 // selects the adjoint kernels of the context (plain FP64 form; adjoint.cu)

@@ -70,6 +70,7 @@ struct Args
   A rk_coef[6];      // a_s (mode 1: [0]) or b_s (mode 2)
   A dt;
   int64_t ntiles;
+  const A *dops;     // triangles: dense operators (TriOps layout), nullptr otherwise
   Phys<A> ph;
 };
 
@@ -256,39 +257,16 @@ __device__ __forceinline__ void conv_common(const Args<T, A> &a, const A Uo[D + 
 }
 
 // ---------------------------------------------------------------------------
-// Final per-point residual: volume part + surface correction, then optional
-// RK update (src/solver.cpp:2916-2937, 3040-3094).
+// Store the residual of one point and apply the optional RK update
+// (src/solver.cpp:2916-2937, 3040-3094).
 // ---------------------------------------------------------------------------
-template <typename T, typename A, int D, int N>
-__device__ __forceinline__ void finish_point(const Args<T, A> &a, int64_t tile, int s, int l, const A vol[D + 2],
-                                             const A *sFc, const SOps<A, N> &o, A *sUnew)
+template <typename T, typename A, int S, int V, int NM>
+__device__ __forceinline__ void store_rk(const Args<T, A> &a, int64_t tile, int s, int l, const A res[V], A *sUnew)
 {
-  using G = Shape<D, N>;
-  constexpr int S = G::S, V = G::V, NM = G::NM;
-  A surf[V];
-#pragma unroll
-  for (int v = 0; v < V; v++) surf[v] = A(0);
-  // surface terms in ascending flux point order = ascending face order
-#pragma unroll
-  for (int face = 0; face < 2 * D; face++)
-  {
-    int dim, side;
-    face_dim_side<D>(face, dim, side);
-    int i, fm, fp;
-    spt_ends<D, N>(s, dim, i, fm, fp);
-    const int f = side < 0 ? fm : fp;
-    const A c = side < 0 ? -o.Dbm[i] : o.Dbp[i];
-#pragma unroll
-    for (int v = 0; v < V; v++) surf[v] += c * sFc[(f * V + v) * TW + l];
-  }
+  constexpr int D = NM == 5 ? 2 : 3;
   const int64_t base = (tile * S + s) * (int64_t)V * TW;
-  A res[V];
 #pragma unroll
-  for (int v = 0; v < V; v++)
-  {
-    res[v] = vol[v] + surf[v];
-    a.divF[base + v * TW + l] = res[v];
-  }
+  for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
   if (a.rk_mode == 0) return;
   const A detJ = a.mets[((tile * S + s) * NM + D * D) * TW + l];
 #pragma unroll
@@ -333,6 +311,38 @@ __device__ __forceinline__ void finish_point(const Args<T, A> &a, int64_t tile, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Final per-point residual: volume part + surface correction, then optional
+// RK update (src/solver.cpp:2916-2937, 3040-3094).
+// ---------------------------------------------------------------------------
+template <typename T, typename A, int D, int N>
+__device__ __forceinline__ void finish_point(const Args<T, A> &a, int64_t tile, int s, int l, const A vol[D + 2],
+                                             const A *sFc, const SOps<A, N> &o, A *sUnew)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, V = G::V, NM = G::NM;
+  A surf[V];
+#pragma unroll
+  for (int v = 0; v < V; v++) surf[v] = A(0);
+  // surface terms in ascending flux point order = ascending face order
+#pragma unroll
+  for (int face = 0; face < 2 * D; face++)
+  {
+    int dim, side;
+    face_dim_side<D>(face, dim, side);
+    int i, fm, fp;
+    spt_ends<D, N>(s, dim, i, fm, fp);
+    const int f = side < 0 ? fm : fp;
+    const A c = side < 0 ? -o.Dbm[i] : o.Dbp[i];
+#pragma unroll
+    for (int v = 0; v < V; v++) surf[v] += c * sFc[(f * V + v) * TW + l];
+  }
+  A res[V];
+#pragma unroll
+  for (int v = 0; v < V; v++) res[v] = vol[v] + surf[v];
+  store_rk<T, A, S, V, NM>(a, tile, s, l, res, sUnew);
+}
+
 template <typename T, typename A, int D, int N>
 __device__ __forceinline__ void extrap_next_tile(const Args<T, A> &a, int64_t tile, const A *sUnew, const SOps<A, N> &o)
 {
@@ -351,19 +361,16 @@ __device__ __forceinline__ void extrap_next_tile(const Args<T, A> &a, int64_t ti
 // Euler: volume flux, common flux and divergence of one tile in one kernel.
 // ---------------------------------------------------------------------------
 template <typename T, typename A, int D, int N>
-__global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(const __grid_constant__ Args<T, A> a,
-                                                                   const __grid_constant__ LineOpsT<A, N> ops)
+__device__ __forceinline__ void euler_tile(const Args<T, A> &a, const LineOpsT<A, N> &ops, int64_t tile,
+                                           unsigned char *smem_raw)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, NM = G::NM;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sU = reinterpret_cast<A *>(smem_raw);
   A *sF = sU + S * V * TW;
   A *sFc = sF + D * S * V * TW;
   A *sops = sFc + Fp * V * TW;
   load_ops<A, N>(sops, ops);
-  const int64_t tile = blockIdx.x;
-  if (tile >= a.ntiles) return;
   {
     const T *src = a.U + tile * (int64_t)S * V * TW;
     for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
@@ -445,6 +452,24 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(const __grid_constant
     __syncthreads();
     extrap_next_tile<T, A, D, N>(a, tile, sU, o);
   }
+}
+
+
+// Shared memory of euler_tile (elements of the arithmetic type)
+template <int D, int N>
+constexpr int euler_smem_elems()
+{
+  return (Shape<D, N>::S * Shape<D, N>::V * (1 + D) + Shape<D, N>::Fp * Shape<D, N>::V) * TW + N * N + 4 * N;
+}
+
+template <typename T, typename A, int D, int N>
+__global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(const __grid_constant__ Args<T, A> a,
+                                                                   const __grid_constant__ LineOpsT<A, N> ops)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int64_t tile = blockIdx.x;
+  if (tile >= a.ntiles) return;
+  euler_tile<T, A, D, N>(a, ops, tile, smem_raw);
 }
 
 // ---------------------------------------------------------------------------

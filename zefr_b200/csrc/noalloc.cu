@@ -258,6 +258,7 @@ void run_kernels(const Plan &p, unsigned char *base, const Regions &r, cudaStrea
 void dispatch(const Plan &p, unsigned char *base, const Regions &r, cudaStream_t st)
 {
   const int D = p.ndims, N = p.N;
+  if (p.etype == ET_TRI) ZB_THROW(ZB_ERR_UNSUPPORTED, "the allocation-free residual is built for quads and hexes");
 #define NA_CASE(DD, NN) \
   if (D == DD && N == NN) return run_kernels<DD, NN>(p, base, r, st);
   NA_CASE(2, 2) NA_CASE(2, 3) NA_CASE(2, 4) NA_CASE(2, 5) NA_CASE(2, 6)

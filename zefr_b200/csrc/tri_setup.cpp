@@ -98,28 +98,34 @@ static void ws_points(int P, std::vector<double> &loc, std::vector<double> &w)
 // ---------------------------------------------------------------------------
 static double jacobi_n(double x, double al, double be, int n)
 {
-  // three-term recurrence of the orthonormal Jacobi polynomials (H&W
-  // Appendix A, JacobiP)
-  const double g0 = std::pow(2.0, al + be + 1) / (al + be + 1) * std::tgamma(al + 1) * std::tgamma(be + 1) /
-                    std::tgamma(al + be + 1);
-  double p0 = 1.0 / std::sqrt(g0);
-  if (n == 0) return p0;
-  const double g1 = (al + 1) * (be + 1) / (al + be + 3) * g0;
-  double p1 = ((al + be + 2) * x / 2 + (al - be) / 2) / std::sqrt(g1);
-  if (n == 1) return p1;
-  double aold = 2.0 / (2 + al + be) * std::sqrt((al + 1) * (be + 1) / (al + be + 3));
-  for (int i = 1; i < n; i++)
+  // orthonormal Jacobi polynomials by their three-term recurrence, evaluated
+  // upward with the same expressions per degree as the reference's recursive
+  // HiFiLES form (src/polynomials.cpp:28-83), so the values agree bitwise
+  const double c0 = std::pow(2.0, (-al - be - 1)) *
+                    (std::tgamma(al + be + 2) / (std::tgamma(al + 1) * std::tgamma(be + 1)));
+  double pm2 = std::sqrt(c0);
+  if (n == 0) return pm2;
+  double pm1 = 0.5 * std::sqrt(c0) * std::sqrt((al + be + 3) / ((al + 1) * (be + 1))) * (x * (al + be + 2) + (al - be));
+  if (n == 1) return pm1;
+  double p = pm1;
+  for (int m = 2; m <= n; m++)
   {
-    const double h1 = 2 * i + al + be;
-    const double anew = 2.0 / (h1 + 2) *
-                        std::sqrt((i + 1) * (i + 1 + al + be) * (i + 1 + al) * (i + 1 + be) / (h1 + 1) / (h1 + 3));
-    const double bnew = -(al * al - be * be) / h1 / (h1 + 2);
-    const double p2 = (-aold * p0 + (x - bnew) * p1) / anew;
-    p0 = p1;
-    p1 = p2;
-    aold = anew;
+    const double d0 = m * (m + al + be) * (m + al) * (m + be);
+    const double d1 = ((2 * m) + al + be - 1) * ((2 * m) + al + be + 1);
+    const double d3 = (2 * m) + al + be;
+    const double d4 = (m - 1) * ((m - 1) + al + be) * ((m - 1) + al) * ((m - 1) + be);
+    const double d5 = ((2 * (m - 1)) + al + be - 1) * ((2 * (m - 1)) + al + be + 1);
+    const double d6 = (2 * (m - 1)) + al + be;
+    const double d7 = -((al * al) - (be * be));
+    const double d8 = ((2 * (m - 1)) + al + be) * ((2 * (m - 1)) + al + be + 2);
+    const double d9 = (2.0 / d3) * std::sqrt(d0 / d1);
+    const double d10 = (2.0 / d6) * std::sqrt(d4 / d5);
+    const double d11 = d7 / d8;
+    p = (1.0 / d9) * (x * pm1 - d10 * pm2 - d11 * pm1);
+    pm2 = pm1;
+    pm1 = p;
   }
-  return p1;
+  return p;
 }
 
 static double djacobi_n(double x, double al, double be, int n)
@@ -168,14 +174,11 @@ double dubiner_d(int mode, double xi, double eta, int dim)
   const double gb = jacobi_n(b, 2 * i + 1, 0, j), dgb = djacobi_n(b, 2 * i + 1, 0, j);
   const double s2 = std::sqrt(2.0);
   if (dim == 0) return (i == 0) ? 0.0 : 2.0 * s2 * dfa * gb * std::pow(1.0 - b, i - 1);
-  // eta derivative
-  double v = s2 * fa * dgb * std::pow(1.0 - b, i);
-  if (i > 0)
-  {
-    v += s2 * dfa * gb * std::pow(1.0 - b, i - 1) * (1.0 + a);
-    v -= s2 * fa * gb * i * std::pow(1.0 - b, i - 1);
-  }
-  return v;
+  // eta derivative, grouped as the reference's dDubiner2D groups it
+  const double j3 = dgb * std::pow(1.0 - b, i);
+  if (i == 0) return s2 * fa * j3;
+  const double j4 = gb * i * std::pow(1.0 - b, i - 1);
+  return s2 * (dfa * gb * std::pow(1.0 - b, i - 1) * (1.0 + a) + fa * (j3 - j4));
 }
 
 // Gauss-Jordan inverse with partial pivoting of an n x n row-major matrix.

@@ -290,6 +290,13 @@ class FRSolver:
                                _lib.ZB_HOST, pptr))
         return (out, pbar) if params else out
 
+    def wall_force(self) -> Dict[str, np.ndarray]:
+        """FP64 force and moment (about the origin) on the wall boundaries
+        (compute_moments) of the current state."""
+        out = np.zeros(6)
+        check(lib().zb_wall_force(self.h, out.ctypes.data_as(_DP)))
+        return {"force": out[:3].copy(), "moment": out[3:].copy()}
+
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().zb_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
 
