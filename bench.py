@@ -234,6 +234,130 @@ def time_e2e(s, U, K: int, W: int, world: int):
     return max_over_ranks(ms, world), Un.nbytes, Rn.nbytes
 
 
+def triangle_side(K: int, W: int):
+    """Triangle workload: 128 x 128 quads on periodic [0,1]^2 split along seeded
+    diagonals (32,768 triangles), interior nodes jittered 15% of h, P4
+    (15 Williams-Shunn points), Roe + LDG (beta 0.5, tau 0.1), Ma 0.2, Re 1000,
+    Pr 0.71, double shear layer with seeded 1e-3 velocity noise.  GDOF/s per
+    residual of both forms and the mixed form's relative L2 error."""
+    import torch
+    from zefr_b200 import ics, meshgen
+    from zefr_b200.solver import FRSolver, params_from_deck
+    mesh = meshgen.box_tris(128, seed=2024, jitter=0.15)
+    out = {"workload": "triangles_128x128x2_P4_navier_stokes_roe_ldg", "elements": int(mesh.n_elements)}
+    R = {}
+    for form in ("mixed", "fp64"):
+        p = params_from_deck(ndims=2, order=4, viscous=1, disable_nondim=1, fix_vis=1, mach_fs=0.2, Re_fs=1000.0,
+                             prandtl=0.71, P_fs=1.0, rho_fs=1.0, L_fs=1.0, ldg_b=0.5, ldg_tau=0.1, fconv=2,
+                             precision={"mixed": 1, "fp64": 0}[form], gamma=1.4, dt=1e-4)
+        s = FRSolver(mesh, p, {"PERIODIC": "periodic"})
+        s.set_stream(torch.cuda.current_stream().cuda_stream)
+        X = s.plan.get("coord_spts").reshape(s.nspts, 2, s.neles)
+        s.set_state(ics.double_shear_layer(X, mach=0.2, noise=1e-3, seed=7))
+        for i in range(W):
+            s.compute_residual(i % 4)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for i in range(K):
+            s.compute_residual(i % 4)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / K
+        dof = s.nspts * s.nvars * s.neles
+        s.compute_residual(0)
+        R[form] = s.get_residual(0)
+        out[form] = {"gdof_s": dof / (ms * 1e-3) / 1e9, "ms_per_residual": ms, "dof": dof}
+        s.close()
+    out["mixed_rel_l2_err_vs_fp64"] = float(np.linalg.norm(R["mixed"] - R["fp64"]) / np.linalg.norm(R["fp64"]))
+    out["mixed_over_fp64"] = out["fp64"]["ms_per_residual"] / out["mixed"]["ms_per_residual"]
+    return out
+
+
+def batched_side(steps: int = 5, ncases: int = 512, seed: int = 4):
+    """Batched vortex workload: 512 independent periodic quad meshes n x n on
+    [-5,5]^2 (n uniform in [8,96]), P uniform in 1..5, isentropic vortex of
+    strength uniform in [1,5] at a centre uniform in [-2,2]^2 on a stream of
+    Mach uniform in [0.2,0.8], all from one seed; mixed form.  Throughput of
+    the autotuned persistent stages under a CUDA graph against the same cases
+    stepped one launch per case and stage."""
+    from zefr_b200 import batch as zbatch
+    t0 = time.perf_counter()
+    cases = zbatch.vortex_cases(ncases, seed, precision="mixed")
+    setup_s = time.perf_counter() - t0
+    dof = sum(c.nspts * c.nvars * c.neles for c in cases)
+    bt = zbatch.Batch(cases)
+    cfg = bt.autotune(steps=2)
+    bt.step(2)
+    bt.synchronize()
+    t0 = time.perf_counter()
+    bt.step(steps)
+    bt.synchronize()
+    ms_batch = (time.perf_counter() - t0) * 1e3 / steps
+    # one launch per case and stage, every case on its own context stream
+    for c in cases:
+        c.step(1)
+    for c in cases:
+        c.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for c in cases:
+            c.step(1)
+    for c in cases:
+        c.synchronize()
+    ms_single = (time.perf_counter() - t0) * 1e3 / steps
+    res_per_step = 4  # RK44 stages, one residual each
+    out = {"workload": "batched_vortex_512_quads_n8-96_P1-5_euler", "cases": ncases, "dof": dof,
+           "setup_s": setup_s, "autotuned": cfg,
+           "batched": {"gdof_s": dof * res_per_step / (ms_batch * 1e-3) / 1e9, "ms_per_step": ms_batch,
+                       "launches_per_step": 4},
+           "one_launch_per_case": {"gdof_s": dof * res_per_step / (ms_single * 1e-3) / 1e9,
+                                   "ms_per_step": ms_single, "launches_per_step": 4 * ncases},
+           "timing": "host clock around synchronised steps (both paths), 4 residuals per RK44 step"}
+    out["batched_over_single"] = ms_single / ms_batch
+    bt.close()
+    for c in cases:
+        c.close()
+    return out
+
+
+def cylinder_adjoint_side(nsteps: int = 500, every: int = 50):
+    """Cylinder adjoint workload: curved O-mesh of 48 x 96 nine-node quads
+    (r 0.5 to 20, stretch 1.1), P3, Ma 0.2, Re 100, characteristic far field,
+    adiabatic no-slip wall; objective = drag averaged over 500 RK44 steps;
+    gradient with respect to 16 wall Fourier coefficients and the free-stream
+    angle through the hand-written adjoint, checkpoints every 50 steps, FP64.
+    Checked against central differences (step 1e-6) of the forward run for one
+    coefficient and the angle."""
+    from zefr_b200.shape import CylinderDrag
+    prob = CylinderDrag(nr=48, nt=96, order=3, dt=1e-4, checkpoint_every=every)
+    coef = np.zeros(16)
+    coef[:4] = (0.01, -0.005, 0.003, 0.002)
+    alpha = 0.05
+    t0 = time.perf_counter()
+    J = prob.drag(coef, alpha, nsteps)
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    g = prob.gradient(coef, alpha, nsteps)
+    t_adj = time.perf_counter() - t0
+    h = 1e-6
+    cp, cm = coef.copy(), coef.copy()
+    cp[0] += h
+    cm[0] -= h
+    fd0 = (prob.drag(cp, alpha, nsteps) - prob.drag(cm, alpha, nsteps)) / (2 * h)
+    fda = (prob.drag(coef, alpha + h, nsteps) - prob.drag(coef, alpha - h, nsteps)) / (2 * h)
+    return {"workload": "cylinder_omesh_48x96_quad9_P3_ns_drag_adjoint", "steps": nsteps,
+            "checkpoint_every": every, "J_mean_drag": J,
+            "dJ_dcoef": [float(x) for x in g["dJ_dcoef"]], "dJ_dalpha": g["dJ_dalpha"],
+            "fd_check": {"coef0": {"adjoint": float(g["dJ_dcoef"][0]), "central_difference": fd0,
+                                   "rel_err": abs(g["dJ_dcoef"][0] - fd0) / abs(fd0)},
+                         "alpha": {"adjoint": g["dJ_dalpha"], "central_difference": fda,
+                                   "rel_err": abs(g["dJ_dalpha"] - fda) / abs(fda)}},
+            "forward_s": t_fwd, "gradient_s": t_adj,
+            "timing": "host clock; the gradient run includes the forward pass, checkpoint "
+                      "recomputation and host copies of the geometry adjoint"}
+
+
 def cpu_baseline_sample(n: int = 16, min_seconds: float = 10.0, max_calls: int = 40):
     """Reference CPU residual (compiled reference, release flags, OpenMP on all
     host cores) on a bounded sample: the same TGV workload at n^3 hexes."""
@@ -402,6 +526,14 @@ def gpu_arm(args):
     }
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline_sample()
+    if world == 1 and not args.no_side:
+        import torch
+        torch.cuda.empty_cache()
+        line["triangles"] = triangle_side(K, W)
+        torch.cuda.empty_cache()
+        line["batched"] = batched_side()
+        torch.cuda.empty_cache()
+        line["cylinder_adjoint"] = cylinder_adjoint_side()
     return line
 
 
@@ -469,6 +601,7 @@ def main():
     ap.add_argument("--cells", type=int, default=NCELL, help=argparse.SUPPRESS)
     ap.add_argument("--ref-cells", type=int, default=20, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--no-side", action="store_true", help="skip the triangle and batched side workloads")
     ap.add_argument("--profile-form", choices=["mixed", "fp64"], default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -177,7 +177,10 @@ zb_status zb_plan_info(const zb_plan *plan, zb_info *out);
  * inv_jaco_spts, oppE, oppD, oppD_fpts, oppDiv, oppDiv_fpts, fpt_partner
  * (partner element*nfpts+fpt per element fpt, -1-bc on boundaries),
  * fpt_slot, fpt_norm (left-element normal per element fpt [fpt][dim][ele]),
- * fpt_dA.  With out == NULL, *n receives the element count. */
+ * fpt_dA, coord_fpts, weights_spts, loc_spts, loc_fpts, tnorm ([fpt][dim]
+ * reference normals), dshape_spts [dim][spt][node], dshape_fpts
+ * [dim][fpt][node], shape_fpts [fpt][node] (shape functions, gmsh node order;
+ * for geometry derivatives).  With out == NULL, *n receives the element count. */
 zb_status zb_plan_get(const zb_plan *plan, const char *name, double *out, int64_t *n);
 
 /* Create a device context from a plan on the current device. */
@@ -239,6 +242,19 @@ zb_status zb_wall_force(zb_ctx *ctx, double *out);
  * counterpart (the reference fixes them at set-up). */
 zb_status zb_set_freestream(zb_ctx *ctx, double rho_fs, const double *V_fs, double P_fs);
 
+/* zb_vjp plus the adjoint with respect to the geometry the residual is built
+ * on, in the layouts zb_plan_get exports (host arrays, FP64):
+ * inv_jaco_bar [D][S][D][E] and jaco_det_bar [S][E] (adjugate and |J| at
+ * solution points), norm_bar [Fp][D][E] and dA_bar [Fp][E] (face unit normal
+ * and own face area factor at flux points).  A face's normal is the left
+ * element's (the right element stores a copy), so its whole adjoint is
+ * reported at the left element's flux point and zero at the right one's.
+ * For Navier-Stokes the call first evaluates the residual of the current
+ * state into register 0.  No reference counterpart. */
+zb_status zb_vjp_geometry(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride, int64_t var_stride,
+                          int64_t ele_stride, int where, double *param_bar, double *inv_jaco_bar,
+                          double *jaco_det_bar, double *norm_bar, double *dA_bar);
+
 /* ---- Batched stepping of independent cases ----
  * Many Euler cases on quadrilaterals (each its own context: mesh, order
  * P1-P5, state, dt) advance together: one persistent launch per RK stage
@@ -248,10 +264,12 @@ zb_status zb_set_freestream(zb_ctx *ctx, double rho_fs, const double *V_fs, doub
  * first).  No reference counterpart (the reference steps one mesh). */
 typedef struct zb_batch zb_batch;
 typedef struct zb_batch_config {
-  int threads;        /* threads per CTA: 128 or 256 */
+  int threads;        /* threads per CTA: 64, 128 or 256 */
   int blocks_per_sm;  /* persistent CTAs per SM */
   int order;          /* work order: 0 by polynomial order (costliest first), 1 case-major */
   double ms_per_step; /* autotuner: measured time of one RK44 step */
+  int group;          /* threads per tile group (64, 128 or 256, dividing threads): a CTA
+                         runs threads/group tiles at once */
 } zb_batch_config;
 
 zb_status zb_batch_create(zb_ctx *const *ctxs, int n, zb_batch **out);

@@ -37,6 +37,21 @@ def test_batch_matches_cases_stepped_alone(precision, graph):
         assert _same(s1.get_state(), s2.get_state(), precision)
 
 
+@pytest.mark.parametrize("shape", [(256, 256), (128, 64), (64, 64)])
+def test_batch_launch_shapes_agree(shape):
+    """Whole-CTA tiles (one group) and several tile groups per CTA (named
+    barriers) compute the same stages."""
+    alone, batched = _pair("fp64", seed=13, n=7)
+    for s in alone:
+        s.step(2)
+    bt = zbatch.Batch(batched)
+    bt.set_config(threads=shape[0], blocks_per_sm=3, order=0, group=shape[1])
+    bt.step(2)
+    bt.synchronize()
+    for s1, s2 in zip(alone, batched):
+        assert _same(s1.get_state(), s2.get_state(), "fp64")
+
+
 def test_batch_single_stages_match():
     alone, batched = _pair("fp64", seed=9, n=6)
     bt = zbatch.Batch(batched)
@@ -53,7 +68,8 @@ def test_autotune_keeps_state_and_picks_a_shape():
     before = [s.get_state() for s in cases]
     bt = zbatch.Batch(cases)
     cfg = bt.autotune(steps=2)
-    assert cfg["threads"] in (128, 256) and cfg["blocks_per_sm"] >= 1 and cfg["ms_per_step"] > 0
+    assert cfg["threads"] in (64, 128, 256) and cfg["threads"] % cfg["group"] == 0
+    assert cfg["blocks_per_sm"] >= 1 and cfg["ms_per_step"] > 0
     for s, u in zip(cases, before):
         assert np.array_equal(s.get_state(), u)
     # stepping after tuning still matches the cases stepped alone

@@ -33,7 +33,7 @@ EXPORTED = [
     "zb_destroy", "zb_info_get", "zb_set_stream", "zb_set_dt", "zb_set_state", "zb_get_state",
     "zb_compute_residual", "zb_get_residual", "zb_rk_stage", "zb_step", "zb_residual_norms",
     "zb_synchronize", "zb_launch_count", "zb_profile_enable", "zb_profile_read", "zb_kernel_name",
-    "zb_compute_residual_noalloc", "zb_functionals", "zb_vjp", "zb_set_freestream", "zb_wall_force",
+    "zb_compute_residual_noalloc", "zb_functionals", "zb_vjp", "zb_set_freestream", "zb_wall_force", "zb_vjp_geometry",
     "zb_batch_create", "zb_batch_destroy", "zb_batch_autotune", "zb_batch_set_config", "zb_batch_step",
     "zb_batch_stage", "zb_batch_synchronize", "zb_batch_launch_count",
 ]
@@ -64,7 +64,7 @@ class ZbParams(ctypes.Structure):
 
 class ZbBatchConfig(ctypes.Structure):
     _fields_ = [("threads", ctypes.c_int), ("blocks_per_sm", ctypes.c_int), ("order", ctypes.c_int),
-                ("ms_per_step", ctypes.c_double)]
+                ("ms_per_step", ctypes.c_double), ("group", ctypes.c_int)]
 
 
 class ZbDeck(ctypes.Structure):
@@ -148,6 +148,7 @@ def lib() -> ctypes.CDLL:
         L.zb_batch_launch_count.restype = i64
         L.zb_set_freestream.argtypes = [vp, ctypes.c_double, dp, ctypes.c_double]
         L.zb_vjp.argtypes = [vp, dp, dp, i64, i64, i64, ctypes.c_int, dp]
+        L.zb_vjp_geometry.argtypes = [vp, dp, dp, i64, i64, i64, ctypes.c_int, dp, dp, dp, dp, dp]
         _lib = L
     return _lib
 

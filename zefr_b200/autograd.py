@@ -81,8 +81,9 @@ class TrajectoryAdjoint:
         self.s.get_residual_device(R, 0)
         return R
 
-    def _stages(self, U0: torch.Tensor) -> Tuple[List[torch.Tensor], torch.Tensor]:
-        """Stage states U^(0..3) of one RK44 step and the updated state."""
+    def _stages(self, U0: torch.Tensor, with_residuals: bool = False):
+        """Stage states U^(0..3) of one RK44 step and the updated state (and
+        the stage residuals)."""
         Us, Rs = [U0], []
         for s in range(4):
             Rs.append(self._residual(Us[s]))
@@ -91,51 +92,80 @@ class TrajectoryAdjoint:
         Unew = U0.clone()
         for s in range(4):
             Unew = Unew - RK_BETA[s] * self.dt * self.inv_det * Rs[s]
-        return Us, Unew
+        return (Us, Unew, Rs) if with_residuals else (Us, Unew)
 
     def _step(self, U: torch.Tensor) -> torch.Tensor:
         return self._stages(U)[1]
 
     # -- reverse pieces --
-    def _vjp(self, U: torch.Tensor, lam: torch.Tensor, pbar: np.ndarray) -> torch.Tensor:
+    def _vjp(self, U: torch.Tensor, lam: torch.Tensor, pbar: np.ndarray, gbar=None) -> torch.Tensor:
         self.s.set_state(U)
-        g, p = self.s.vjp(lam.contiguous(), params=True)
+        if gbar is None:
+            g, p = self.s.vjp(lam.contiguous(), params=True)
+            pbar += p
+            return g
+        g, p, geo = self.s.vjp_geometry(lam.detach().cpu().numpy())
         pbar += p
-        return g
+        for k in gbar:
+            gbar[k] += geo[k]
+        return torch.from_numpy(g).to(U.device)
 
-    def _step_adjoint(self, U0: torch.Tensor, Ubar_new: torch.Tensor, pbar: np.ndarray) -> torch.Tensor:
-        Us, _ = self._stages(U0)
+    def _step_adjoint(self, U0: torch.Tensor, Ubar_new: torch.Tensor, pbar: np.ndarray, gbar=None) -> torch.Tensor:
+        Us, _, Rs = self._stages(U0, with_residuals=True)
         Ubar0 = Ubar_new.clone()
         Rbar = [-RK_BETA[s] * self.dt * self.inv_det * Ubar_new for s in range(4)]
+        inv2 = (self.inv_det * self.inv_det)[:, 0, :]
         for s in range(3, 0, -1):
-            Ubar_s = self._vjp(Us[s], Rbar[s], pbar)
+            Ubar_s = self._vjp(Us[s], Rbar[s], pbar, gbar)
             Ubar0 += Ubar_s
             Rbar[s - 1] = Rbar[s - 1] - RK_ALPHA[s - 1] * self.dt * self.inv_det * Ubar_s
-        Ubar0 += self._vjp(Us[0], Rbar[0], pbar)
+            if gbar is not None:
+                # U^(s) = U0 - a dt R_{s-1} / |J|
+                gbar["jaco_det"] += (RK_ALPHA[s - 1] * self.dt * (Ubar_s * Rs[s - 1]).sum(dim=1) *
+                                     inv2).cpu().numpy()
+        Ubar0 += self._vjp(Us[0], Rbar[0], pbar, gbar)
+        if gbar is not None:
+            Rsum = sum(RK_BETA[s] * Rs[s] for s in range(4))
+            gbar["jaco_det"] += (self.dt * (Ubar_new * Rsum).sum(dim=1) * inv2).cpu().numpy()
         return Ubar0
 
     @staticmethod
-    def _obj_grad(objective: Callable, U: torch.Tensor) -> Tuple[float, torch.Tensor]:
+    def _obj_grad(objective: Callable, U: torch.Tensor, geo=None):
         x = U.detach().clone().requires_grad_(True)
-        j = objective(x)
-        (g,) = torch.autograd.grad(j, x)
-        return float(j.detach()), g
+        if geo is None:
+            j = objective(x)
+            (g,) = torch.autograd.grad(j, x)
+            return float(j.detach()), g, None
+        leaves = {k: v.detach().clone().requires_grad_(True) for k, v in geo.items()}
+        j = objective(x, leaves)
+        grads = torch.autograd.grad(j, [x] + list(leaves.values()))
+        return float(j.detach()), grads[0], {k: gk.cpu().numpy() for k, gk in zip(leaves, grads[1:])}
 
-    def run(self, U0, nsteps: int, objective: Callable) -> Dict[str, object]:
-        """Returns J, dJ/dU0 (CUDA tensor) and dJ/d(rho_fs, V_fs[0..2], P_fs)."""
+    def run(self, U0, nsteps: int, objective: Callable, geometry=None) -> Dict[str, object]:
+        """Returns J, dJ/dU0 (CUDA tensor) and dJ/d(rho_fs, V_fs[0..2], P_fs).
+
+        With ``geometry`` (a dict of the current metric tensors, as
+        ``geometry.GeometryMap.metrics`` returns them), ``objective(U, geo)``
+        also takes the metrics and the result adds ``dJ_dgeometry``: the
+        gradient with respect to inv_jaco, jaco_det, norm and dA, summed over
+        the residual's adjoint, the RK update's 1/|J| and the objective."""
         U = torch.as_tensor(U0, dtype=torch.float64).cuda().contiguous()
         checkpoints = {0: U.clone()}
+        obj = objective if geometry is None else (lambda x, geo=geometry: objective(x, geo))
         J = 0.0
         with torch.no_grad():
             for k in range(1, nsteps + 1):
                 U = self._step(U)
-                J += float(objective(U))
+                J += float(obj(U))
                 if k % self.every == 0:
                     checkpoints[k] = U.clone()
         J /= nsteps
         # reverse sweep, one checkpointed segment at a time from the end
         Ubar = torch.zeros_like(U)
         pbar = np.zeros(5)
+        gbar = None
+        if geometry is not None:
+            gbar = {k: np.zeros(tuple(v.shape)) for k, v in geometry.items()}
         starts = [k for k in sorted(checkpoints) if k < nsteps]
         for i in range(len(starts) - 1, -1, -1):
             k0 = starts[i]
@@ -149,9 +179,16 @@ class TrajectoryAdjoint:
                     Unext = states[m + 1]
                 else:
                     Unext = checkpoints[k1] if k1 in checkpoints else self._step(states[m])
-                Ubar = Ubar + self._obj_grad(objective, Unext)[1] / nsteps
-                Ubar = self._step_adjoint(states[m], Ubar, pbar)
-        return {"J": J, "dJ_dU0": Ubar, "dJ_dfreestream": pbar}
+                _, gU, gG = self._obj_grad(objective, Unext, geometry)
+                Ubar = Ubar + gU / nsteps
+                if gG is not None:
+                    for k in gbar:
+                        gbar[k] += gG[k] / nsteps
+                Ubar = self._step_adjoint(states[m], Ubar, pbar, gbar)
+        out = {"J": J, "dJ_dU0": Ubar, "dJ_dfreestream": pbar}
+        if gbar is not None:
+            out["dJ_dgeometry"] = gbar
+        return out
 
 
 def kinetic_energy(solver: FRSolver) -> Callable[[torch.Tensor], torch.Tensor]:

@@ -11,8 +11,42 @@ using dev::TW;
 
 // Adjoint of the residual (plain FP64 form): lift, then the volume/face
 // pass, then for Navier-Stokes the common-solution pass.
+// The volume/face pass and the trace pass, with or without the geometry
+// outputs (a separate instantiation, so the state adjoint carries none of
+// their registers).
+template <int D, int N, bool GEO>
+static void launch_adj_kernels(Ctx &c, const dev::AdjArgs &a, const LineOpsT<double, N> &ops)
+{
+  using G = Shape<D, N>;
+  constexpr int S = G::S, Fp = G::Fp, V = G::V, NT = G::NT;
+  if (!c.plan.params.viscous)
+  {
+    const size_t smem = (size_t)(S * V + Fp * V) * TW * sizeof(double);
+    set_smem(dev::k_adj_euler<D, N, GEO>, smem);
+    ProfScope ps(c, ZB_K_ADJ_VOL);
+    dev::k_adj_euler<D, N, GEO><<<(unsigned)c.ntiles, NT, smem, c.stream>>>(a, ops);
+    c.launches++;
+    CK(cudaGetLastError());
+    return;
+  }
+  const size_t smem1 = (size_t)(2 * S * V + Fp * V + 2 * D * S * V) * TW * sizeof(double);
+  set_smem(dev::k_adj_ns1<D, N, GEO>, smem1);
+  {
+    ProfScope ps(c, ZB_K_ADJ_VOL);
+    dev::k_adj_ns1<D, N, GEO><<<(unsigned)c.ntiles, NT, smem1, c.stream>>>(a, ops);
+    c.launches++;
+    CK(cudaGetLastError());
+  }
+  const size_t smem2 = (size_t)Fp * V * TW * sizeof(double);
+  set_smem(dev::k_adj_ns2<D, N, GEO>, smem2);
+  ProfScope ps(c, ZB_K_ADJ_TRACE);
+  dev::k_adj_ns2<D, N, GEO><<<(unsigned)c.ntiles, NT, smem2, c.stream>>>(a, ops);
+  c.launches++;
+  CK(cudaGetLastError());
+}
+
 template <int D, int N>
-static void launch_vjp_impl(Ctx &c, bool params)
+static void launch_vjp_impl(Ctx &c, bool params, bool geo)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, NT = G::NT;
@@ -30,6 +64,10 @@ static void launch_vjp_impl(Ctx &c, bool params)
   a.UCb = c.UCb;
   a.Ubar = c.Ubar;
   a.pbar = params ? c.pbar : nullptr;
+  a.mbar = geo ? c.mbar : nullptr;
+  a.gbar = geo ? c.gbar : nullptr;
+  a.nbx = geo ? c.nbx : nullptr;
+  a.Fvn = (const double *)c.Fvn;
   a.ntiles = c.ntiles;
   a.ph = phys_of<double>(c.plan.params, c.uref, D, false);
   const LineOpsT<double, N> ops = line_ops<double, N>(c.plan);
@@ -39,30 +77,10 @@ static void launch_vjp_impl(Ctx &c, bool params)
     c.launches++;
     CK(cudaGetLastError());
   }
-  if (!c.plan.params.viscous)
-  {
-    const size_t smem = (size_t)(S * V + Fp * V) * TW * sizeof(double);
-    set_smem(dev::k_adj_euler<D, N>, smem);
-    ProfScope ps(c, ZB_K_ADJ_VOL);
-    dev::k_adj_euler<D, N><<<(unsigned)c.ntiles, NT, smem, c.stream>>>(a, ops);
-    c.launches++;
-    CK(cudaGetLastError());
-    return;
-  }
-  const size_t smem1 = (size_t)(2 * S * V + Fp * V + 2 * D * S * V) * TW * sizeof(double);
-  set_smem(dev::k_adj_ns1<D, N>, smem1);
-  {
-    ProfScope ps(c, ZB_K_ADJ_VOL);
-    dev::k_adj_ns1<D, N><<<(unsigned)c.ntiles, NT, smem1, c.stream>>>(a, ops);
-    c.launches++;
-    CK(cudaGetLastError());
-  }
-  const size_t smem2 = (size_t)Fp * V * TW * sizeof(double);
-  set_smem(dev::k_adj_ns2<D, N>, smem2);
-  ProfScope ps(c, ZB_K_ADJ_TRACE);
-  dev::k_adj_ns2<D, N><<<(unsigned)c.ntiles, NT, smem2, c.stream>>>(a, ops);
-  c.launches++;
-  CK(cudaGetLastError());
+  if (geo)
+    launch_adj_kernels<D, N, true>(c, a, ops);
+  else
+    launch_adj_kernels<D, N, false>(c, a, ops);
 }
 
 void bind_vjp(Ctx &c)

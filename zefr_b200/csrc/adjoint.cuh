@@ -659,6 +659,97 @@ ZB_HD_COLD void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const double 
 // Kernels
 // ---------------------------------------------------------------------------
 
+// ---- geometry adjoint: derivatives with respect to the face normal ----
+
+// nb += d (w . Fc(UL, UR, n)) / d n for an interior face (dual-number seeds on n)
+template <int D>
+ZB_HD_COLD void conv_face_n_vjp(const double UL[D + 2], const double UR[D + 2], const double n[D],
+                                const double w[D + 2], const Phys<double> &ph, double nb[D])
+{
+  constexpr int V = D + 2;
+  using DD = Dual<double>;
+  const Phys<DD> pd = dual_phys(ph);
+  DD L[V], R[V];
+  for (int v = 0; v < V; v++)
+  {
+    L[v] = DD(UL[v]);
+    R[v] = DD(UR[v]);
+  }
+  for (int k = 0; k < D; k++)
+  {
+    DD nd[D], F[V];
+    for (int d = 0; d < D; d++) nd[d] = DD(n[d], d == k ? 1.0 : 0.0);
+    conv_face<D, DD>(-1, L, R, nd, F, pd);
+    double acc = 0.0;
+    for (int v = 0; v < V; v++) acc += w[v] * F[v].d;
+    nb[k] += acc;
+  }
+}
+
+// nb += d (w . phi) / d n for the boundary face function of bnd_face_vjp
+template <int D, bool VISC>
+ZB_HD_COLD void bnd_face_n_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+                               const double w[D + 2], const Phys<double> &ph, double nb[D])
+{
+  constexpr int V = D + 2;
+  using DD = Dual<double>;
+  const Phys<DD> pd = dual_phys(ph);
+  DD L[V], dL[V][D];
+  for (int v = 0; v < V; v++)
+  {
+    L[v] = DD(U[v]);
+    for (int d = 0; d < D; d++) dL[v][d] = DD(dU[v][d]);
+  }
+  for (int k = 0; k < D; k++)
+  {
+    DD nd[D], F[V];
+    for (int d = 0; d < D; d++) nd[d] = DD(n[d], d == k ? 1.0 : 0.0);
+    conv_face<D, DD>(bc, L, L, nd, F, pd);
+    if (VISC)
+    {
+      DD UR[V], UB[V], dUB[V][D], Fn[V];
+      ghost_state<DD, D>(bc, L, nd, UR, UB, pd);
+      ghost_grad<DD, D>(bc, L, dL, nd, dUB);
+      visc_normal<DD, D>(UB, dUB, nd, Fn, pd);
+      for (int v = 0; v < V; v++) F[v] += Fn[v] + pd.ldg_tau * (L[v] - UB[v]);
+    }
+    double acc = 0.0;
+    for (int v = 0; v < V; v++) acc += w[v] * F[v].d;
+    nb[k] += acc;
+  }
+}
+
+// nb += d (w . UB(U, n)) / d n for the LDG boundary common solution
+template <int D>
+ZB_HD_COLD void bnd_ucomm_n_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+                                const Phys<double> &ph, double nb[D])
+{
+  constexpr int V = D + 2;
+  using DD = Dual<double>;
+  const Phys<DD> pd = dual_phys(ph);
+  DD L[V];
+  for (int v = 0; v < V; v++) L[v] = DD(U[v]);
+  for (int k = 0; k < D; k++)
+  {
+    DD nd[D], UR[V], UB[V];
+    for (int d = 0; d < D; d++) nd[d] = DD(n[d], d == k ? 1.0 : 0.0);
+    ghost_state<DD, D>(bc, L, nd, UR, UB, pd);
+    double acc = 0.0;
+    for (int v = 0; v < V; v++) acc += w[v] * UB[v].d;
+    nb[k] += acc;
+  }
+}
+
+// Viscous flux matrix F_visc[var][dim] of one trace (the part flux_visc_add adds)
+template <int D>
+ZB_HD void visc_matrix(const double U[D + 2], const double dU[D + 2][D], const Phys<double> &ph,
+                       double F[D + 2][D])
+{
+  for (int v = 0; v < D + 2; v++)
+    for (int d = 0; d < D; d++) F[v][d] = 0.0;
+  flux_visc_add<double, D>(U, dU, F, ph);
+}
+
 // Deterministic block sum of pb[5] into out[5] (fixed shuffle and warp order).
 __device__ __forceinline__ void block_sum5(double pb[5], double *out)
 {
@@ -694,9 +785,56 @@ struct AdjArgs
   double *UCb;         // NS: [tile][Fp][V][TW] adjoint of the own common solution
   double *Ubar;        // [tile][S][V][TW] result
   double *pbar;        // [ntiles][5] per-tile free-stream adjoint (nullptr: off)
+  // geometry adjoint (nullptr: off)
+  double *mbar;        // [tile][S][NM][TW] adjoint of the adjugate and |J|
+  double *gbar;        // [tile][Fp][D+1][TW] adjoint of the face normal (whole face, kept at the
+                       // left side or the boundary; zero at right sides) and of the own dA
+  double *nbx;         // NS: [tile][Fp][D][TW] right side's part of its face's normal adjoint
+  const double *Fvn;   // NS: forward viscous normal flux at own flux points
   int64_t ntiles;
   Phys<double> ph;
 };
+
+// Geometry adjoint of F~_d = sum_k adj[d][k] F_k at one solution point:
+// mbar(adj[d][k]) = sum_v Ft[d][v] F[v][k]; |J| gets 0 here (written, not added).
+template <int D>
+__device__ __forceinline__ void geo_adj_bar(const AdjArgs &a, int64_t tile, int s, int l, const double Ft[D][D + 2],
+                                            const double F[D + 2][D], int S)
+{
+  constexpr int NM = D * D + 1;
+  double *mb = a.mbar + (tile * S + s) * (int64_t)NM * TW + l;
+#pragma unroll
+  for (int d = 0; d < D; d++)
+#pragma unroll
+    for (int k = 0; k < D; k++)
+    {
+      double acc = 0.0;
+#pragma unroll
+      for (int v = 0; v < D + 2; v++) acc += Ft[d][v] * F[v][k];
+      mb[(d * D + k) * TW] = acc;
+    }
+  mb[D * D * TW] = 0.0;
+}
+
+// Geometry adjoint at an own flux point: the own surface term is
+// +-phi dA_own (minus on the right side), so dA_own_bar = +-Lfp . phi; the
+// normal's adjoint nb (the whole face's, or zero on a right side) is stored
+// beside it.
+template <int D, int N>
+__device__ __forceinline__ void geo_face_bar(const AdjArgs &a, int64_t tile, int f, int l, int code,
+                                             const double phi[D + 2], const double nb[D])
+{
+  constexpr int Fp = Shape<D, N>::Fp, V = D + 2;
+  const double *lo = a.Lfp + (tile * Fp + f) * (int64_t)V * TW + l;
+  double acc = 0.0;
+#pragma unroll
+  for (int v = 0; v < V; v++) acc += lo[v * TW] * phi[v];
+  const bool right = (code >= 0) && (code & 1);
+  double *g = a.gbar + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+  for (int d = 0; d < D; d++) g[d * TW] = nb[d];
+  g[D * TW] = right ? -acc : acc;
+}
 
 // Weight of the own surface flux point: the transpose of the surface
 // correction of finish_point, Lfp(f) = sum over the line of f of
@@ -733,12 +871,11 @@ __global__ void __launch_bounds__(256) k_adj_lift(const __grid_constant__ AdjArg
 // Fb[v][k] = sum_d adj[d][k] (Dm^T lam)_d[v].
 template <int D, int N>
 __device__ __forceinline__ void vol_weight(const AdjArgs &a, const LineOpsT<double, N> &ops, int64_t tile, int s, int l,
-                                           double Fb[D + 2][D])
+                                           double Fb[D + 2][D], double Ft[D][D + 2])
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, V = G::V, NM = G::NM;
   const double *Lt = a.lam + tile * (int64_t)S * V * TW;
-  double Ft[D][V];
 #pragma unroll
   for (int d = 0; d < D; d++)
   {
@@ -800,10 +937,83 @@ __device__ __forceinline__ void face_weight(const AdjArgs &a, int64_t tile, int 
   for (int v = 0; v < V; v++) w[v] = so * Lo[v] + sn * Ln[v];
 }
 
+// Navier-Stokes geometry adjoint at an own flux point: the face value
+// phi = Fc + Fv (Fv from the forward viscous normal fluxes), dA_own_bar, and
+// the normal's adjoint: the left side (or the boundary) takes the Riemann
+// part and its own viscous part; a right side leaves its viscous part in nbx
+// for the left side to collect in the second pass.
+template <int D, int N>
+__device__ __forceinline__ void geo_face_ns(const AdjArgs &a, int64_t tile, int f, int l, int code, const double n[D],
+                                            const double w[D + 2], const double Uo[D + 2],
+                                            const double dUo[D + 2][D])
+{
+  constexpr int Fp = Shape<D, N>::Fp, V = D + 2;
+  const double beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
+  double phi[V], nb[D];
+#pragma unroll
+  for (int d = 0; d < D; d++) nb[d] = 0.0;
+  const double *fo = a.Fvn + (tile * Fp + f) * (int64_t)V * TW + l;
+  if (code >= 0)
+  {
+    double Un[V];
+    gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
+    const bool own_left = !(code & 1);
+    const double *UL = own_left ? Uo : Un, *UR = own_left ? Un : Uo;
+    conv_face<D, double>(-1, UL, UR, n, phi, a.ph);
+    const double cL = 0.5 + beta, cR = 0.5 - beta;
+    double Fx[V];
+    if ((own_left && cR != 0.0) || (!own_left && cL != 0.0)) gather_fpt<double, double, V>(a.Fvn, code >> 1, Fx);
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      double fv = tau * (UL[v] - UR[v]);
+      if (cL != 0.0) fv += cL * (own_left ? fo[v * TW] : Fx[v]);
+      if (cR != 0.0) fv += cR * (own_left ? Fx[v] : fo[v * TW]);
+      phi[v] += fv;
+    }
+    const double c_own = own_left ? cL : cR;
+    double own[D];
+#pragma unroll
+    for (int d = 0; d < D; d++) own[d] = 0.0;
+    if (c_own != 0.0)
+    {
+      double Fv[V][D];
+      visc_matrix<D>(Uo, dUo, a.ph, Fv);
+#pragma unroll
+      for (int d = 0; d < D; d++)
+#pragma unroll
+        for (int v = 0; v < V; v++) own[d] += c_own * w[v] * Fv[v][d];
+    }
+    if (own_left)
+    {
+      conv_face_n_vjp<D>(UL, UR, n, w, a.ph, nb);
+#pragma unroll
+      for (int d = 0; d < D; d++) nb[d] += own[d];
+    }
+    else
+    {
+      double *x = a.nbx + (tile * Fp + f) * (int64_t)D * TW + l;
+#pragma unroll
+      for (int d = 0; d < D; d++) x[d * TW] = own[d];
+    }
+  }
+  else
+  {
+    const int bc = -code - 1;
+    double UR[V], UB[V];
+    conv_face<D, double>(bc, Uo, Uo, n, phi, a.ph);
+    ghost_state<double, D>(bc, Uo, n, UR, UB, a.ph);
+#pragma unroll
+    for (int v = 0; v < V; v++) phi[v] += fo[v * TW] + tau * (Uo[v] - UB[v]);
+    bnd_face_n_vjp<D, true>(bc, Uo, dUo, n, w, a.ph, nb);
+  }
+  geo_face_bar<D, N>(a, tile, f, l, code, phi, nb);
+}
+
 // ---------------------------------------------------------------------------
 // Euler: one kernel after k_adj_lift
 // ---------------------------------------------------------------------------
-template <int D, int N>
+template <int D, int N, bool GEO>
 __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_constant__ AdjArgs a,
                                                                const __grid_constant__ LineOpsT<double, N> ops)
 {
@@ -819,7 +1029,8 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_cons
   {
     const int s = it / TW, l = it % TW;
     double Fb[V][D], U[V], Ub[V];
-    vol_weight<D, N>(a, ops, tile, s, l, Fb);
+    double Ft[D][V];
+    vol_weight<D, N>(a, ops, tile, s, l, Fb, Ft);
     const double *ut = a.U + (tile * S + s) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++)
@@ -830,6 +1041,13 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_cons
     flux_conv_vjp<D>(U, Fb, a.ph.gamma, Ub);
 #pragma unroll
     for (int v = 0; v < V; v++) sUb[(s * V + v) * TW + l] = Ub[v];
+    if (GEO && a.mbar)
+    {
+      // F~_d = sum_k adj[d][k] F_k: adj_bar[d][k] = sum_v F~bar_d[v] F[v][k]
+      double F[V][D], P;
+      flux_conv<double, D>(U, F, P, a.ph.gamma);
+      geo_adj_bar<D>(a, tile, s, l, Ft, F, S);
+    }
   }
   for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
   {
@@ -863,6 +1081,30 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_cons
     }
 #pragma unroll
     for (int v = 0; v < V; v++) sUbfp[(f * V + v) * TW + l] = Ub[v];
+    if (GEO && a.gbar)
+    {
+      // face value phi = Fc; sFc = +-phi dA_own
+      double Fc[V], nb[D], Un[V], dUz[V][D];
+#pragma unroll
+      for (int d = 0; d < D; d++) nb[d] = 0.0;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+#pragma unroll
+        for (int d = 0; d < D; d++) dUz[v][d] = 0.0;
+      if (code >= 0)
+      {
+        gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
+        const bool own_left = !(code & 1);
+        conv_face<D, double>(-1, own_left ? Uo : Un, own_left ? Un : Uo, n, Fc, a.ph);
+        if (own_left) conv_face_n_vjp<D>(Uo, Un, n, w, a.ph, nb);
+      }
+      else
+      {
+        conv_face<D, double>(-code - 1, Uo, Uo, n, Fc, a.ph);
+        bnd_face_n_vjp<D, false>(-code - 1, Uo, dUz, n, w, a.ph, nb);
+      }
+      geo_face_bar<D, N>(a, tile, f, l, code, Fc, nb);
+    }
   }
   if (a.pbar) block_sum5(pb, a.pbar + tile * 5);
   __syncthreads();
@@ -892,7 +1134,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_cons
 // the volume flux, of the face fluxes and of the gradient; writes the partial
 // solution-point result, the trace adjoint and the common-solution adjoint.
 // ---------------------------------------------------------------------------
-template <int D, int N>
+template <int D, int N, bool GEO>
 __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_constant__ AdjArgs a,
                                                              const __grid_constant__ LineOpsT<double, N> ops)
 {
@@ -993,7 +1235,8 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
   {
     const int s = it / TW, l = it % TW;
     double Fb[V][D], U[V], dU[V][D], Ub[V], dUb[V][D];
-    vol_weight<D, N>(a, ops, tile, s, l, Fb);
+    double Ft[D][V];
+    vol_weight<D, N>(a, ops, tile, s, l, Fb, Ft);
 #pragma unroll
     for (int v = 0; v < V; v++)
     {
@@ -1014,6 +1257,13 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
       sUb[(s * V + v) * TW + l] = Ub[v];
 #pragma unroll
       for (int d = 0; d < D; d++) sG[((d * S + s) * V + v) * TW + l] = dUb[v][d];
+    }
+    if (GEO && a.mbar)
+    {
+      double F[V][D], P;
+      flux_conv<double, D>(U, F, P, a.ph.gamma);
+      flux_visc_add<double, D>(U, dU, F, a.ph);
+      geo_adj_bar<D>(a, tile, s, l, Ft, F, S);
     }
   }
   // adjoint of the face fluxes at own flux points
@@ -1060,6 +1310,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
       bnd_face_vjp<D, true>(-code - 1, Uo, dUo, n, w, dual_phys(a.ph), Ub, dUb);
       if (a.pbar) bnd_face_param_vjp<D, true>(-code - 1, Uo, dUo, n, w, dual_phys(a.ph), pb);
     }
+    if (GEO && a.gbar) geo_face_ns<D, N>(a, tile, f, l, code, n, w, Uo, dUo);
     double *ub = a.Ubfp + (tile * Fp + f) * (int64_t)V * TW + l;
     double *dub = a.dUbfp + (tile * Fp + f) * (int64_t)V * D * TW + l;
 #pragma unroll
@@ -1095,6 +1346,42 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
     }
     const double *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
     const double inv_det = 1.0 / m[D * D * TW];
+    if (GEO && a.mbar)
+    {
+      // dU[v][d1] = sum_d2 tdU[v][d2] adj[d2][d1] / |J|
+      double *mb = a.mbar + (tile * S + s) * (int64_t)NM * TW + l;
+      double detb = 0.0;
+#pragma unroll
+      for (int d2 = 0; d2 < D; d2++)
+      {
+        int i, fm, fp;
+        spt_ends<D, N>(s, d2, i, fm, fp);
+        const int st = pow_n<N>(d2);
+        const int b = s - i * st;
+        double ab[D];
+#pragma unroll
+        for (int d1 = 0; d1 < D; d1++) ab[d1] = 0.0;
+#pragma unroll
+        for (int v = 0; v < V; v++)
+        {
+          double acc = 0.0;
+#pragma unroll
+          for (int mm = 0; mm < N; mm++) acc += ops.Dm[i * N + mm] * sU[((b + mm * st) * V + v) * TW + l];
+          const double cm = ops.Dbm[i] * sUC[(fm * V + v) * TW + l];
+          const double cp = ops.Dbp[i] * sUC[(fp * V + v) * TW + l];
+          const double tdu = acc + ((fm < fp) ? (cm + cp) : (cp + cm));
+#pragma unroll
+          for (int d1 = 0; d1 < D; d1++) ab[d1] += g[v][d1] * tdu;
+        }
+#pragma unroll
+        for (int d1 = 0; d1 < D; d1++) mb[(d2 * D + d1) * TW] += ab[d1] * inv_det;
+      }
+#pragma unroll
+      for (int v = 0; v < V; v++)
+#pragma unroll
+        for (int d1 = 0; d1 < D; d1++) detb -= g[v][d1] * sdU[((d1 * S + s) * V + v) * TW + l];
+      mb[D * D * TW] += detb * inv_det;
+    }
 #pragma unroll
     for (int v = 0; v < V; v++)
 #pragma unroll
@@ -1172,6 +1459,16 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
       }
       bnd_ucomm_vjp<D>(-code - 1, Uo, n, ucb, dual_phys(a.ph), Ub);
       if (a.pbar) bnd_ucomm_param_vjp<D>(-code - 1, Uo, n, ucb, dual_phys(a.ph), pb);
+      if (GEO && a.gbar)
+      {
+        double nb[D];
+#pragma unroll
+        for (int d = 0; d < D; d++) nb[d] = 0.0;
+        bnd_ucomm_n_vjp<D>(-code - 1, Uo, n, ucb, a.ph, nb);
+        double *gg = a.gbar + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+        for (int d = 0; d < D; d++) gg[d * TW] += nb[d];
+      }
 #pragma unroll
       for (int v = 0; v < V; v++) ub[v * TW] += Ub[v];
     }
@@ -1183,7 +1480,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
 // Navier-Stokes pass 2: both sides' common-solution adjoints reach the own
 // trace, then the transposed extrapolation finishes Ubar.
 // ---------------------------------------------------------------------------
-template <int D, int N>
+template <int D, int N, bool GEO>
 __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns2(const __grid_constant__ AdjArgs a,
                                                              const __grid_constant__ LineOpsT<double, N> ops)
 {
@@ -1202,6 +1499,15 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns2(const __grid_consta
     double Ub[V];
 #pragma unroll
     for (int v = 0; v < V; v++) Ub[v] = ub[v * TW];
+    if (GEO && a.gbar && code >= 0 && !(code & 1))
+    {
+      // collect the right side's viscous part of this face's normal adjoint
+      const int pidx = code >> 1;
+      double *gg = a.gbar + (tile * Fp + f) * (int64_t)(D + 1) * TW + l;
+#pragma unroll
+      for (int d = 0; d < D; d++)
+        gg[d * TW] += a.nbx[((int64_t)(pidx / TW) * D + d) * TW + pidx % TW];
+    }
     if (code >= 0)
     {
       // UC = (1/2 - beta) UL + (1/2 + beta) UR, shared by both sides

@@ -33,26 +33,49 @@ struct BatchCase
   A ops[kBatchMaxN * kBatchMaxN + 4 * kBatchMaxN];  // LineOpsT<A, N> laid out flat
 };
 
+// Shared memory of one tile group: its copy of the case descriptor, then the
+// tile body's arrays.
+template <typename T, typename A>
+constexpr size_t batch_desc_bytes()
+{
+  return (sizeof(BatchCase<T, A>) + 15) / 16 * 16;
+}
+
+// A CTA holds blockDim.x / gsz independent groups of gsz threads (whole warps);
+// each group walks its own share of the work items with its own named barrier,
+// so low-order tiles do not leave most of a large CTA idle.
 template <typename T, typename A>
 __global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__restrict__ cases,
-                                                     const int2 *__restrict__ items, int nitems)
+                                                     const int2 *__restrict__ items, int nitems, int gsz,
+                                                     int gstride)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x)
+  const int ng = blockDim.x / gsz, g = threadIdx.x / gsz, tid = threadIdx.x % gsz;
+  const int bar = (ng == 1) ? 0 : g + 1;
+  unsigned char *gbase = smem_raw + (size_t)g * gstride;
+  BatchCase<T, A> *sbc = reinterpret_cast<BatchCase<T, A> *>(gbase);
+  unsigned char *tsm = gbase + batch_desc_bytes<T, A>();
+  constexpr int nwords = (int)(sizeof(BatchCase<T, A>) / sizeof(int));
+  for (int it = blockIdx.x * ng + g; it < nitems; it += gridDim.x * ng)
   {
     const int2 w = items[it];
-    const BatchCase<T, A> &bc = cases[w.x];
-    switch (bc.N)
+    // the descriptor is read throughout the tile: keep a shared copy
+    const int *src = reinterpret_cast<const int *>(&cases[w.x]);
+    int *dst = reinterpret_cast<int *>(sbc);
+    for (int k = tid; k < nwords; k += gsz) dst[k] = src[k];
+    dev::group_sync(bar, gsz);
+    switch (sbc->N)
     {
-#define ZB_BATCH_N(NN)                                                                                         \
-  case NN:                                                                                                     \
-    dev::euler_tile<T, A, 2, NN>(bc.a, *reinterpret_cast<const LineOpsT<A, NN> *>(bc.ops), w.y, smem_raw); \
+#define ZB_BATCH_N(NN)                                                                                            \
+  case NN:                                                                                                        \
+    dev::euler_tile<T, A, 2, NN>(sbc->a, *reinterpret_cast<const LineOpsT<A, NN> *>(sbc->ops), w.y, tsm, tid, gsz, \
+                                 bar);                                                                            \
     break;
       ZB_BATCH_N(2) ZB_BATCH_N(3) ZB_BATCH_N(4) ZB_BATCH_N(5) ZB_BATCH_N(6)
 #undef ZB_BATCH_N
       default: break;
     }
-    __syncthreads();
+    dev::group_sync(bar, gsz);
   }
 }
 
@@ -78,9 +101,10 @@ struct Batch
   int2 *items = nullptr;
   int nitems = 0;
   std::vector<int> parity;  // Ufp parity of every case the descriptors assume
-  size_t smem = 0;
+  size_t smem = 0;     // tile arrays of one group (largest order)
+  size_t gstride = 0;  // one group's shared memory: descriptor + tile arrays
   int sms = 148;
-  zb_batch_config cfg{256, 4, 0, 0.0};
+  zb_batch_config cfg{256, 4, 0, 0.0, 64};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int64_t launches = 0;
@@ -162,9 +186,10 @@ static void build_items(Batch &b, int order)
 template <typename T, typename A>
 static void launch_stage_t(Batch &b, unsigned st)
 {
-  const int blocks = std::max(1, std::min(b.nitems, b.cfg.blocks_per_sm * b.sms));
-  k_batch_euler<T, A><<<blocks, b.cfg.threads, b.smem, b.stream>>>((const BatchCase<T, A> *)b.cases[st], b.items,
-                                                                    b.nitems);
+  const int ng = b.cfg.threads / b.cfg.group;
+  const int blocks = std::max(1, std::min((b.nitems + ng - 1) / ng, b.cfg.blocks_per_sm * b.sms));
+  k_batch_euler<T, A><<<blocks, b.cfg.threads, ng * b.gstride, b.stream>>>(
+      (const BatchCase<T, A> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride);
   b.launches++;
   CK(cudaGetLastError());
 }
@@ -191,13 +216,14 @@ static void build_graph(Batch &b)
   CK(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
   for (unsigned st = 0; st < 4; st++)
   {
-    const int blocks = std::max(1, std::min(b.nitems, b.cfg.blocks_per_sm * b.sms));
+    const int ng = b.cfg.threads / b.cfg.group;
+    const int blocks = std::max(1, std::min((b.nitems + ng - 1) / ng, b.cfg.blocks_per_sm * b.sms));
     if (b.prec == ZB_FP64)
-      k_batch_euler<double, double><<<blocks, b.cfg.threads, b.smem, b.stream>>>(
-          (const BatchCase<double, double> *)b.cases[st], b.items, b.nitems);
+      k_batch_euler<double, double><<<blocks, b.cfg.threads, ng * b.gstride, b.stream>>>(
+          (const BatchCase<double, double> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride);
     else
-      k_batch_euler<float, float><<<blocks, b.cfg.threads, b.smem, b.stream>>>(
-          (const BatchCase<float, float> *)b.cases[st], b.items, b.nitems);
+      k_batch_euler<float, float><<<blocks, b.cfg.threads, ng * b.gstride, b.stream>>>(
+          (const BatchCase<float, float> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride);
   }
   cudaError_t e = cudaStreamEndCapture(b.stream, &b.graph);
   if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -256,12 +282,15 @@ Batch *batch_create(Ctx *const *ctxs, int n)
   int maxN = 2;
   for (Ctx *c : b->ctx) maxN = std::max(maxN, c->N);
   b->smem = euler_smem_bytes(maxN, b->asz);
+  b->gstride = (b->prec == ZB_FP64 ? batch_desc_bytes<double, double>() : batch_desc_bytes<float, float>()) +
+               (b->smem + 15) / 16 * 16;
   CK(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev0));
   CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  const int max_smem = (int)(4 * b->gstride);  // up to four groups per CTA
   if (b->prec == ZB_FP64)
-    CK(cudaFuncSetAttribute(k_batch_euler<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+    CK(cudaFuncSetAttribute(k_batch_euler<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
   else
-    CK(cudaFuncSetAttribute(k_batch_euler<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+    CK(cudaFuncSetAttribute(k_batch_euler<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
   build_items(*b, b->cfg.order);
   return b.release();
 }
@@ -332,17 +361,18 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  const int threads[] = {128, 256};
+  const int shapes[][2] = {{64, 64}, {128, 64}, {128, 128}, {256, 64}, {256, 128}, {256, 256}};
   const int bps[] = {2, 4, 8, 16};
   const int orders[] = {0, 1};
-  zb_batch_config best{0, 0, 0, 1e300};
+  zb_batch_config best{0, 0, 0, 1e300, 0};
   for (int order : orders)
   {
     build_items(*b, order);
-    for (int th : threads)
+    for (const auto &sh : shapes)
       for (int bp : bps)
       {
-        b->cfg.threads = th;
+        b->cfg.threads = sh[0];
+        b->cfg.group = sh[1];
         b->cfg.blocks_per_sm = bp;
         b->cfg.order = order;
         build_graph(*b);
@@ -354,7 +384,7 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e0, e1));
         const double per = ms / steps;
-        if (per < best.ms_per_step) best = zb_batch_config{th, bp, order, per};
+        if (per < best.ms_per_step) best = zb_batch_config{sh[0], bp, order, per, sh[1]};
       }
   }
   cudaEventDestroy(e0);
@@ -382,7 +412,10 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
 
 void batch_config(Batch *b, const zb_batch_config *cfg)
 {
-  if (cfg->threads != 128 && cfg->threads != 256) ZB_THROW(ZB_ERR_ARG, "threads must be 128 or 256");
+  if (cfg->threads != 64 && cfg->threads != 128 && cfg->threads != 256)
+    ZB_THROW(ZB_ERR_ARG, "threads must be 64, 128 or 256");
+  if (cfg->group < 64 || cfg->group > cfg->threads || cfg->threads % cfg->group != 0 || cfg->group % 32 != 0)
+    ZB_THROW(ZB_ERR_ARG, "group must be a multiple of 32, at least 64, dividing threads");
   if (cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 64) ZB_THROW(ZB_ERR_ARG, "blocks_per_sm out of range");
   if (cfg->order != 0 && cfg->order != 1) ZB_THROW(ZB_ERR_ARG, "order must be 0 or 1");
   CK(cudaStreamSynchronize(b->stream));

@@ -159,6 +159,10 @@ zb_status zb_plan_get(const zb_plan *plan, const char *name, double *out, int64_
     else if (nm == "weights_spts") put(p.weights_spts);
     else if (nm == "loc_spts") put(p.loc_spts);
     else if (nm == "loc_fpts") put(p.loc_fpts);
+    else if (nm == "tnorm") put(p.tnorm);
+    else if (nm == "dshape_spts") put(p.dshape_spts);
+    else if (nm == "dshape_fpts") put(p.dshape_fpts);
+    else if (nm == "shape_fpts") put(p.shape_fpts);
     else if (nm == "fpt_partner")
     {
       tmp.assign(p.partner.begin(), p.partner.end());
@@ -416,6 +420,18 @@ zb_status zb_wall_force(zb_ctx *ctx, double *out)
   ZB_GUARD({
     ZB_REQUIRE(ctx && out, "null argument");
     zb::ctx_wall_force(ctx->impl, out);
+  })
+}
+
+zb_status zb_vjp_geometry(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride, int64_t var_stride,
+                          int64_t ele_stride, int where, double *param_bar, double *inv_jaco_bar,
+                          double *jaco_det_bar, double *norm_bar, double *dA_bar)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && lam && Ubar && inv_jaco_bar && jaco_det_bar && norm_bar && dA_bar, "null argument");
+    ZB_REQUIRE(where == ZB_HOST || where == ZB_DEVICE, "where must be ZB_HOST or ZB_DEVICE");
+    zb::ctx_vjp(ctx->impl, lam, Ubar, spt_stride, var_stride, ele_stride, where, param_bar, inv_jaco_bar,
+                jaco_det_bar, norm_bar, dA_bar);
   })
 }
 

@@ -500,7 +500,8 @@ static void free_all(Ctx *c)
 {
   void *bufs[] = {c->U, c->U_ini, c->divF[0], c->divF[1], c->divF[2], c->divF[3], c->divF_vol, c->Ufp[0],
                   c->Ufp[1], c->Fvn, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
-                  c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubar, c->pbar, c->dops, c->dwall};
+                  c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubar, c->pbar, c->dops, c->dwall,
+                  c->mbar, c->gbar, c->nbx};
   for (void *b : bufs)
     if (b) cudaFree(b);
   for (auto &r : c->recs)
@@ -926,8 +927,11 @@ void ctx_functionals(Ctx *c, double *out)
 }
 
 void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, int64_t es, int where,
-             double *param_bar)
+             double *param_bar, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar, double *dA_bar)
 {
+  const bool geo = inv_jaco_bar || jaco_det_bar || norm_bar || dA_bar;
+  if (geo && !(inv_jaco_bar && jaco_det_bar && norm_bar && dA_bar))
+    ZB_THROW(ZB_ERR_ARG, "the geometry adjoint needs all four output arrays");
   if (c->prec != ZB_FP64) ZB_THROW(ZB_ERR_UNSUPPORTED, "the adjoint is built for the plain FP64 form only");
   if (!c->launch_vjp)
     ZB_THROW(ZB_ERR_UNSUPPORTED, "no adjoint kernels for ndims=" + std::to_string(c->D) + " P=" + std::to_string(c->N - 1));
@@ -960,8 +964,54 @@ void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, in
   // linearisation point: the current state and its traces
   c->ufp_valid = false;
   ensure_ufp(c);
-  c->launch_vjp(*c, param_bar != nullptr);
+  const int NM = c->D * c->D + 1;
+  if (geo)
+  {
+    if (!c->mbar)
+    {
+      c->mbar = (double *)dalloc((size_t)c->ntiles * c->S * NM * TW * sizeof(double));
+      c->gbar = (double *)dalloc((size_t)c->ntiles * c->Fp * (c->D + 1) * TW * sizeof(double));
+      c->nbx = (double *)dalloc((size_t)c->ntiles * c->Fp * c->D * TW * sizeof(double));
+    }
+    // the face values need the forward viscous normal fluxes of this state
+    // (residual register 0 is overwritten with this state's residual)
+    if (c->plan.params.viscous)
+    {
+      StageCfg sc{0, 0, 0, 0};
+      c->launch_stage(*c, sc);
+    }
+  }
+  c->launch_vjp(*c, param_bar != nullptr, geo);
   from_tiles(c, c->Ubar, nullptr, nullptr, Ubar, ss, vs, es, where);
+  if (geo)
+  {
+    // tile layout -> the reference's inv_jaco_spts [D][S][D][E], jaco_det_spts
+    // [S][E], face norm [Fp][D][E] and dA [Fp][E] layouts
+    const int S = c->S, Fp = c->Fp, D = c->D;
+    const int64_t E = c->plan.neles;
+    std::vector<double> hm((size_t)c->ntiles * S * NM * TW), hg((size_t)c->ntiles * Fp * (D + 1) * TW);
+    CK(cudaMemcpyAsync(hm.data(), c->mbar, hm.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hg.data(), c->gbar, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int64_t e = 0; e < E; e++)
+    {
+      const int64_t t = e / TW;
+      const int l = (int)(e % TW);
+      for (int sp = 0; sp < S; sp++)
+      {
+        for (int d1 = 0; d1 < D; d1++)
+          for (int d2 = 0; d2 < D; d2++)
+            inv_jaco_bar[(((size_t)d1 * S + sp) * D + d2) * E + e] = hm[(((size_t)t * S + sp) * NM + d1 * D + d2) * TW + l];
+        jaco_det_bar[(size_t)sp * E + e] = hm[(((size_t)t * S + sp) * NM + D * D) * TW + l];
+      }
+      for (int f = 0; f < Fp; f++)
+      {
+        for (int d = 0; d < D; d++)
+          norm_bar[((size_t)f * D + d) * E + e] = hg[(((size_t)t * Fp + f) * (D + 1) + d) * TW + l];
+        dA_bar[(size_t)f * E + e] = hg[(((size_t)t * Fp + f) * (D + 1) + D) * TW + l];
+      }
+    }
+  }
   if (param_bar)
   {
     std::vector<double> h((size_t)c->ntiles * 5);

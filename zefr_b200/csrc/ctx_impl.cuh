@@ -78,9 +78,10 @@ struct Ctx
   // adjoint (plain FP64 form), allocated on first use
   double *lam = nullptr, *Lfp = nullptr, *Ubfp = nullptr, *dUbfp = nullptr, *UCb = nullptr, *Ubar = nullptr;
   double *pbar = nullptr;
+  double *mbar = nullptr, *gbar = nullptr, *nbx = nullptr;  // geometry adjoint
   void (*launch_extrap)(Ctx &) = nullptr;
   void (*launch_stage)(Ctx &, const StageCfg &) = nullptr;
-  void (*launch_vjp)(Ctx &, bool) = nullptr;
+  void (*launch_vjp)(Ctx &, bool, bool) = nullptr;
 };
 
 static cudaEvent_t take_event(Ctx &c)

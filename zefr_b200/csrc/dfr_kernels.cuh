@@ -150,11 +150,27 @@ __device__ __forceinline__ void face_dim_side(int face, int &dim, int &side)
 }
 
 template <typename A, int N>
-__device__ __forceinline__ void load_ops(A *sops, const LineOpsT<A, N> &ops)
+__device__ __forceinline__ void load_ops(A *sops, const LineOpsT<A, N> &ops, int tid, int nth)
 {
   const A *src = reinterpret_cast<const A *>(&ops);
   constexpr int n = N * N + 4 * N;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) sops[i] = src[i];
+  for (int i = tid; i < n; i += nth) sops[i] = src[i];
+}
+
+template <typename A, int N>
+__device__ __forceinline__ void load_ops(A *sops, const LineOpsT<A, N> &ops)
+{
+  load_ops<A, N>(sops, ops, threadIdx.x, blockDim.x);
+}
+
+// Barrier of the threads running one tile: the whole block (bar == 0) or a
+// warp-aligned group of nth threads on named barrier `bar` (batched stages).
+__device__ __forceinline__ void group_sync(int bar, int nth)
+{
+  if (bar == 0)
+    __syncthreads();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nth) : "memory");
 }
 
 // Shared-memory views of the line operators
@@ -344,11 +360,12 @@ __device__ __forceinline__ void finish_point(const Args<T, A> &a, int64_t tile, 
 }
 
 template <typename T, typename A, int D, int N>
-__device__ __forceinline__ void extrap_next_tile(const Args<T, A> &a, int64_t tile, const A *sUnew, const SOps<A, N> &o)
+__device__ __forceinline__ void extrap_next_tile(const Args<T, A> &a, int64_t tile, const A *sUnew, const SOps<A, N> &o,
+                                                 int tid, int nth)
 {
   using G = Shape<D, N>;
   constexpr int Fp = G::Fp, V = G::V;
-  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  for (int it = tid; it < Fp * TW; it += nth)
   {
     const int f = it / TW, l = it % TW;
     T *out = a.Ufp_next + (tile * Fp + f) * (int64_t)V * TW;
@@ -357,12 +374,18 @@ __device__ __forceinline__ void extrap_next_tile(const Args<T, A> &a, int64_t ti
   }
 }
 
+template <typename T, typename A, int D, int N>
+__device__ __forceinline__ void extrap_next_tile(const Args<T, A> &a, int64_t tile, const A *sUnew, const SOps<A, N> &o)
+{
+  extrap_next_tile<T, A, D, N>(a, tile, sUnew, o, threadIdx.x, blockDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // Euler: volume flux, common flux and divergence of one tile in one kernel.
 // ---------------------------------------------------------------------------
 template <typename T, typename A, int D, int N>
 __device__ __forceinline__ void euler_tile(const Args<T, A> &a, const LineOpsT<A, N> &ops, int64_t tile,
-                                           unsigned char *smem_raw)
+                                           unsigned char *smem_raw, int tid, int nth, int bar)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, NM = G::NM;
@@ -370,15 +393,15 @@ __device__ __forceinline__ void euler_tile(const Args<T, A> &a, const LineOpsT<A
   A *sF = sU + S * V * TW;
   A *sFc = sF + D * S * V * TW;
   A *sops = sFc + Fp * V * TW;
-  load_ops<A, N>(sops, ops);
+  load_ops<A, N>(sops, ops, tid, nth);
   {
     const T *src = a.U + tile * (int64_t)S * V * TW;
-    for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
+    for (int i = tid; i < S * V * TW; i += nth) sU[i] = src[i];
   }
-  __syncthreads();
+  group_sync(bar, nth);
   SOps<A, N> o(sops);
   // transformed volume flux F~ = adj F (src/elements.cpp:1588-1699)
-  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  for (int it = tid; it < S * TW; it += nth)
   {
     const int s = it / TW, l = it % TW;
     A U[V], F[V][D], P, Pp;
@@ -403,7 +426,7 @@ __device__ __forceinline__ void euler_tile(const Args<T, A> &a, const LineOpsT<A
       }
   }
   // common flux at the tile's flux points
-  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  for (int it = tid; it < Fp * TW; it += nth)
   {
     const int f = it / TW, l = it % TW;
     const int64_t fi = (tile * Fp + f) * (int64_t)TW + l;
@@ -423,8 +446,8 @@ __device__ __forceinline__ void euler_tile(const Args<T, A> &a, const LineOpsT<A
 #pragma unroll
     for (int v = 0; v < V; v++) sFc[(f * V + v) * TW + l] = right ? -Fc[v] * dA : Fc[v] * dA;
   }
-  __syncthreads();
-  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+  group_sync(bar, nth);
+  for (int it = tid; it < S * TW; it += nth)
   {
     const int s = it / TW, l = it % TW;
     A vol[V];
@@ -449,8 +472,8 @@ __device__ __forceinline__ void euler_tile(const Args<T, A> &a, const LineOpsT<A
   }
   if (a.extrap_next)
   {
-    __syncthreads();
-    extrap_next_tile<T, A, D, N>(a, tile, sU, o);
+    group_sync(bar, nth);
+    extrap_next_tile<T, A, D, N>(a, tile, sU, o, tid, nth);
   }
 }
 
@@ -469,7 +492,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_euler(const __grid_constant
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
-  euler_tile<T, A, D, N>(a, ops, tile, smem_raw);
+  euler_tile<T, A, D, N>(a, ops, tile, smem_raw, threadIdx.x, blockDim.x, 0);
 }
 
 // ---------------------------------------------------------------------------

@@ -501,6 +501,9 @@ void build_plan(const zb_mesh &mesh, const zb_params &params, Plan &p)
   Shape shs = (p.etype == ET_TRI) ? simplex_shape(nn, p.loc_spts, S) : tensor_shape(mesh.gmsh_type, D, p.loc_spts, S);
   Shape shf = (p.etype == ET_TRI) ? simplex_shape(nn, p.loc_fpts, Fp) : tensor_shape(mesh.gmsh_type, D, p.loc_fpts, Fp);
 
+  p.dshape_spts = shs.dval;
+  p.dshape_fpts = shf.dval;
+  p.shape_fpts = shf.val;
   p.coord_spts.assign((size_t)S * D * E, 0.0);
   p.coord_fpts.assign((size_t)Fp * D * E, 0.0);
   p.jaco_det_spts.assign((size_t)S * E, 0.0);

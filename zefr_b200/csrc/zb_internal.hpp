@@ -69,6 +69,9 @@ struct Plan
   std::vector<double> jaco_det_spts; // [S][E]
   std::vector<double> inv_jaco_spts; // [D][S][D][E]  (adjugate)
   std::vector<double> weights_spts;  // [S]
+  std::vector<double> dshape_spts;   // [D][S][nNodes] shape-function derivatives (geometry adjoint)
+  std::vector<double> dshape_fpts;   // [D][Fp][nNodes]
+  std::vector<double> shape_fpts;    // [Fp][nNodes]
 
   // Face connectivity per element flux point
   std::vector<int64_t> partner;  // [Fp][E]: e'*Fp + f' (interior) or -1-bc (boundary)

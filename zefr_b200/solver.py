@@ -297,6 +297,26 @@ class FRSolver:
         check(lib().zb_wall_force(self.h, out.ctypes.data_as(_DP)))
         return {"force": out[:3].copy(), "moment": out[3:].copy()}
 
+    def vjp_geometry(self, lam):
+        """Adjoint of the residual at the current state with respect to the
+        state, the free-stream state and the geometry (plain FP64 form, host
+        arrays): returns (Ubar, pbar, {"inv_jaco": [D,S,D,E], "jaco_det":
+        [S,E], "norm": [Fp,D,E], "dA": [Fp,E]})."""
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        if lam.shape != self.state_shape:
+            raise ValueError(f"lam shape {lam.shape} != {self.state_shape}")
+        S, V, E = self.state_shape
+        D, Fp = self.ndims, self.info.nfpts
+        out = np.zeros(self.state_shape)
+        pbar = np.zeros(5)
+        g = {"inv_jaco": np.zeros((D, S, D, E)), "jaco_det": np.zeros((S, E)), "norm": np.zeros((Fp, D, E)),
+             "dA": np.zeros((Fp, E))}
+        check(lib().zb_vjp_geometry(self.h, lam.ctypes.data_as(_DP), out.ctypes.data_as(_DP), *self._strides(),
+                                    _lib.ZB_HOST, pbar.ctypes.data_as(_DP), g["inv_jaco"].ctypes.data_as(_DP),
+                                    g["jaco_det"].ctypes.data_as(_DP), g["norm"].ctypes.data_as(_DP),
+                                    g["dA"].ctypes.data_as(_DP)))
+        return out, pbar, g
+
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().zb_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
 
