@@ -135,11 +135,13 @@ def build_solver(precision: str, n: int):
 
 def barrier_sync(world):
     import torch
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-        torch.cuda.synchronize()
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
 
 
 def max_over_ranks(x: float, world: int) -> float:
@@ -147,7 +149,8 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -538,13 +541,19 @@ def gpu_arm(args):
 
 
 def profile_run(args):
-    """Short run of one form for an external profiler: W + K residuals, no timing."""
+    """Short run of one form for an external profiler: W + K residuals (or
+    adjoint applications at the FP64 form), no timing."""
     import torch
     torch.cuda.set_device(0)
-    s, U = build_solver(args.profile_form, args.cells)
+    adj = args.profile_form == "adjoint"
+    s, U = build_solver("fp64" if adj else args.profile_form, args.cells)
     s.set_state(U)
+    lam = torch.ones(s.state_shape, dtype=torch.float64, device="cuda") if adj else None
     for i in range(args.warmup + args.steps):
-        s.compute_residual(i % 4)
+        if adj:
+            s.vjp(lam)
+        else:
+            s.compute_residual(i % 4)
     torch.cuda.synchronize()
     s.close()
 
@@ -602,7 +611,7 @@ def main():
     ap.add_argument("--ref-cells", type=int, default=20, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-side", action="store_true", help="skip the triangle and batched side workloads")
-    ap.add_argument("--profile-form", choices=["mixed", "fp64"], default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--profile-form", choices=["mixed", "fp64", "adjoint"], default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
