@@ -40,6 +40,9 @@ TGV_DECK = dict(ndims=3, order=ORDER, viscous=1, disable_nondim=1, fix_vis=1, ma
                 prandtl=0.71, P_fs=1.0, rho_fs=1.0, L_fs=1.0, ldg_b=0.5, ldg_tau=0.1, dt=5e-4, gamma=1.4)
 
 
+MIXED_DRAM_BYTES_PER_ELEMENT = 20150.0
+
+
 def b_alg(E: int, S: int, V: int, D: int, G: int, Fp: int, w: int) -> float:
     """Compulsory bytes of one residual: state in + residual out, adjugate + |J|
     at solution points, face normal + two dA per face point, int32 partner +
@@ -470,13 +473,11 @@ def gpu_arm(args):
     b64 = b_alg(E, S, V, D, G, Fp, 8)
     achieved = bm / (t_res * 1e-3) / 1e9
     t_res64 = sum(prof_fp64[k]["ms_avg"] for k in prof_fp64 if k in res_kernels)
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic_per_element.json")
-    if os.path.exists(tf):
-        try:
-            traffic = json.load(open(tf))["mixed_bytes_per_element_per_residual"] * E
-        except Exception:
-            traffic = None
+    # DRAM bytes (read + write) per element of one mixed-form residual
+    # (k_hex_extrap + k_hex_ns_grad + k_hex_ns_face), measured by ncu
+    # (dram__bytes_read.sum + dram__bytes_write.sum) on the same workload at
+    # 48^3 hexes, state 141 MB > L2; it grows with the element count
+    traffic = MIXED_DRAM_BYTES_PER_ELEMENT * E
     value = world * dof / (ms_mixed * 1e-3) / 1e9
     line = {
         "metric": METRIC,
