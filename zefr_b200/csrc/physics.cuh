@@ -229,14 +229,15 @@ ZB_HD void rusanov(const T UL[D + 2], const T UR[D + 2], const T n[D], T Fc[D + 
   T AL[D + 2], AR[D + 2];
   to_abs<T, D>(UL, AL, ph);
   to_abs<T, D>(UR, AR, ph);
-  const T aL = dsqrt<T>(ph.gamma * PL / AL[0]);
-  const T aR = dsqrt<T>(ph.gamma * PR / AR[0]);
-  T VnL = AL[1] / AL[0] * n[0], VnR = AR[1] / AR[0] * n[0];
+  const T irL = T(1) / AL[0], irR = T(1) / AR[0];
+  const T aL = dsqrt<T>(ph.gamma * PL * irL);
+  const T aR = dsqrt<T>(ph.gamma * PR * irR);
+  T VnL = AL[1] * irL * n[0], VnR = AR[1] * irR * n[0];
 #pragma unroll
   for (int d = 1; d < D; d++)
   {
-    VnL += AL[d + 1] / AL[0] * n[d];
-    VnR += AR[d + 1] / AR[0] * n[d];
+    VnL += AL[d + 1] * irL * n[d];
+    VnR += AR[d + 1] * irR * n[d];
   }
   const T eig = dmax<T>(dabs<T>(VnL) + aL, dabs<T>(VnR) + aR);
   const T diss = T(0.5) * eig * (T(1) - ph.rus_k);
@@ -273,17 +274,20 @@ ZB_HD void roe(const T SL[D + 2], const T SR[D + 2], const T n[D], T Fc[D + 2],
   const T rL = UL[0], rR = UR[0];
   const T sL = dsqrt<T>(rL), sR = dsqrt<T>(rR);
   const T inv = T(1) / (sL + sR);
-  T u[D];
+  // one reciprocal per state: velocities and enthalpies by multiplication
+  const T irL = T(1) / rL, irR = T(1) / rR;
+  T u[D], uL[D], uR[D];
   T unL = T(0), unR = T(0);
 #pragma unroll
   for (int d = 0; d < D; d++)
   {
-    const T uL = UL[d + 1] / rL, uR = UR[d + 1] / rR;
-    u[d] = (sL * uL + sR * uR) * inv;
-    unL += uL * n[d];
-    unR += uR * n[d];
+    uL[d] = UL[d + 1] * irL;
+    uR[d] = UR[d + 1] * irR;
+    u[d] = (sL * uL[d] + sR * uR[d]) * inv;
+    unL += uL[d] * n[d];
+    unR += uR[d] * n[d];
   }
-  const T HL = (UL[D + 1] + PL) / rL, HR = (UR[D + 1] + PR) / rR;
+  const T HL = (UL[D + 1] + PL) * irL, HR = (UR[D + 1] + PR) * irR;
   const T H = (sL * HL + sR * HR) * inv;
   T q2 = T(0), un = T(0);
 #pragma unroll
@@ -295,33 +299,29 @@ ZB_HD void roe(const T SL[D + 2], const T SR[D + 2], const T n[D], T Fc[D + 2],
   T a2 = (g - T(1)) * (H - T(0.5) * q2);
   a2 = dmax<T>(a2, T(1e-30));
   const T a = dsqrt<T>(a2);
+  const T ia2 = T(1) / a2;
   const T rho = sL * sR;
   const T dp = QR - QL, dr = SR[0] - SL[0], dun = unR - unL;
   // wave strengths
-  const T a1 = (dp - rho * a * dun) / (T(2) * a2);
-  const T a3 = (dp + rho * a * dun) / (T(2) * a2);
-  const T a2w = dr - dp / a2;
+  const T a1 = (dp - rho * a * dun) * (T(0.5) * ia2);
+  const T a3 = (dp + rho * a * dun) * (T(0.5) * ia2);
+  const T a2w = dr - dp * ia2;
   T l1 = dabs<T>(un - a), l2 = dabs<T>(un), l3 = dabs<T>(un + a);
   const T delta = T(0.1) * (dabs<T>(un) + a);
-  if (l1 < delta) l1 = (l1 * l1 + delta * delta) / (T(2) * delta);
-  if (l2 < delta) l2 = (l2 * l2 + delta * delta) / (T(2) * delta);
-  if (l3 < delta) l3 = (l3 * l3 + delta * delta) / (T(2) * delta);
+  const T i2d = T(0.5) / delta;
+  if (l1 < delta) l1 = (l1 * l1 + delta * delta) * i2d;
+  if (l2 < delta) l2 = (l2 * l2 + delta * delta) * i2d;
+  if (l3 < delta) l3 = (l3 * l3 + delta * delta) * i2d;
   // |A| dU = l1 a1 r1 + l2 (a2w r2 + rho dv_t) + l3 a3 r3
   T diss[D + 2];
   diss[0] = l1 * a1 + l2 * a2w + l3 * a3;
-#pragma unroll
-  for (int d = 0; d < D; d++)
-  {
-    const T uLd = UL[d + 1] / rL, uRd = UR[d + 1] / rR;
-    const T dvt = (uRd - uLd) - dun * n[d];
-    diss[d + 1] = l1 * a1 * (u[d] - a * n[d]) + l2 * (a2w * u[d] + rho * dvt) + l3 * a3 * (u[d] + a * n[d]);
-  }
   T udvt = T(0);
 #pragma unroll
   for (int d = 0; d < D; d++)
   {
-    const T uLd = UL[d + 1] / rL, uRd = UR[d + 1] / rR;
-    udvt += u[d] * ((uRd - uLd) - dun * n[d]);
+    const T dvt = (uR[d] - uL[d]) - dun * n[d];
+    diss[d + 1] = l1 * a1 * (u[d] - a * n[d]) + l2 * (a2w * u[d] + rho * dvt) + l3 * a3 * (u[d] + a * n[d]);
+    udvt += u[d] * dvt;
   }
   diss[D + 1] = l1 * a1 * (H - a * un) + l2 * (a2w * T(0.5) * q2 + rho * udvt) + l3 * a3 * (H + a * un);
 #pragma unroll
