@@ -312,15 +312,33 @@ def batched_side(steps: int = 5, ncases: int = 512, seed: int = 4):
     for c in cases:
         c.synchronize()
     ms_single = (time.perf_counter() - t0) * 1e3 / steps
+    # the same launches serialised on one stream (a host loop over cases)
+    import torch
+    shared = torch.cuda.Stream()
+    for c in cases:
+        c.set_stream(shared.cuda_stream)
+    for c in cases:
+        c.step(1)
+    shared.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for c in cases:
+            c.step(1)
+    shared.synchronize()
+    ms_serial = (time.perf_counter() - t0) * 1e3 / steps
     res_per_step = 4  # RK44 stages, one residual each
     out = {"workload": "batched_vortex_512_quads_n8-96_P1-5_euler", "cases": ncases, "dof": dof,
            "setup_s": setup_s, "autotuned": cfg,
            "batched": {"gdof_s": dof * res_per_step / (ms_batch * 1e-3) / 1e9, "ms_per_step": ms_batch,
                        "launches_per_step": 4},
            "one_launch_per_case": {"gdof_s": dof * res_per_step / (ms_single * 1e-3) / 1e9,
-                                   "ms_per_step": ms_single, "launches_per_step": 4 * ncases},
+                                   "ms_per_step": ms_single, "launches_per_step": 4 * ncases,
+                                   "streams": "one per case (concurrent)"},
+           "one_launch_per_case_one_stream": {"gdof_s": dof * res_per_step / (ms_serial * 1e-3) / 1e9,
+                                              "ms_per_step": ms_serial, "launches_per_step": 4 * ncases},
            "timing": "host clock around synchronised steps (both paths), 4 residuals per RK44 step"}
     out["batched_over_single"] = ms_single / ms_batch
+    out["batched_over_single_one_stream"] = ms_serial / ms_batch
     bt.close()
     for c in cases:
         c.close()

@@ -37,7 +37,7 @@ def test_batch_matches_cases_stepped_alone(precision, graph):
         assert _same(s1.get_state(), s2.get_state(), precision)
 
 
-@pytest.mark.parametrize("shape", [(256, 256), (128, 64), (64, 64)])
+@pytest.mark.parametrize("shape", [(256, 256, 1), (128, 64, 1), (64, 64, 1), (256, 64, 8), (128, 128, 32)])
 def test_batch_launch_shapes_agree(shape):
     """Whole-CTA tiles (one group) and several tile groups per CTA (named
     barriers) compute the same stages."""
@@ -45,7 +45,7 @@ def test_batch_launch_shapes_agree(shape):
     for s in alone:
         s.step(2)
     bt = zbatch.Batch(batched)
-    bt.set_config(threads=shape[0], blocks_per_sm=3, order=0, group=shape[1])
+    bt.set_config(threads=shape[0], blocks_per_sm=3, order=0, group=shape[1], chunk=shape[2])
     bt.step(2)
     bt.synchronize()
     for s1, s2 in zip(alone, batched):

@@ -47,7 +47,7 @@ constexpr size_t batch_desc_bytes()
 template <typename T, typename A>
 __global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__restrict__ cases,
                                                      const int2 *__restrict__ items, int nitems, int gsz,
-                                                     int gstride)
+                                                     int gstride, int chunk)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ng = blockDim.x / gsz, g = threadIdx.x / gsz, tid = threadIdx.x % gsz;
@@ -56,26 +56,37 @@ __global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__re
   BatchCase<T, A> *sbc = reinterpret_cast<BatchCase<T, A> *>(gbase);
   unsigned char *tsm = gbase + batch_desc_bytes<T, A>();
   constexpr int nwords = (int)(sizeof(BatchCase<T, A>) / sizeof(int));
-  for (int it = blockIdx.x * ng + g; it < nitems; it += gridDim.x * ng)
+  const int gid = blockIdx.x * ng + g, ngroups = gridDim.x * ng;
+  int have = -1;  // case whose descriptor the group holds
+  // a group takes chunks of `chunk` consecutive items; consecutive items of
+  // one case reuse the shared descriptor
+  for (int c0 = gid * chunk; c0 < nitems; c0 += ngroups * chunk)
   {
-    const int2 w = items[it];
-    // the descriptor is read throughout the tile: keep a shared copy
-    const int *src = reinterpret_cast<const int *>(&cases[w.x]);
-    int *dst = reinterpret_cast<int *>(sbc);
-    for (int k = tid; k < nwords; k += gsz) dst[k] = src[k];
-    dev::group_sync(bar, gsz);
-    switch (sbc->N)
+    const int c1 = min(c0 + chunk, nitems);
+    for (int it = c0; it < c1; it++)
     {
+      const int2 w = items[it];
+      if (w.x != have)
+      {
+        dev::group_sync(bar, gsz);  // the previous tile is done with the old descriptor
+        const int *src = reinterpret_cast<const int *>(&cases[w.x]);
+        int *dst = reinterpret_cast<int *>(sbc);
+        for (int k = tid; k < nwords; k += gsz) dst[k] = src[k];
+        have = w.x;
+      }
+      dev::group_sync(bar, gsz);
+      switch (sbc->N)
+      {
 #define ZB_BATCH_N(NN)                                                                                            \
   case NN:                                                                                                        \
     dev::euler_tile<T, A, 2, NN>(sbc->a, *reinterpret_cast<const LineOpsT<A, NN> *>(sbc->ops), w.y, tsm, tid, gsz, \
                                  bar);                                                                            \
     break;
-      ZB_BATCH_N(2) ZB_BATCH_N(3) ZB_BATCH_N(4) ZB_BATCH_N(5) ZB_BATCH_N(6)
+        ZB_BATCH_N(2) ZB_BATCH_N(3) ZB_BATCH_N(4) ZB_BATCH_N(5) ZB_BATCH_N(6)
 #undef ZB_BATCH_N
-      default: break;
+        default: break;
+      }
     }
-    dev::group_sync(bar, gsz);
   }
 }
 
@@ -104,7 +115,7 @@ struct Batch
   size_t smem = 0;     // tile arrays of one group (largest order)
   size_t gstride = 0;  // one group's shared memory: descriptor + tile arrays
   int sms = 148;
-  zb_batch_config cfg{256, 4, 0, 0.0, 64};
+  zb_batch_config cfg{256, 4, 0, 0.0, 64, 1};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int64_t launches = 0;
@@ -187,9 +198,10 @@ template <typename T, typename A>
 static void launch_stage_t(Batch &b, unsigned st)
 {
   const int ng = b.cfg.threads / b.cfg.group;
-  const int blocks = std::max(1, std::min((b.nitems + ng - 1) / ng, b.cfg.blocks_per_sm * b.sms));
+  const int blocks = std::max(1, std::min((b.nitems + ng * b.cfg.chunk - 1) / (ng * b.cfg.chunk),
+                                          b.cfg.blocks_per_sm * b.sms));
   k_batch_euler<T, A><<<blocks, b.cfg.threads, ng * b.gstride, b.stream>>>(
-      (const BatchCase<T, A> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride);
+      (const BatchCase<T, A> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride, b.cfg.chunk);
   b.launches++;
   CK(cudaGetLastError());
 }
@@ -217,13 +229,16 @@ static void build_graph(Batch &b)
   for (unsigned st = 0; st < 4; st++)
   {
     const int ng = b.cfg.threads / b.cfg.group;
-    const int blocks = std::max(1, std::min((b.nitems + ng - 1) / ng, b.cfg.blocks_per_sm * b.sms));
+    const int blocks = std::max(1, std::min((b.nitems + ng * b.cfg.chunk - 1) / (ng * b.cfg.chunk),
+                                            b.cfg.blocks_per_sm * b.sms));
     if (b.prec == ZB_FP64)
       k_batch_euler<double, double><<<blocks, b.cfg.threads, ng * b.gstride, b.stream>>>(
-          (const BatchCase<double, double> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride);
+          (const BatchCase<double, double> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride,
+          b.cfg.chunk);
     else
       k_batch_euler<float, float><<<blocks, b.cfg.threads, ng * b.gstride, b.stream>>>(
-          (const BatchCase<float, float> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride);
+          (const BatchCase<float, float> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride,
+          b.cfg.chunk);
   }
   cudaError_t e = cudaStreamEndCapture(b.stream, &b.graph);
   if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -364,17 +379,20 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
   const int shapes[][2] = {{64, 64}, {128, 64}, {128, 128}, {256, 64}, {256, 128}, {256, 256}};
   const int bps[] = {2, 4, 8, 16};
   const int orders[] = {0, 1};
-  zb_batch_config best{0, 0, 0, 1e300, 0};
+  const int chunks[] = {1, 8, 32};
+  zb_batch_config best{0, 0, 0, 1e300, 0, 1};
   for (int order : orders)
   {
     build_items(*b, order);
     for (const auto &sh : shapes)
       for (int bp : bps)
+        for (int ch : chunks)
       {
         b->cfg.threads = sh[0];
         b->cfg.group = sh[1];
         b->cfg.blocks_per_sm = bp;
         b->cfg.order = order;
+        b->cfg.chunk = ch;
         build_graph(*b);
         CK(cudaGraphLaunch(b->exec, b->stream));  // warm-up
         CK(cudaEventRecord(e0, b->stream));
@@ -384,7 +402,7 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e0, e1));
         const double per = ms / steps;
-        if (per < best.ms_per_step) best = zb_batch_config{sh[0], bp, order, per, sh[1]};
+        if (per < best.ms_per_step) best = zb_batch_config{sh[0], bp, order, per, sh[1], ch};
       }
   }
   cudaEventDestroy(e0);
@@ -418,6 +436,7 @@ void batch_config(Batch *b, const zb_batch_config *cfg)
     ZB_THROW(ZB_ERR_ARG, "group must be a multiple of 32, at least 64, dividing threads");
   if (cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 64) ZB_THROW(ZB_ERR_ARG, "blocks_per_sm out of range");
   if (cfg->order != 0 && cfg->order != 1) ZB_THROW(ZB_ERR_ARG, "order must be 0 or 1");
+  if (cfg->chunk < 1) ZB_THROW(ZB_ERR_ARG, "chunk must be at least 1");
   CK(cudaStreamSynchronize(b->stream));
   b->cfg = *cfg;
   build_items(*b, cfg->order);
