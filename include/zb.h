@@ -255,6 +255,15 @@ zb_status zb_vjp_geometry(zb_ctx *ctx, const double *lam, double *Ubar, int64_t 
                           int64_t ele_stride, int where, double *param_bar, double *inv_jaco_bar,
                           double *jaco_det_bar, double *norm_bar, double *dA_bar);
 
+/* zb_vjp that also adds the geometry adjoint to sums kept on the device
+ * (for unsteady adjoints, one call per RK stage without host copies);
+ * zb_geometry_adjoint_get copies the sums out in the zb_vjp_geometry layouts
+ * and, with reset != 0, clears them.  No reference counterpart. */
+zb_status zb_vjp_geometry_accumulate(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride,
+                                     int64_t var_stride, int64_t ele_stride, int where, double *param_bar);
+zb_status zb_geometry_adjoint_get(zb_ctx *ctx, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar,
+                                  double *dA_bar, int reset);
+
 /* ---- Batched stepping of independent cases ----
  * Many Euler cases on quadrilaterals (each its own context: mesh, order
  * P1-P5, state, dt) advance together: one persistent launch per RK stage

@@ -34,6 +34,7 @@ EXPORTED = [
     "zb_compute_residual", "zb_get_residual", "zb_rk_stage", "zb_step", "zb_residual_norms",
     "zb_synchronize", "zb_launch_count", "zb_profile_enable", "zb_profile_read", "zb_kernel_name",
     "zb_compute_residual_noalloc", "zb_functionals", "zb_vjp", "zb_set_freestream", "zb_wall_force", "zb_vjp_geometry",
+    "zb_vjp_geometry_accumulate", "zb_geometry_adjoint_get",
     "zb_batch_create", "zb_batch_destroy", "zb_batch_autotune", "zb_batch_set_config", "zb_batch_step",
     "zb_batch_stage", "zb_batch_synchronize", "zb_batch_launch_count",
 ]
@@ -148,6 +149,8 @@ def lib() -> ctypes.CDLL:
         L.zb_batch_launch_count.restype = i64
         L.zb_set_freestream.argtypes = [vp, ctypes.c_double, dp, ctypes.c_double]
         L.zb_vjp.argtypes = [vp, dp, dp, i64, i64, i64, ctypes.c_int, dp]
+        L.zb_vjp_geometry_accumulate.argtypes = [vp, dp, dp, i64, i64, i64, ctypes.c_int, dp]
+        L.zb_geometry_adjoint_get.argtypes = [vp, dp, dp, dp, dp, ctypes.c_int]
         L.zb_vjp_geometry.argtypes = [vp, dp, dp, i64, i64, i64, ctypes.c_int, dp, dp, dp, dp, dp]
         _lib = L
     return _lib

@@ -104,11 +104,10 @@ class TrajectoryAdjoint:
             g, p = self.s.vjp(lam.contiguous(), params=True)
             pbar += p
             return g
-        g, p, geo = self.s.vjp_geometry(lam.detach().cpu().numpy())
+        # geometry adjoint summed on the device by the library
+        g, p = self.s.vjp_geometry_accumulate(lam)
         pbar += p
-        for k in gbar:
-            gbar[k] += geo[k]
-        return torch.from_numpy(g).to(U.device)
+        return g
 
     def _step_adjoint(self, U0: torch.Tensor, Ubar_new: torch.Tensor, pbar: np.ndarray, gbar=None) -> torch.Tensor:
         Us, _, Rs = self._stages(U0, with_residuals=True)
@@ -121,12 +120,11 @@ class TrajectoryAdjoint:
             Rbar[s - 1] = Rbar[s - 1] - RK_ALPHA[s - 1] * self.dt * self.inv_det * Ubar_s
             if gbar is not None:
                 # U^(s) = U0 - a dt R_{s-1} / |J|
-                gbar["jaco_det"] += (RK_ALPHA[s - 1] * self.dt * (Ubar_s * Rs[s - 1]).sum(dim=1) *
-                                     inv2).cpu().numpy()
+                gbar["jaco_det"] += RK_ALPHA[s - 1] * self.dt * (Ubar_s * Rs[s - 1]).sum(dim=1) * inv2
         Ubar0 += self._vjp(Us[0], Rbar[0], pbar, gbar)
         if gbar is not None:
             Rsum = sum(RK_BETA[s] * Rs[s] for s in range(4))
-            gbar["jaco_det"] += (self.dt * (Ubar_new * Rsum).sum(dim=1) * inv2).cpu().numpy()
+            gbar["jaco_det"] += self.dt * (Ubar_new * Rsum).sum(dim=1) * inv2
         return Ubar0
 
     @staticmethod
@@ -139,7 +137,7 @@ class TrajectoryAdjoint:
         leaves = {k: v.detach().clone().requires_grad_(True) for k, v in geo.items()}
         j = objective(x, leaves)
         grads = torch.autograd.grad(j, [x] + list(leaves.values()))
-        return float(j.detach()), grads[0], {k: gk.cpu().numpy() for k, gk in zip(leaves, grads[1:])}
+        return float(j.detach()), grads[0], dict(zip(leaves, grads[1:]))
 
     def run(self, U0, nsteps: int, objective: Callable, geometry=None) -> Dict[str, object]:
         """Returns J, dJ/dU0 (CUDA tensor) and dJ/d(rho_fs, V_fs[0..2], P_fs).
@@ -165,7 +163,8 @@ class TrajectoryAdjoint:
         pbar = np.zeros(5)
         gbar = None
         if geometry is not None:
-            gbar = {k: np.zeros(tuple(v.shape)) for k, v in geometry.items()}
+            # the objective's and the RK update's parts, on the device
+            gbar = {k: torch.zeros_like(v) for k, v in geometry.items()}
         starts = [k for k in sorted(checkpoints) if k < nsteps]
         for i in range(len(starts) - 1, -1, -1):
             k0 = starts[i]
@@ -187,7 +186,8 @@ class TrajectoryAdjoint:
                 Ubar = self._step_adjoint(states[m], Ubar, pbar, gbar)
         out = {"J": J, "dJ_dU0": Ubar, "dJ_dfreestream": pbar}
         if gbar is not None:
-            out["dJ_dgeometry"] = gbar
+            lib_part = self.s.geometry_adjoint(reset=True)
+            out["dJ_dgeometry"] = {k: gbar[k].cpu().numpy() + lib_part[k] for k in gbar}
         return out
 
 

@@ -435,6 +435,26 @@ zb_status zb_vjp_geometry(zb_ctx *ctx, const double *lam, double *Ubar, int64_t 
   })
 }
 
+zb_status zb_vjp_geometry_accumulate(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride,
+                                     int64_t var_stride, int64_t ele_stride, int where, double *param_bar)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && lam && Ubar, "null argument");
+    ZB_REQUIRE(where == ZB_HOST || where == ZB_DEVICE, "where must be ZB_HOST or ZB_DEVICE");
+    zb::ctx_vjp(ctx->impl, lam, Ubar, spt_stride, var_stride, ele_stride, where, param_bar, nullptr, nullptr, nullptr,
+                nullptr, true);
+  })
+}
+
+zb_status zb_geometry_adjoint_get(zb_ctx *ctx, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar,
+                                  double *dA_bar, int reset)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && inv_jaco_bar && jaco_det_bar && norm_bar && dA_bar, "null argument");
+    zb::ctx_geometry_adjoint_get(ctx->impl, inv_jaco_bar, jaco_det_bar, norm_bar, dA_bar, reset);
+  })
+}
+
 zb_status zb_synchronize(zb_ctx *ctx)
 {
   ZB_GUARD({

@@ -501,7 +501,7 @@ static void free_all(Ctx *c)
   void *bufs[] = {c->U, c->U_ini, c->divF[0], c->divF[1], c->divF[2], c->divF[3], c->divF_vol, c->Ufp[0],
                   c->Ufp[1], c->Fvn, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
                   c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubar, c->pbar, c->dops, c->dwall,
-                  c->mbar, c->gbar, c->nbx};
+                  c->mbar, c->gbar, c->nbx, c->mbar_acc, c->gbar_acc};
   for (void *b : bufs)
     if (b) cudaFree(b);
   for (auto &r : c->recs)
@@ -926,12 +926,64 @@ void ctx_functionals(Ctx *c, double *out)
   out[2] = h[2];
 }
 
-void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, int64_t es, int where,
-             double *param_bar, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar, double *dA_bar)
+// acc[i] += x[i]
+__global__ void k_accumulate(double *__restrict__ acc, const double *__restrict__ x, int64_t n)
 {
-  const bool geo = inv_jaco_bar || jaco_det_bar || norm_bar || dA_bar;
-  if (geo && !(inv_jaco_bar && jaco_det_bar && norm_bar && dA_bar))
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    acc[i] += x[i];
+}
+
+// tile-layout geometry adjoint -> the reference layouts of zb_plan_get
+static void geo_to_reference(Ctx *c, const double *dm, const double *dg, double *inv_jaco_bar, double *jaco_det_bar,
+                             double *norm_bar, double *dA_bar)
+{
+  const int S = c->S, Fp = c->Fp, D = c->D, NM = D * D + 1;
+  const int64_t E = c->plan.neles;
+  std::vector<double> hm((size_t)c->ntiles * S * NM * TW), hg((size_t)c->ntiles * Fp * (D + 1) * TW);
+  CK(cudaMemcpyAsync(hm.data(), dm, hm.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(hg.data(), dg, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int64_t e = 0; e < E; e++)
+  {
+    const int64_t t = e / TW;
+    const int l = (int)(e % TW);
+    for (int sp = 0; sp < S; sp++)
+    {
+      for (int d1 = 0; d1 < D; d1++)
+        for (int d2 = 0; d2 < D; d2++)
+          inv_jaco_bar[(((size_t)d1 * S + sp) * D + d2) * E + e] = hm[(((size_t)t * S + sp) * NM + d1 * D + d2) * TW + l];
+      jaco_det_bar[(size_t)sp * E + e] = hm[(((size_t)t * S + sp) * NM + D * D) * TW + l];
+    }
+    for (int f = 0; f < Fp; f++)
+    {
+      for (int d = 0; d < D; d++)
+        norm_bar[((size_t)f * D + d) * E + e] = hg[(((size_t)t * Fp + f) * (D + 1) + d) * TW + l];
+      dA_bar[(size_t)f * E + e] = hg[(((size_t)t * Fp + f) * (D + 1) + D) * TW + l];
+    }
+  }
+}
+
+void ctx_geometry_adjoint_get(Ctx *c, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar, double *dA_bar,
+                              int reset)
+{
+  if (!c->mbar_acc) ZB_THROW(ZB_ERR_ARG, "no geometry adjoint has been accumulated");
+  geo_to_reference(c, c->mbar_acc, c->gbar_acc, inv_jaco_bar, jaco_det_bar, norm_bar, dA_bar);
+  if (reset)
+  {
+    const int NM = c->D * c->D + 1;
+    CK(cudaMemsetAsync(c->mbar_acc, 0, (size_t)c->ntiles * c->S * NM * TW * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->gbar_acc, 0, (size_t)c->ntiles * c->Fp * (c->D + 1) * TW * sizeof(double), c->stream));
+  }
+}
+
+void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, int64_t es, int where,
+             double *param_bar, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar, double *dA_bar,
+             bool accumulate)
+{
+  const bool geo_out = inv_jaco_bar || jaco_det_bar || norm_bar || dA_bar;
+  if (geo_out && !(inv_jaco_bar && jaco_det_bar && norm_bar && dA_bar))
     ZB_THROW(ZB_ERR_ARG, "the geometry adjoint needs all four output arrays");
+  const bool geo = geo_out || accumulate;
   if (c->prec != ZB_FP64) ZB_THROW(ZB_ERR_UNSUPPORTED, "the adjoint is built for the plain FP64 form only");
   if (!c->launch_vjp)
     ZB_THROW(ZB_ERR_UNSUPPORTED, "no adjoint kernels for ndims=" + std::to_string(c->D) + " P=" + std::to_string(c->N - 1));
@@ -983,35 +1035,22 @@ void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, in
   }
   c->launch_vjp(*c, param_bar != nullptr, geo);
   from_tiles(c, c->Ubar, nullptr, nullptr, Ubar, ss, vs, es, where);
-  if (geo)
+  if (accumulate)
   {
-    // tile layout -> the reference's inv_jaco_spts [D][S][D][E], jaco_det_spts
-    // [S][E], face norm [Fp][D][E] and dA [Fp][E] layouts
-    const int S = c->S, Fp = c->Fp, D = c->D;
-    const int64_t E = c->plan.neles;
-    std::vector<double> hm((size_t)c->ntiles * S * NM * TW), hg((size_t)c->ntiles * Fp * (D + 1) * TW);
-    CK(cudaMemcpyAsync(hm.data(), c->mbar, hm.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(hg.data(), c->gbar, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (int64_t e = 0; e < E; e++)
+    const size_t nm = (size_t)c->ntiles * c->S * NM * TW, ng = (size_t)c->ntiles * c->Fp * (c->D + 1) * TW;
+    if (!c->mbar_acc)
     {
-      const int64_t t = e / TW;
-      const int l = (int)(e % TW);
-      for (int sp = 0; sp < S; sp++)
-      {
-        for (int d1 = 0; d1 < D; d1++)
-          for (int d2 = 0; d2 < D; d2++)
-            inv_jaco_bar[(((size_t)d1 * S + sp) * D + d2) * E + e] = hm[(((size_t)t * S + sp) * NM + d1 * D + d2) * TW + l];
-        jaco_det_bar[(size_t)sp * E + e] = hm[(((size_t)t * S + sp) * NM + D * D) * TW + l];
-      }
-      for (int f = 0; f < Fp; f++)
-      {
-        for (int d = 0; d < D; d++)
-          norm_bar[((size_t)f * D + d) * E + e] = hg[(((size_t)t * Fp + f) * (D + 1) + d) * TW + l];
-        dA_bar[(size_t)f * E + e] = hg[(((size_t)t * Fp + f) * (D + 1) + D) * TW + l];
-      }
+      c->mbar_acc = (double *)dalloc(nm * sizeof(double));
+      c->gbar_acc = (double *)dalloc(ng * sizeof(double));
+      CK(cudaMemsetAsync(c->mbar_acc, 0, nm * sizeof(double), c->stream));
+      CK(cudaMemsetAsync(c->gbar_acc, 0, ng * sizeof(double), c->stream));
     }
+    k_accumulate<<<grid_for((int64_t)nm, 256), 256, 0, c->stream>>>(c->mbar_acc, c->mbar, (int64_t)nm);
+    k_accumulate<<<grid_for((int64_t)ng, 256), 256, 0, c->stream>>>(c->gbar_acc, c->gbar, (int64_t)ng);
+    c->launches += 2;
+    CK(cudaGetLastError());
   }
+  if (geo_out) geo_to_reference(c, c->mbar, c->gbar, inv_jaco_bar, jaco_det_bar, norm_bar, dA_bar);
   if (param_bar)
   {
     std::vector<double> h((size_t)c->ntiles * 5);

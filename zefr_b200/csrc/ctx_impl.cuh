@@ -79,6 +79,7 @@ struct Ctx
   double *lam = nullptr, *Lfp = nullptr, *Ubfp = nullptr, *dUbfp = nullptr, *UCb = nullptr, *Ubar = nullptr;
   double *pbar = nullptr;
   double *mbar = nullptr, *gbar = nullptr, *nbx = nullptr;  // geometry adjoint
+  double *mbar_acc = nullptr, *gbar_acc = nullptr;          // its device-side sums
   void (*launch_extrap)(Ctx &) = nullptr;
   void (*launch_stage)(Ctx &, const StageCfg &) = nullptr;
   void (*launch_vjp)(Ctx &, bool, bool) = nullptr;

@@ -317,6 +317,33 @@ class FRSolver:
                                     g["dA"].ctypes.data_as(_DP)))
         return out, pbar, g
 
+    def vjp_geometry_accumulate(self, lam):
+        """``vjp(lam, params=True)`` on a CUDA tensor that also adds the
+        geometry adjoint to device-side sums (read with
+        :meth:`geometry_adjoint`)."""
+        import torch
+        lam = lam.to(torch.float64).contiguous()
+        assert tuple(lam.shape) == self.state_shape
+        out = torch.empty_like(lam)
+        pbar = np.zeros(5)
+        self._torch_ready()
+        check(lib().zb_vjp_geometry_accumulate(self.h, ctypes.cast(lam.data_ptr(), _DP),
+                                               ctypes.cast(out.data_ptr(), _DP), *self._strides(), _lib.ZB_DEVICE,
+                                               pbar.ctypes.data_as(_DP)))
+        self.synchronize()
+        return out, pbar
+
+    def geometry_adjoint(self, reset: bool = True) -> Dict[str, np.ndarray]:
+        """The summed geometry adjoint of vjp_geometry_accumulate (host arrays)."""
+        S, V, E = self.state_shape
+        D, Fp = self.ndims, self.info.nfpts
+        g = {"inv_jaco": np.zeros((D, S, D, E)), "jaco_det": np.zeros((S, E)), "norm": np.zeros((Fp, D, E)),
+             "dA": np.zeros((Fp, E))}
+        check(lib().zb_geometry_adjoint_get(self.h, g["inv_jaco"].ctypes.data_as(_DP),
+                                            g["jaco_det"].ctypes.data_as(_DP), g["norm"].ctypes.data_as(_DP),
+                                            g["dA"].ctypes.data_as(_DP), 1 if reset else 0))
+        return g
+
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().zb_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
 
