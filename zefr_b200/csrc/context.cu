@@ -349,11 +349,12 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
     }
     else
     {
+      constexpr int ZG = dev::HexNsShape<A, N>::grad_zs, ZF = dev::HexNsShape<A, N>::face_zs;
       const size_t smem1 = (size_t)(S * V + Fp * V + 3 * S * V) * TW * sizeof(A);
       set_smem(dev::k_hex_ns_grad<T, A, N>, smem1);
       {
         ProfScope ps(c, ZB_K_NS_GRAD);
-        dev::k_hex_ns_grad<T, A, N><<<(unsigned)c.ntiles, HT, smem1, c.stream>>>(a, ops);
+        dev::k_hex_ns_grad<T, A, N><<<(unsigned)c.ntiles, HT * ZG, smem1, c.stream>>>(a, ops);
         c.launches++;
         CK(cudaGetLastError());
       }
@@ -361,7 +362,7 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
       const size_t smem2 = (size_t)(Fp * V + S * V) * TW * sizeof(A);
       set_smem(dev::k_hex_ns_face<T, A, N>, smem2);
       ProfScope ps(c, ZB_K_NS_FACE);
-      dev::k_hex_ns_face<T, A, N><<<(unsigned)c.ntiles, HT, smem2, c.stream>>>(a, ops);
+      dev::k_hex_ns_face<T, A, N><<<(unsigned)c.ntiles, HT * ZF, smem2, c.stream>>>(a, ops);
       c.launches++;
       CK(cudaGetLastError());
     }

@@ -131,15 +131,17 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_extrap(const T *__restrict__
 // common convective (+LDG) flux at the thread's six flux points, dA-scaled and
 // signed for this element, into sFc [Fp][V][TW]
 // ---------------------------------------------------------------------------
-template <typename T, typename A, int N, bool VISC>
-__device__ __forceinline__ void hex_common_flux(const Args<T, A> &a, int64_t tile, int l, int ix, int iy, A *sFc)
+template <typename T, typename A, int N, bool VISC, int ZS = 1>
+__device__ __forceinline__ void hex_common_flux(const Args<T, A> &a, int64_t tile, int l, int ix, int iy, A *sFc,
+                                                int zs = 0)
 {
   using H = HexIdx<N>;
   constexpr int V = 5;
   const A beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
 #pragma unroll 1
-  for (int q = 0; q < 6; q++)
+  for (int k = 0; k < 6 / ZS; k++)
   {
+    const int q = zs + ZS * k;  // ZS = 2: the thread of half zs takes faces of one side
     const int fq = H::fpt(q, ix, iy);
     A n[3], dA;
     int code;
@@ -289,16 +291,17 @@ __device__ __forceinline__ void hex_finish(const Args<T, A> &a, int64_t tile, in
   }
 }
 
-template <typename T, typename A, int N>
+template <typename T, typename A, int N, int ZS = 1>
 __device__ __forceinline__ void hex_extrap_next(const Args<T, A> &a, int64_t tile, int l, int ix, int iy, const int f[6],
-                                                const A *sUnew, const LineOpsT<A, N> &o)
+                                                const A *sUnew, const LineOpsT<A, N> &o, int zs = 0)
 {
   using H = HexIdx<N>;
   constexpr int V = 5;
 #pragma unroll
-  for (int q = 0; q < 6; q++)
+  for (int k = 0; k < 6 / ZS; k++)
   {
-    T *out = a.Ufp_next + (tile * H::Fp + f[q]) * (int64_t)V * TW + l;
+    const int q = zs + ZS * k;
+    T *out = a.Ufp_next + (tile * H::Fp + (ZS == 1 ? f[q] : H::fpt(q, ix, iy))) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++)
     {
@@ -392,20 +395,39 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_euler(const __grid_constant_
 }
 
 // ---------------------------------------------------------------------------
+// Launch shape of the Navier-Stokes kernels.  zs = 2 splits each (element,
+// x, y) column between two threads (z-levels and flux points by halves),
+// doubling the warps per CTA for the same shared memory; minb is the CTAs per
+// SM the register allocation is held to (0: the compiler's choice).  Chosen by
+// timing P3 on B200: the split pays for the gradient kernel in both
+// precisions and for the face kernel in FP64 only.
+// ---------------------------------------------------------------------------
+template <typename A, int N>
+struct HexNsShape
+{
+  static constexpr int grad_zs = (N % 2 == 0) ? 2 : 1;
+  static constexpr int grad_minb = grad_zs == 2 ? (sizeof(A) == 4 ? 4 : 2) : 0;
+  static constexpr int face_zs = (N % 2 == 0 && sizeof(A) == 8) ? 2 : 1;
+  static constexpr int face_minb = face_zs == 2 ? 2 : 0;
+};
+
+// ---------------------------------------------------------------------------
 // Navier-Stokes kernel 1 (column mapping): common solution, gradient, viscous
 // normal flux at own flux points, flux, volume divergence
 // ---------------------------------------------------------------------------
 template <typename T, typename A, int N>
-__global__ void __launch_bounds__(TW * N * N) k_hex_ns_grad(const __grid_constant__ Args<T, A> a,
-                                                          const __grid_constant__ LineOpsT<A, N> ops)
+__global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsShape<A, N>::grad_minb)
+    k_hex_ns_grad(const __grid_constant__ Args<T, A> a, const __grid_constant__ LineOpsT<A, N> ops)
 {
   using H = HexIdx<N>;
-  constexpr int S = H::S, Fp = H::Fp, V = 5;
+  constexpr int ZS = HexNsShape<A, N>::grad_zs;
+  constexpr int S = H::S, Fp = H::Fp, V = 5, NZ = N / ZS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sU = reinterpret_cast<A *>(smem_raw);   // [S][V][TW]
   A *sUC = sU + S * V * TW;                  // [Fp][V][TW] common solution
   A *sX = sUC + Fp * V * TW;                 // [3][S][V][TW] physical gradient, then F~
-  const int l = threadIdx.x % TW, c = threadIdx.x / TW, ix = c % N, iy = c / N;
+  const int l = threadIdx.x % TW, c = (threadIdx.x / TW) % H::N2, zs = threadIdx.x / (TW * H::N2);
+  const int ix = c % N, iy = c / N, iz0 = zs * NZ;
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
   RowOps<A, N> o;
@@ -413,24 +435,23 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_ns_grad(const __grid_constan
   int f[6];
   H::fpts(ix, iy, f);
   const A beta = a.ph.ldg_b;
-  // own column of the state -> registers and shared memory
-  A Uc[N][V];
+  // own part of the column of the state -> shared memory
   {
     const T *Ut = a.U + tile * (int64_t)S * V * TW;
 #pragma unroll
-    for (int iz = 0; iz < N; iz++)
+    for (int k = 0; k < NZ; k++)
 #pragma unroll
       for (int v = 0; v < V; v++)
       {
-        const int s = ix + N * iy + H::N2 * iz;
-        Uc[iz][v] = Ut[(s * V + v) * TW + l];
-        sU[(s * V + v) * TW + l] = Uc[iz][v];
+        const int s = ix + N * iy + H::N2 * (iz0 + k);
+        sU[(s * V + v) * TW + l] = Ut[(s * V + v) * TW + l];
       }
   }
   // common solution at own flux points (LDG, flip_beta = 1)
 #pragma unroll 1
-  for (int q = 0; q < 6; q++)
+  for (int kq = 0; kq < 6 / ZS; kq++)
   {
+    const int q = zs + ZS * kq;
     const int fq = H::fpt(q, ix, iy);
     A n[3], dA;
     int code;
@@ -471,7 +492,7 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_ns_grad(const __grid_constan
   // corrected reference gradient -> physical gradient
   const int fzm = H::fpt(0, ix, iy), fzp = H::fpt(1, ix, iy);
 #pragma unroll 1
-  for (int iz = 0; iz < N; iz++)
+  for (int iz = iz0; iz < iz0 + NZ; iz++)
   {
     const int s = ix + N * iy + H::N2 * iz;
     const int fxm = H::fxm(iy, iz), fxp = H::fxp(iy, iz), fym = H::fym(ix, iz), fyp = H::fyp(ix, iz);
@@ -501,7 +522,7 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_ns_grad(const __grid_constan
       {
         A acc = A(0);
 #pragma unroll
-        for (int m = 0; m < N; m++) acc += ops.Dm[iz * N + m] * Uc[m][v];
+        for (int m = 0; m < N; m++) acc += ops.Dm[iz * N + m] * sU[((ix + N * iy + H::N2 * m) * V + v) * TW + l];
         const A cm = ops.Dbm[iz] * sUC[(fzm * V + v) * TW + l];
         const A cp = ops.Dbp[iz] * sUC[(fzp * V + v) * TW + l];
         td[2] = acc + (cm + cp);
@@ -520,8 +541,9 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_ns_grad(const __grid_constan
   __syncthreads();
   // viscous normal flux at own flux points
 #pragma unroll 1
-  for (int q = 0; q < 6; q++)
+  for (int kq = 0; kq < 6 / ZS; kq++)
   {
+    const int q = zs + ZS * kq;
     const int fq = H::fpt(q, ix, iy);
     A n[3], dA;
     int code;
@@ -561,16 +583,19 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_ns_grad(const __grid_constan
   __syncthreads();
   // flux at own column, transformed F~ = adj F (overwrites the gradient in place)
 #pragma unroll 1
-  for (int iz = 0; iz < N; iz++)
+  for (int iz = iz0; iz < iz0 + NZ; iz++)
   {
     const int s = ix + N * iy + H::N2 * iz;
-    A dU[V][3], F[V][3], P, Pp, Ua[V], adj[3][3], det;
+    A dU[V][3], F[V][3], P, Pp, Us[V], Ua[V], adj[3][3], det;
 #pragma unroll
     for (int v = 0; v < V; v++)
+    {
+      Us[v] = sU[(s * V + v) * TW + l];
 #pragma unroll
       for (int d = 0; d < 3; d++) dU[v][d] = sX[((d * S + s) * V + v) * TW + l];
-    flux_conv_stored<A, 3>(Uc[iz], F, P, Pp, a.ph);
-    to_abs<A, 3>(Uc[iz], Ua, a.ph);
+    }
+    flux_conv_stored<A, 3>(Us, F, P, Pp, a.ph);
+    to_abs<A, 3>(Us, Ua, a.ph);
     flux_visc_add<A, 3>(Ua, dU, F, a.ph);
     load_adj<T, A>(a, tile, S, s, l, adj, det);
 #pragma unroll
@@ -587,7 +612,7 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_ns_grad(const __grid_constan
   __syncthreads();
   // volume divergence
 #pragma unroll 1
-  for (int iz = 0; iz < N; iz++)
+  for (int iz = iz0; iz < iz0 + NZ; iz++)
   {
     const int s = ix + N * iy + H::N2 * iz;
     A *out = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
@@ -611,25 +636,27 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_ns_grad(const __grid_constan
 // RK update, next-stage extrapolation
 // ---------------------------------------------------------------------------
 template <typename T, typename A, int N>
-__global__ void __launch_bounds__(TW * N * N) k_hex_ns_face(const __grid_constant__ Args<T, A> a,
-                                                          const __grid_constant__ LineOpsT<A, N> ops)
+__global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::face_zs, HexNsShape<A, N>::face_minb)
+    k_hex_ns_face(const __grid_constant__ Args<T, A> a, const __grid_constant__ LineOpsT<A, N> ops)
 {
   using H = HexIdx<N>;
-  constexpr int S = H::S, Fp = H::Fp, V = 5;
+  constexpr int ZS = HexNsShape<A, N>::face_zs;
+  constexpr int S = H::S, Fp = H::Fp, V = 5, NZ = N / ZS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sFc = reinterpret_cast<A *>(smem_raw);  // [Fp][V][TW]
   A *sUnew = sFc + Fp * V * TW;              // [S][V][TW]
-  const int l = threadIdx.x % TW, c = threadIdx.x / TW, ix = c % N, iy = c / N;
+  const int l = threadIdx.x % TW, c = (threadIdx.x / TW) % H::N2, zs = threadIdx.x / (TW * H::N2);
+  const int ix = c % N, iy = c / N;
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
   RowOps<A, N> o;
   o.load(ops, ix, iy);
   int f[6];
   H::fpts(ix, iy, f);
-  hex_common_flux<T, A, N, true>(a, tile, l, ix, iy, sFc);
+  hex_common_flux<T, A, N, true, ZS>(a, tile, l, ix, iy, sFc, zs);
   __syncthreads();
 #pragma unroll 1
-  for (int iz = 0; iz < N; iz++)
+  for (int iz = zs * NZ; iz < (zs + 1) * NZ; iz++)
   {
     const int s = ix + N * iy + H::N2 * iz;
     const A *dv = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
@@ -641,7 +668,7 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_ns_face(const __grid_constan
   if (a.extrap_next)
   {
     __syncthreads();
-    hex_extrap_next<T, A, N>(a, tile, l, ix, iy, f, sUnew, ops);
+    hex_extrap_next<T, A, N, ZS>(a, tile, l, ix, iy, f, sUnew, ops, zs);
   }
 }
 
