@@ -350,7 +350,7 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
     else
     {
       constexpr int ZG = dev::HexNsShape<A, N>::grad_zs, ZF = dev::HexNsShape<A, N>::face_zs;
-      const size_t smem1 = (size_t)(S * V + Fp * V + 3 * S * V) * TW * sizeof(A);
+      const size_t smem1 = (size_t)((S * V + Fp * V + 3 * S * V) * TW + 3 * N * TW) * sizeof(A);  // + sX padding
       set_smem(dev::k_hex_ns_grad<T, A, N>, smem1);
       {
         ProfScope ps(c, ZB_K_NS_GRAD);

@@ -426,6 +426,10 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
   A *sU = reinterpret_cast<A *>(smem_raw);   // [S][V][TW]
   A *sUC = sU + S * V * TW;                  // [Fp][V][TW] common solution
   A *sX = sUC + Fp * V * TW;                 // [3][S][V][TW] physical gradient, then F~
+  // sX is padded by TW words per z-level: the lanes of a warp differ in x, so
+  // along an x-line (viscous flux at x-faces) they read points N^2 apart,
+  // which would otherwise fall in one bank group
+  const auto xo = [](int p) { return p * V * TW + TW * (p / H::N2); };
   const int l = threadIdx.x % TW, c = (threadIdx.x / TW) % H::N2, zs = threadIdx.x / (TW * H::N2);
   const int ix = c % N, iy = c / N, iz0 = zs * NZ;
   const int64_t tile = blockIdx.x;
@@ -533,7 +537,7 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
         A g = td[0] * adj[0][d1];
         g += td[1] * adj[1][d1];
         g += td[2] * adj[2][d1];
-        sX[((d1 * S + s) * V + v) * TW + l] = g * inv_det;
+        sX[xo(d1 * S + s) + v * TW + l] = g * inv_det;
         if (a.dU_out) a.dU_out[(((tile * 3 + d1) * S + s) * V + v) * TW + l] = (T)(g * inv_det);
       }
     }
@@ -558,10 +562,10 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
 #pragma unroll
       for (int d = 0; d < 3; d++)
       {
-        A acc = (q_minus(q) ? ops.Em[0] : ops.Ep[0]) * sX[((d * S + H::line_spt(q, ix, iy, 0)) * V + v) * TW + l];
+        A acc = (q_minus(q) ? ops.Em[0] : ops.Ep[0]) * sX[xo(d * S + H::line_spt(q, ix, iy, 0)) + v * TW + l];
 #pragma unroll
         for (int m = 1; m < N; m++)
-          acc += (q_minus(q) ? ops.Em[m] : ops.Ep[m]) * sX[((d * S + H::line_spt(q, ix, iy, m)) * V + v) * TW + l];
+          acc += (q_minus(q) ? ops.Em[m] : ops.Ep[m]) * sX[xo(d * S + H::line_spt(q, ix, iy, m)) + v * TW + l];
         dUf[v][d] = acc;
       }
     }
@@ -592,7 +596,7 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
     {
       Us[v] = sU[(s * V + v) * TW + l];
 #pragma unroll
-      for (int d = 0; d < 3; d++) dU[v][d] = sX[((d * S + s) * V + v) * TW + l];
+      for (int d = 0; d < 3; d++) dU[v][d] = sX[xo(d * S + s) + v * TW + l];
     }
     flux_conv_stored<A, 3>(Us, F, P, Pp, a.ph);
     to_abs<A, 3>(Us, Ua, a.ph);
@@ -606,7 +610,7 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
         A t = F[v][0] * adj[d1][0];
         t += F[v][1] * adj[d1][1];
         t += F[v][2] * adj[d1][2];
-        sX[((d1 * S + s) * V + v) * TW + l] = t;
+        sX[xo(d1 * S + s) + v * TW + l] = t;
       }
   }
   __syncthreads();
@@ -621,11 +625,11 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
     {
       A vol = A(0);
 #pragma unroll
-      for (int m = 0; m < N; m++) vol += o.Dx[m] * sX[((0 * S + m + N * iy + H::N2 * iz) * V + v) * TW + l];
+      for (int m = 0; m < N; m++) vol += o.Dx[m] * sX[xo(0 * S + m + N * iy + H::N2 * iz) + v * TW + l];
 #pragma unroll
-      for (int m = 0; m < N; m++) vol += o.Dy[m] * sX[((1 * S + ix + N * m + H::N2 * iz) * V + v) * TW + l];
+      for (int m = 0; m < N; m++) vol += o.Dy[m] * sX[xo(1 * S + ix + N * m + H::N2 * iz) + v * TW + l];
 #pragma unroll
-      for (int m = 0; m < N; m++) vol += ops.Dm[iz * N + m] * sX[((2 * S + ix + N * iy + H::N2 * m) * V + v) * TW + l];
+      for (int m = 0; m < N; m++) vol += ops.Dm[iz * N + m] * sX[xo(2 * S + ix + N * iy + H::N2 * m) + v * TW + l];
       out[v * TW] = vol;
     }
   }
