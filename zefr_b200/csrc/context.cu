@@ -500,7 +500,7 @@ static void *dalloc(size_t bytes)
 static void free_all(Ctx *c)
 {
   void *bufs[] = {c->U, c->U_ini, c->divF[0], c->divF[1], c->divF[2], c->divF[3], c->divF_vol, c->Ufp[0],
-                  c->Ufp[1], c->Fvn, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
+                  c->Ufp[1], c->Fvn, c->Fcom, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
                   c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubar, c->pbar, c->dops, c->dwall,
                   c->mbar, c->gbar, c->nbx, c->mbar_acc, c->gbar_acc};
   for (void *b : bufs)
@@ -609,6 +609,7 @@ Ctx *ctx_create(const Plan &plan)
     {
       c->divF_vol = dalloc(nU * c->asz);
       c->Fvn = dalloc(nF * c->tsz);
+      if (c->D == 3) c->Fcom = dalloc(nF * c->tsz);  // hexahedra: one-sided common flux
     }
     if (c->prec != ZB_FP64) c->Ucomp = dalloc(nU * c->tsz);
     c->mets = dalloc((size_t)c->ntiles * c->S * (c->D * c->D + 1) * TW * c->tsz);

@@ -49,7 +49,8 @@ struct Ctx
   int D = 0, N = 0, S = 0, Fp = 0, V = 0, nstages = 4;
   int64_t ntiles = 0;
   void *U = nullptr, *U_ini = nullptr, *divF[4] = {nullptr, nullptr, nullptr, nullptr};
-  void *divF_vol = nullptr, *Ufp[2] = {nullptr, nullptr}, *Fvn = nullptr, *mets = nullptr, *fgeo = nullptr;
+  void *divF_vol = nullptr, *Ufp[2] = {nullptr, nullptr}, *Fvn = nullptr, *Fcom = nullptr, *mets = nullptr,
+       *fgeo = nullptr;
   void *Ucomp = nullptr;
   void *dops = nullptr;  // triangles: dense operators in the arithmetic type
   double *dwall = nullptr;  // wall force: FP64 oppE, face weights, flux point coordinates
@@ -208,6 +209,7 @@ static Args<T, A> make_args(Ctx &c, const StageCfg &sc)
   a.divF = (T *)c.divF[sc.stage];
   a.divF_vol = (A *)c.divF_vol;
   a.Fvn = (T *)c.Fvn;
+  if (c.Fcom && (c.plan.params.ldg_b == 0.5 || c.plan.params.ldg_b == -0.5)) a.Fcom = (T *)c.Fcom;
   a.rk_mode = sc.rk_mode;
   a.save_ini = sc.save_ini;
   a.extrap_next = sc.extrap_next;

@@ -56,6 +56,9 @@ struct Args
   A *divF_vol;       // NS: volume part of the residual (arithmetic type: it cancels
                      // against the surface part)
   T *Fvn;            // NS: viscous normal flux at own flux points
+  T *Fcom;           // NS hexahedra, LDG beta = +-1/2, optional: common flux (convective
+                     // + viscous, not dA-scaled) at the flux points whose side supplies
+                     // the LDG normal flux; the partner reads it from there
   T *dU_out;         // NS, optional: physical gradient [tile][D][S][V][TW] (the
                      // reference keeps it in dU_spts for diagnostics)
   // RK update fused into the last kernel of a stage

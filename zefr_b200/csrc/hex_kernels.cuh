@@ -84,6 +84,16 @@ struct RowOps
 // own flux point q (0..5): side of the face
 __device__ __forceinline__ bool q_minus(int q) { return (q & 1) == 0; }
 
+// k-th of the own flux points a thread handles when ZS threads share a column:
+// all six for ZS = 1; for ZS = 2 half 0 takes faces z-, x+, y- and half 1
+// takes z+, x-, y+, so the work done by only one side of a face (the LDG
+// normal flux, usually the side with the + face) is spread over both halves
+template <int ZS>
+__device__ __forceinline__ int own_face(int zs, int k)
+{
+  return ZS == 1 ? k : 2 * k + ((zs + k) & 1);
+}
+
 template <typename T, typename A, int N>
 __device__ __forceinline__ void load_face_geo(const Args<T, A> &a, int64_t tile, int f, int l, A n[3], A &dA, int &code)
 {
@@ -141,7 +151,7 @@ __device__ __forceinline__ void hex_common_flux(const Args<T, A> &a, int64_t til
 #pragma unroll 1
   for (int k = 0; k < 6 / ZS; k++)
   {
-    const int q = zs + ZS * k;  // ZS = 2: the thread of half zs takes faces of one side
+    const int q = own_face<ZS>(zs, k);
     const int fq = H::fpt(q, ix, iy);
     A n[3], dA;
     int code;
@@ -224,6 +234,39 @@ __device__ __forceinline__ void hex_common_flux(const Args<T, A> &a, int64_t til
   }
 }
 
+// common flux formed by the gradient kernel (Args::Fcom) at the thread's flux
+// points: read from this element where it supplied the LDG normal flux, else
+// from the partner's flux point; dA-scaled and signed for this element
+template <typename T, typename A, int N, int ZS = 1>
+__device__ __forceinline__ void hex_gather_common(const Args<T, A> &a, int64_t tile, int l, int ix, int iy, A *sFc,
+                                                  int zs = 0)
+{
+  using H = HexIdx<N>;
+  constexpr int V = 5;
+  const int supplier = a.ph.ldg_b == A(0.5) ? 0 : 1;  // slot whose normal flux LDG takes
+#pragma unroll 1
+  for (int k = 0; k < 6 / ZS; k++)
+  {
+    const int q = own_face<ZS>(zs, k);
+    const int fq = H::fpt(q, ix, iy);
+    const int64_t gi = (tile * H::Fp + fq) * (int64_t)TW + l;
+    const A dA = a.fgeo[(tile * H::Fp + fq) * (int64_t)4 * TW + 3 * TW + l];
+    const int code = a.nbr[gi];
+    A F[V];
+    if (code < 0 || (code & 1) == supplier)
+    {
+      const T *fc = a.Fcom + (tile * H::Fp + fq) * (int64_t)V * TW + l;
+#pragma unroll
+      for (int v = 0; v < V; v++) F[v] = fc[v * TW];
+    }
+    else
+      gather_fpt<T, A, V>(a.Fcom, code >> 1, F);
+    const bool right = (code >= 0) && (code & 1);
+#pragma unroll
+    for (int v = 0; v < V; v++) sFc[(fq * V + v) * TW + l] = right ? -F[v] * dA : F[v] * dA;
+  }
+}
+
 // surface correction for spt (ix, iy, iz) in flux-point order (faces 0..5)
 template <typename A, int N>
 __device__ __forceinline__ A hex_surface(const LineOpsT<A, N> &ops, const RowOps<A, N> &o, const A *sFc, int ix, int iy,
@@ -300,7 +343,7 @@ __device__ __forceinline__ void hex_extrap_next(const Args<T, A> &a, int64_t til
 #pragma unroll
   for (int k = 0; k < 6 / ZS; k++)
   {
-    const int q = zs + ZS * k;
+    const int q = own_face<ZS>(zs, k);
     T *out = a.Ufp_next + (tile * H::Fp + (ZS == 1 ? f[q] : H::fpt(q, ix, iy))) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++)
@@ -455,7 +498,7 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
 #pragma unroll 1
   for (int kq = 0; kq < 6 / ZS; kq++)
   {
-    const int q = zs + ZS * kq;
+    const int q = own_face<ZS>(zs, kq);
     const int fq = H::fpt(q, ix, iy);
     A n[3], dA;
     int code;
@@ -547,7 +590,7 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
 #pragma unroll 1
   for (int kq = 0; kq < 6 / ZS; kq++)
   {
-    const int q = zs + ZS * kq;
+    const int q = own_face<ZS>(zs, kq);
     const int fq = H::fpt(q, ix, iy);
     A n[3], dA;
     int code;
@@ -583,6 +626,30 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
     T *out = a.Fvn + (tile * Fp + fq) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++) out[v * TW] = Fn[v];
+    if (a.Fcom)
+    {
+      // this side supplies the LDG normal flux, so it forms the whole common
+      // flux of the point once for both elements (same terms as
+      // hex_common_flux with the partner's normal flux zero)
+      const A tau = a.ph.ldg_tau;
+      A Un[V], UL[V], UR[V], UB[V], Fc[V];
+      if (code >= 0) gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
+      conv_common<T, A, 3>(a, Uf, Un, code, n, UL, UR, UB, Fc);
+      T *fc = a.Fcom + (tile * Fp + fq) * (int64_t)V * TW + l;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+      {
+        A Fv;
+        if (code >= 0)
+        {
+          const A FnL = beta == A(0.5) ? Fn[v] : A(0), FnR = beta == A(0.5) ? A(0) : Fn[v];
+          Fv = A(0.5) * (FnL + FnR) + tau * (UL[v] - UR[v]) + beta * (FnL - FnR);
+        }
+        else
+          Fv = Fn[v] + tau * (UL[v] - UB[v]);
+        fc[v * TW] = Fc[v] + Fv;
+      }
+    }
   }
   __syncthreads();
   // flux at own column, transformed F~ = adj F (overwrites the gradient in place)
@@ -657,7 +724,10 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::face_zs, HexNsS
   o.load(ops, ix, iy);
   int f[6];
   H::fpts(ix, iy, f);
-  hex_common_flux<T, A, N, true, ZS>(a, tile, l, ix, iy, sFc, zs);
+  if (a.Fcom)
+    hex_gather_common<T, A, N, ZS>(a, tile, l, ix, iy, sFc, zs);
+  else
+    hex_common_flux<T, A, N, true, ZS>(a, tile, l, ix, iy, sFc, zs);
   __syncthreads();
 #pragma unroll 1
   for (int iz = zs * NZ; iz < (zs + 1) * NZ; iz++)
