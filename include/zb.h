@@ -211,8 +211,51 @@ zb_status zb_get_residual(zb_ctx *ctx, unsigned stage, double *out, int64_t spt_
  * stage s, then U = U_ini - a_s dt/|J| divF_s, or on the last stage
  * U = U_ini - sum_s b_s dt/|J| divF_s.  Stage 0 first saves U_ini. */
 zb_status zb_rk_stage(zb_ctx *ctx, unsigned stage);
-/* n full RK44 steps (FRSolver::update with dt_scheme RK44). */
+/* n time steps of FRSolver::update (src/solver.cpp:2600-2660): RK44
+ * (step_RK) by default, or the scheme set with zb_set_time_scheme. */
 zb_status zb_step(zb_ctx *ctx, int n);
+
+/* Time integration options of the reference deck (dt_scheme, dt_type, CFL,
+ * CFL_type, adapt_dt and its controller keys; src/input.cpp:72-127).
+ *  - scheme ZB_RK44: step_RK (src/solver.cpp:2864-3097); with dt_type != 0
+ *    the time step is the CFL estimate of compute_element_dt
+ *    (src/solver.cpp:4105-4272) from the state at the start of the step:
+ *    dt_type 1 the global minimum, 2 one step per element.
+ *  - scheme ZB_RK54: five-stage low-storage RK (step_LSRK, src/solver.cpp:
+ *    3100-3255; coefficients src/solver.cpp:749-777) at the fixed dt, or with
+ *    adapt_dt the embedded error estimate and PI controller of
+ *    step_adaptive (src/solver.cpp:2663-2757): max over points of
+ *    |err| / (atol + rtol max(|U|, |U_ini|)), factor
+ *    err^(-pi_alpha/4) prev_err^(pi_beta/4) clamped by safety, min_factor and
+ *    max_factor, dt capped at max_dt; a step whose error is >= 1 is redone from
+ *    its start state with the new dt.
+ * CFL_type 1: dt = 2 CFL c_adv(P) vol / sum_fpt w dA waveSp; CFL_type 2:
+ * per direction max over the face points of waveSp / (c_adv h) (+ diffCo /
+ * (c_diff h^2) for Navier-Stokes), dt = CFL / sum over directions.  waveSp is
+ * max(|Vn| + a) over the two sides of the point (the reference's Rusanov wave
+ * speed, also used with the Roe flux), diffCo max(mu/rho, gamma mu/(Pr rho)).
+ * Quadrilaterals and hexahedra; dt_type != 0 is refused for triangles. */
+enum { ZB_RK44 = 0, ZB_RK54 = 1 };
+typedef struct zb_time_scheme {
+  int scheme;         /* ZB_RK44 or ZB_RK54 */
+  int dt_type;        /* 0 fixed dt (zb_params.dt / zb_set_dt), 1 CFL global, 2 CFL local */
+  int cfl_type;       /* 1 or 2 */
+  double cfl;
+  int adapt_dt;       /* ZB_RK54 only */
+  double atol, rtol, pi_alpha, pi_beta, safety, max_factor, min_factor, max_dt;
+} zb_time_scheme;
+/* Deck defaults (src/input.cpp:72-127): RK44, dt_type 0, CFL 1, CFL_type 1,
+ * err_atol = err_rtol = 1e-5, pi_alpha 0.7, pi_beta 0.4, safety_factor 0.8,
+ * max_factor 2.5, min_factor 0.3, max_dt 100. */
+void zb_time_scheme_defaults(zb_time_scheme *out);
+zb_status zb_set_time_scheme(zb_ctx *ctx, const zb_time_scheme *ts);
+/* After zb_step: the reference's dt(0) -- the fixed step, the last CFL step
+ * (element 0's under dt_type 2) or, with adapt_dt, the step the next step
+ * starts from -- the last accepted error estimate, the number of rejected
+ * steps so far and the flow time (sum of the steps' dt(0)). */
+zb_status zb_time_state(zb_ctx *ctx, double *dt, double *prev_err, int64_t *rejected, double *flow_time);
+/* Per-element time step of the last CFL estimate (dt_type != 0), [n_eles]. */
+zb_status zb_get_element_dt(zb_ctx *ctx, double *out);
 
 /* Residual norms of report_residuals (src/solver.cpp:6990-7137), FP64 device
  * reduction of divF(stage 0)/|J| per variable: out[3*nvars] = L1, L2, Linf. */

@@ -547,3 +547,177 @@ def rk44_step(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, dt: 
     for s in range(4):
         Un = Un - beta[s] * dt / det * regs[s]
     return Un
+
+
+# ---------------------------------------------------------------------------
+# time integration: RK54 (step_LSRK + step_adaptive) and the CFL time step
+# (compute_element_dt); src/solver.cpp:749-777, 2663-2757, 3100-3255, 4105-4272
+# ---------------------------------------------------------------------------
+
+# Kennedy-Carpenter RK54 2N pair as tabulated in src/solver.cpp:749-777
+LSRK_A = [970286171893. / 4311952581923., 6584761158862. / 12103376702013.,
+          2251764453980. / 15575788980749., 26877169314380. / 34165994151039.]
+LSRK_B = [1153189308089. / 22510343858157., 1772645290293. / 4653164025191.,
+          -1672844663538. / 4480602732383., 2114624349019. / 3568978502595.,
+          5198255086312. / 14908931495163.]
+LSRK_BHAT = [1016888040809. / 7410784769900., 11231460423587. / 58533540763752.,
+             -1563879915014. / 6823010717585., 606302364029. / 971179775848.,
+             1097981568119. / 3980877426909.]
+# get_cfl_limit_adv / get_cfl_limit_diff (src/funcs.cpp:435-560), orders 0..10
+CFL_ADV = [1.392, 0.4642, 0.2351, 0.1453, 0.1000, 0.07363, 0.05678, 0.04530, 0.03709, 0.03101, 0.02635]
+CFL_DIFF_CENTRED = [2.785, 0.1740, 0.04264, 0.01580, 0.007193, 0.003730, 0.002120, 0.001292, 0.0008314,
+                    0.0005586, 0.0003890]
+CFL_DIFF_UPWIND = [0.6963, 0.07736, 0.01878, 0.006345, 0.002664, 0.001299, 0.0007060, 0.0004153, 0.0002599,
+                   0.0001708, 0.0001168]
+
+
+def lsrk_step(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, dt: float, adapt: bool = False):
+    """One RK54 step (FRSolver::step_LSRK, src/solver.cpp:3100-3255).
+
+    Returns (U_new, rk_err); rk_err is None unless ``adapt``."""
+    det = st.jaco_det[:, None, :]
+    U_til = U.copy()
+    Us = U.copy()
+    err = np.zeros_like(U) if adapt else None
+    for s in range(5):
+        r = residual(st, Us, p, viscous)
+        if adapt:
+            err = err - (LSRK_B[s] - LSRK_BHAT[s]) * dt / det * r
+        if s < 4:
+            Us = U_til - LSRK_A[s] * dt / det * r
+            U_til = Us - (LSRK_B[s] - LSRK_A[s]) * dt / det * r
+        else:
+            Us = U_til - LSRK_B[s] * dt / det * r
+    return Us, err
+
+
+def rk_error(U: np.ndarray, U_ini: np.ndarray, err: np.ndarray, atol: float, rtol: float) -> float:
+    """Infinity norm of the scaled RK error (src/solver.cpp:2671-2684); NaN counts as infinite."""
+    x = np.abs(err) / (atol + rtol * np.maximum(np.abs(U), np.abs(U_ini)))
+    x = np.where(np.isnan(x), np.inf, x)
+    return float(x.max())
+
+
+class AdaptiveRK54:
+    """step_adaptive (src/solver.cpp:2663-2757) around :func:`lsrk_step`."""
+
+    def __init__(self, dt: float, atol=1e-5, rtol=1e-5, pi_alpha=0.7, pi_beta=0.4, safety=0.8, max_factor=2.5,
+                 min_factor=0.3, max_dt=100.0):
+        self.dt, self.atol, self.rtol = dt, atol, rtol
+        self.expa, self.expb = pi_alpha / 4.0, pi_beta / 4.0
+        self.safety, self.max_factor, self.min_factor, self.max_dt = safety, max_factor, min_factor, max_dt
+        self.prev_err, self.rejected = 1.0, 0
+
+    def step(self, st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool) -> np.ndarray:
+        while True:
+            Un, err = lsrk_step(st, U, p, viscous, self.dt, adapt=True)
+            max_err = rk_error(Un, U, err, self.atol, self.rtol)
+            with np.errstate(divide="ignore"):
+                fac = max_err ** -self.expa * self.prev_err ** self.expb
+            fac = min(self.max_factor, max(self.min_factor, self.safety * fac))
+            self.dt = min(self.dt * fac, self.max_dt)
+            if self.dt < 1e-14:
+                raise RuntimeError("dt approaching 0")
+            if max_err < 1.0:
+                self.prev_err = max_err
+                return Un
+            self.rejected += 1
+
+
+def h_ref(coord_fpts: np.ndarray, loc_fpts: np.ndarray, nfpts_face: int) -> np.ndarray:
+    """Tensor-line lengths between paired flux points of opposite faces
+    (src/elements.cpp:408-483) from coord_fpts [Fp, D, E] and loc_fpts [Fp, D].
+
+    2D pairs point i of faces 0/1 with point N-1-i of faces 2/3; 3D sorts the
+    reference positions of each face of a pair (btm/top, left/right,
+    front/back) and pairs equal ranks, with the reference's length expression
+    sqrt(dx^2 + dy^2 * dz^2)."""
+    Fp, D, E = coord_fpts.shape
+    h = np.zeros((Fp, E))
+    if D == 2:
+        N = nfpts_face
+        for f1 in range(Fp // 2):
+            i = f1 % N
+            f2 = (f1 // N + 3) * N - i - 1
+            d = coord_fpts[f1] - coord_fpts[f2]
+            h[f1] = h[f2] = np.sqrt(d[0] * d[0] + d[1] * d[1])
+        return h
+    nf = nfpts_face
+
+    def order(idx):
+        pts = np.round(loc_fpts[idx], 10)
+        return [idx[k] for k in np.lexsort(pts.T[::-1])]
+
+    for f in range(3):
+        a = order(np.arange(2 * f * nf, (2 * f + 1) * nf))
+        b = order(np.arange((2 * f + 1) * nf, (2 * f + 2) * nf))
+        for f1, f2 in zip(a, b):
+            d = coord_fpts[f1] - coord_fpts[f2]
+            h[f1] = h[f2] = np.sqrt(d[0] * d[0] + d[1] * d[1] * d[2] * d[2])
+    return h
+
+
+def element_dt(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, order: int, cfl: float, cfl_type: int,
+               vol: np.ndarray, wfpts: np.ndarray, href: Optional[np.ndarray] = None) -> np.ndarray:
+    """Per-element CFL time step of compute_element_dt (src/solver.cpp:4105-4199)
+    with the face wave speed of the Rusanov flux (src/faces.cpp:1296-1316) and
+    the LDG diffusion coefficient (src/faces.cpp:1572-1577) at the state U."""
+    S, V, E = U.shape
+    D = st.ndims
+    Fp = st.oppE.shape[0]
+    nf = Fp // (2 * D)
+    g = p["gamma"]
+    Ufp = np.einsum("fs,sve->fve", st.oppE, U)
+    own = Ufp.transpose(1, 0, 2).reshape(V, Fp * E)
+    part = st.partner.reshape(-1)
+    interior = part >= 0
+    other = Ufp[np.where(interior, part % Fp, 0), :, np.where(interior, part // Fp, 0)].T
+    n = st.norm.transpose(1, 0, 2).reshape(D, Fp * E)
+    bc = np.where(interior, 0, -1 - part)
+    URg, UBg = _ghost(bc, own, n, p)
+    UR = np.where(interior, other, URg)
+    UB = np.where(interior, other, UBg)
+
+    def ws(Uq):
+        P = (g - 1.0) * (Uq[D + 1] - 0.5 * (Uq[1:D + 1] ** 2).sum(0) / Uq[0])
+        a = np.sqrt(g * P / Uq[0])
+        Vn = sum(Uq[d + 1] / Uq[0] * n[d] for d in range(D))
+        return np.abs(Vn) + a
+
+    wsp = np.maximum(ws(own), ws(UR)).reshape(Fp, E)
+    c_adv = CFL_ADV[order]
+    if cfl_type == 1:
+        w = np.array([wfpts[f % nf] for f in range(Fp)])
+        return 2.0 * cfl * c_adv * vol / (w[:, None] * wsp * st.dA).sum(0)
+    t = wsp / (c_adv * href)
+    if viscous:
+        c_diff = (CFL_DIFF_CENTRED if p["ldg_b"] == 0.0 else CFL_DIFF_UPWIND)[order]
+        mu, pr = p["mu"], p["prandtl"]
+
+        def dc(rho):
+            return np.maximum(mu / rho, g * mu / (pr * rho))
+
+        t = t + np.maximum(dc(own[0]), dc(UB[0])).reshape(Fp, E) / (c_diff * href * href)
+    dtinv = t.reshape(2 * D, nf, E).max(1)
+    if D == 2:
+        return cfl / (np.maximum(dtinv[0], dtinv[2]) + np.maximum(dtinv[1], dtinv[3]))
+    return cfl / (np.maximum(dtinv[0], dtinv[1]) + np.maximum(dtinv[2], dtinv[3]) + np.maximum(dtinv[4], dtinv[5]))
+
+
+def rk44_step_dt(st: Setup, U: np.ndarray, p: Dict[str, float], viscous: bool, dt) -> np.ndarray:
+    """RK44 step with a global (scalar) or per-element ([E]) time step."""
+    alpha = [0.5, 0.5, 1.0]
+    beta = [1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0]
+    dt = np.asarray(dt, dtype=np.float64)
+    U_ini = U.copy()
+    det = st.jaco_det[:, None, :]
+    regs, Us = [], U
+    for s in range(3):
+        r = residual(st, Us, p, viscous)
+        regs.append(r)
+        Us = U_ini - alpha[s] * dt / det * r
+    regs.append(residual(st, Us, p, viscous))
+    Un = U_ini.copy()
+    for s in range(4):
+        Un = Un - beta[s] * dt / det * regs[s]
+    return Un

@@ -258,6 +258,9 @@ long zr_get_array(void *p, const char *cname, double *out, long n)
   if (name == "P") return copy_out(f->P, out, n);
   if (name == "waveSp") return copy_out(f->waveSp, out, n);
   if (name == "diffCo") return copy_out(f->diffCo, out, n);
+  if (name == "dt") return copy_out(e->dt, out, n);
+  if (name == "vol") return copy_out(e->vol, out, n);
+  if (name == "h_ref") return copy_out(e->h_ref, out, n);
   if (name == "fpt2gfpt") return copy_out(geo.fpt2gfptBT[e->etype], out, n);
   if (name == "fpt2gfpt_slot") return copy_out(geo.fpt2gfpt_slotBT[e->etype], out, n);
   if (name == "gfpt2bnd")

@@ -9,7 +9,12 @@ synthetic meshes of every workload shape, with seeded states, and stores:
   U0, R0        input state and divF_spts(0) = reference compute_residual(0)
   Un            state after ``nsteps`` reference RK44 steps (FRSolver::update)
 
-Usage:  python tests/golden/make_golden.py  (needs oracle/_ref/libzefr_ref.so)
+and, under tests/golden/time/, time-integration cases (RK54 with and without
+the adaptive controller, RK44 with CFL time steps) holding the mesh, deck,
+U0, the reference's dt(0) after every step, its per-element dt array after
+the last step and the final state.
+
+Usage:  python tests/golden/make_golden.py [names]  (needs oracle/_ref/libzefr_ref.so)
 """
 from __future__ import annotations
 
@@ -176,14 +181,96 @@ def make_case(name, spec, tmp):
     return out
 
 
+# name -> (mesh builder, ndims, order, viscous, bounds, deck params incl. time keys, state builder, nsteps)
+def _time_cases():
+    cyl_deck = {"disable_nondim": 1, "fix_vis": 1, "mach_fs": 0.2, "Re_fs": 100, "prandtl": 0.72,
+                "P_fs": 1.0, "rho_fs": 1.0, "L_fs": 1.0, "ldg_b": 0.5, "ldg_tau": 0.1}
+    eul = {"mach_fs": 0.3, "rho_fs": 1.0, "P_fs": 1.0}
+
+    def vortex(X, g):
+        return ics.isentropic_vortex(X, beta=5.0, gamma=g)
+
+    def shear(X, g):
+        return ics.double_shear_layer(X * 0.1 + 0.5, mach=0.2, gamma=g)
+
+    def tgv(X, g):
+        return ics.taylor_green(X, mach=0.3, gamma=g)
+
+    def cyl_state(X, g):
+        c = 0.2 * np.sqrt(g)
+        return ics.uniform(X, 1.0, (c, 0.0), 1.0, g)
+
+    per = {"PERIODIC": "periodic"}
+    quads = lambda: meshgen.box_quads(6, 6)  # noqa: E731
+    jq = lambda: meshgen.jitter_interior(meshgen.box_quads(6, 5), 0.4, 11)  # noqa: E731
+    jh = lambda: meshgen.jitter_interior(meshgen.box_hexes(3, 3, 2), 0.15, 5)  # noqa: E731
+    return {
+        "rk54_quad_p3_vortex": (quads, 2, 3, False, per, dict(eul, dt=5e-3, dt_scheme="RK54"), vortex, 3),
+        # the first step is rejected (dt 0.2 is far too large) and redone
+        "rk54_adapt_quad_p3_vortex": (quads, 2, 3, False, per, dict(eul, dt=0.2, dt_scheme="RK54", adapt_dt=1),
+                                      vortex, 4),
+        "rk54_adapt_hex_p1_ns": (lambda: meshgen.box_hexes(3, 2, 2), 3, 1, True, per,
+                                 dict(cyl_deck, mach_fs=0.3, dt=1e-2, dt_scheme="RK54", adapt_dt=1,
+                                      err_atol=1e-6, err_rtol=1e-6), tgv, 3),
+        "cfl1_global_quad_p2_ns": (jq, 2, 2, True, per,
+                                   dict(cyl_deck, ldg_tau=1.0, dt=1e-3, dt_type=1, CFL=0.5, CFL_type=1), shear, 2),
+        "cfl2_local_quad_p2_ns": (jq, 2, 2, True, per,
+                                  dict(cyl_deck, ldg_tau=1.0, dt=1e-3, dt_type=2, CFL=0.5, CFL_type=2), shear, 2),
+        "cfl2_global_hex_p2_ns": (jh, 3, 2, True, per,
+                                  dict(cyl_deck, mach_fs=0.3, dt=1e-3, dt_type=1, CFL=0.5, CFL_type=2), tgv, 2),
+        "cfl1_local_hex_p2_euler": (jh, 3, 2, False, per, dict(eul, dt=1e-3, dt_type=2, CFL=0.8, CFL_type=1),
+                                    tgv, 2),
+        "cfl2_global_cyl_p2_ns_char_adi": (lambda: meshgen.cylinder_omesh(3, 8, r1=4.0), 2, 2, True,
+                                           {"WALL": "wall_ns_adi", "FARFIELD": "char"},
+                                           dict(cyl_deck, dt=1e-4, dt_type=1, CFL=0.5, CFL_type=2), cyl_state, 2),
+    }
+
+
+TIME_DIR = os.path.join(HERE, "time")
+
+
+def make_time_case(name, spec, tmp):
+    build, ndims, order, viscous, bounds, deck, state_fn, nsteps = spec
+    mesh = build()
+    meshgen.write_gmsh(mesh, os.path.join(tmp, name + ".msh"))
+    deck_path = refcpu.write_deck(os.path.join(tmp, name + ".deck"), name + ".msh", ndims, order, viscous,
+                                  bounds, deck)
+    r = refcpu.RefSolver(deck_path)
+    S, V, E = r.state_shape
+    X = r.array("coord_spts").reshape(S, ndims, E)
+    U0 = ics.perturb(state_fn(X, r.params["gamma"]), 1e-3, seed=zlib.crc32(name.encode()))
+    r.set_state(U0)
+    dt0 = []
+    for _ in range(nsteps):
+        r.update(1)
+        dt0.append(float(r.array("dt")[0]))
+    Un = r.get_state()
+    dt_ele = r.array("dt")
+    faces_t = np.array([f[0] for f in mesh.bnd_faces], dtype=np.int64)
+    npf = max(len(f[1]) for f in mesh.bnd_faces)
+    faces_n = np.full((len(mesh.bnd_faces), npf), -1, dtype=np.int64)
+    for i, f in enumerate(mesh.bnd_faces):
+        faces_n[i, :len(f[1])] = f[1]
+    faces_name = np.array([f[2] for f in mesh.bnd_faces])
+    meta = {"name": name, "ndims": ndims, "order": order, "viscous": bool(viscous), "bounds": bounds,
+            "deck": deck, "params": r.params, "nsteps": nsteps, "shape": [S, V, E], "gmsh_type": mesh.gmsh_type}
+    os.makedirs(TIME_DIR, exist_ok=True)
+    out = os.path.join(TIME_DIR, name + ".npz")
+    np.savez_compressed(out, meta=json.dumps(meta), nodes=mesh.nodes, elements=mesh.elements, faces_type=faces_t,
+                        faces_nodes=faces_n, faces_name=faces_name, U0=U0, Un=Un, dt0=np.array(dt0),
+                        dt_ele=dt_ele)
+    r.close()
+    return out
+
+
 def main(names=None):
-    cases = _cases()
     with tempfile.TemporaryDirectory() as tmp:
-        for name, spec in cases.items():
-            if names and name not in names:
-                continue
-            out = make_case(name, spec, tmp)
-            print(f"{name}: {os.path.getsize(out) / 1024:.1f} KiB")
+        for table, fn in ((_cases(), make_case), (_time_cases(), make_time_case)):
+            for name, spec in table.items():
+                if names and name not in names:
+                    continue
+                out = fn(name, spec, tmp)
+                print(f"{name}: {os.path.getsize(out) / 1024:.1f} KiB")
 
 
 if __name__ == "__main__":

@@ -61,3 +61,50 @@ def rel_err(a: np.ndarray, b: np.ndarray) -> float:
     """max |a-b| over the tensor, relative to the largest |b| of the same variable."""
     scale = np.abs(b).max(axis=(0, 2), keepdims=True)
     return float((np.abs(a - b) / np.maximum(scale, 1e-300)).max())
+
+
+TIME_DIR = os.path.join(GOLDEN_DIR, "time")
+
+
+@dataclass
+class TimeGolden:
+    """Time-integration fixture: mesh, deck, U0, the reference's dt(0) after
+    every step (dt0), its per-element dt after the last step (dt_ele) and the
+    final state (Un)."""
+    name: str
+    meta: Dict
+    mesh: Mesh
+    bounds: Dict[str, str]
+    params: Dict[str, float]
+    U0: np.ndarray
+    Un: np.ndarray
+    dt0: np.ndarray
+    dt_ele: np.ndarray
+
+    @property
+    def viscous(self) -> bool:
+        return bool(self.meta["viscous"])
+
+    @property
+    def order(self) -> int:
+        return int(self.meta["order"])
+
+    @property
+    def deck(self) -> Dict:
+        return self.meta["deck"]
+
+
+def time_names() -> List[str]:
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(TIME_DIR, "*.npz")))
+
+
+def load_time(name: str) -> TimeGolden:
+    z = np.load(os.path.join(TIME_DIR, name + ".npz"), allow_pickle=False)
+    meta = json.loads(str(z["meta"]))
+    faces = []
+    for t, nodes, nm in zip(z["faces_type"], z["faces_nodes"], z["faces_name"]):
+        faces.append((int(t), tuple(int(n) for n in nodes if n >= 0), str(nm)))
+    mesh = Mesh(ndims=meta["ndims"], nodes=z["nodes"], gmsh_type=meta["gmsh_type"], elements=z["elements"],
+                bnd_faces=faces)
+    return TimeGolden(name=name, meta=meta, mesh=mesh, bounds=meta["bounds"], params=meta["params"], U0=z["U0"],
+                      Un=z["Un"], dt0=z["dt0"], dt_ele=z["dt_ele"])

@@ -37,7 +37,9 @@ EXPORTED = [
     "zb_vjp_geometry_accumulate", "zb_geometry_adjoint_get",
     "zb_batch_create", "zb_batch_destroy", "zb_batch_autotune", "zb_batch_set_config", "zb_batch_step",
     "zb_batch_stage", "zb_batch_synchronize", "zb_batch_launch_count",
+    "zb_time_scheme_defaults", "zb_set_time_scheme", "zb_time_state", "zb_get_element_dt",
 ]
+ZB_RK44, ZB_RK54 = 0, 1
 ZB_NKERNELS = 11
 
 
@@ -60,6 +62,15 @@ class ZbParams(ctypes.Structure):
         ("V_fs", ctypes.c_double * 3), ("P_fs", ctypes.c_double), ("T_wall", ctypes.c_double),
         ("R_ref", ctypes.c_double), ("V_wall", ctypes.c_double * 3), ("dt", ctypes.c_double),
         ("tri_volume_div", ctypes.c_int),
+    ]
+
+
+class ZbTimeScheme(ctypes.Structure):
+    _fields_ = [
+        ("scheme", ctypes.c_int), ("dt_type", ctypes.c_int), ("cfl_type", ctypes.c_int), ("cfl", ctypes.c_double),
+        ("adapt_dt", ctypes.c_int), ("atol", ctypes.c_double), ("rtol", ctypes.c_double),
+        ("pi_alpha", ctypes.c_double), ("pi_beta", ctypes.c_double), ("safety", ctypes.c_double),
+        ("max_factor", ctypes.c_double), ("min_factor", ctypes.c_double), ("max_dt", ctypes.c_double),
     ]
 
 
@@ -152,6 +163,11 @@ def lib() -> ctypes.CDLL:
         L.zb_vjp_geometry_accumulate.argtypes = [vp, dp, dp, i64, i64, i64, ctypes.c_int, dp]
         L.zb_geometry_adjoint_get.argtypes = [vp, dp, dp, dp, dp, ctypes.c_int]
         L.zb_vjp_geometry.argtypes = [vp, dp, dp, i64, i64, i64, ctypes.c_int, dp, dp, dp, dp, dp]
+        L.zb_time_scheme_defaults.argtypes = [ctypes.POINTER(ZbTimeScheme)]
+        L.zb_time_scheme_defaults.restype = None
+        L.zb_set_time_scheme.argtypes = [vp, ctypes.POINTER(ZbTimeScheme)]
+        L.zb_time_state.argtypes = [vp, dp, dp, ctypes.POINTER(i64), dp]
+        L.zb_get_element_dt.argtypes = [vp, dp]
         _lib = L
     return _lib
 

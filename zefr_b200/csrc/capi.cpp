@@ -311,6 +311,36 @@ zb_status zb_step(zb_ctx *ctx, int n)
   })
 }
 
+void zb_time_scheme_defaults(zb_time_scheme *out)
+{
+  if (!out) return;
+  *out = zb_time_scheme{ZB_RK44, 0, 1, 1.0, 0, 1e-5, 1e-5, 0.7, 0.4, 0.8, 2.5, 0.3, 100.0};
+}
+
+zb_status zb_set_time_scheme(zb_ctx *ctx, const zb_time_scheme *ts)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && ts, "null argument");
+    zb::ctx_set_time_scheme(ctx->impl, ts);
+  })
+}
+
+zb_status zb_time_state(zb_ctx *ctx, double *dt, double *prev_err, int64_t *rejected, double *flow_time)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_time_state(ctx->impl, dt, prev_err, rejected, flow_time);
+  })
+}
+
+zb_status zb_get_element_dt(zb_ctx *ctx, double *out)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx && out, "null argument");
+    zb::ctx_get_element_dt(ctx->impl, out);
+  })
+}
+
 zb_status zb_residual_norms(zb_ctx *ctx, double *out)
 {
   ZB_GUARD({

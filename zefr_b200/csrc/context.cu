@@ -3,6 +3,7 @@
 #include "ctx_impl.cuh"
 #include "hex_kernels.cuh"
 #include "tri_kernels.cuh"
+#include "time_kernels.cuh"
 
 namespace zb {
 
@@ -454,6 +455,7 @@ static void bind(Ctx &c)
 {
   c.launch_extrap = &launch_extrap_impl<T, A, D, N>;
   c.launch_stage = &launch_stage_impl<T, A, D, N>;
+  c.launch_dt = &launch_dt_impl<T, A, D, N>;
 }
 
 template <typename T, typename A>
@@ -502,7 +504,8 @@ static void free_all(Ctx *c)
   void *bufs[] = {c->U, c->U_ini, c->divF[0], c->divF[1], c->divF[2], c->divF[3], c->divF_vol, c->Ufp[0],
                   c->Ufp[1], c->Fvn, c->Fcom, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
                   c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubar, c->pbar, c->dops, c->dwall,
-                  c->mbar, c->gbar, c->nbx, c->mbar_acc, c->gbar_acc};
+                  c->mbar, c->gbar, c->nbx, c->mbar_acc, c->gbar_acc, c->d_dt, c->dt_ele, c->h_ref, c->evol,
+                  c->dfw, c->U_til, c->rk_err};
   for (void *b : bufs)
     if (b) cudaFree(b);
   for (auto &r : c->recs)
@@ -833,6 +836,7 @@ void ctx_get_residual(Ctx *c, unsigned stage, double *out, int64_t ss, int64_t v
 void ctx_rk_stage(Ctx *c, unsigned stage)
 {
   if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  if (c->ts.scheme != ZB_RK44) ZB_THROW(ZB_ERR_UNSUPPORTED, "stage-wise stepping is built for RK44");
   ensure_ufp(c);
   StageCfg sc;
   sc.stage = stage;
@@ -842,12 +846,7 @@ void ctx_rk_stage(Ctx *c, unsigned stage)
   c->launch_stage(*c, sc);
 }
 
-void ctx_step(Ctx *c, int n)
-{
-  if (n < 0) ZB_THROW(ZB_ERR_ARG, "negative step count");
-  for (int i = 0; i < n; i++)
-    for (int s = 0; s < c->nstages; s++) ctx_rk_stage(c, (unsigned)s);
-}
+void ctx_step(Ctx *c, int n) { ctx_step_scheme(c, n); }
 
 void ctx_norms(Ctx *c, double *out)
 {

@@ -28,6 +28,15 @@ void ctx_compute_residual(Ctx *c, unsigned stage);
 void ctx_get_residual(Ctx *c, unsigned stage, double *out, int64_t ss, int64_t vs, int64_t es, int where);
 void ctx_rk_stage(Ctx *c, unsigned stage);
 void ctx_step(Ctx *c, int n);
+// time integration (time_scheme.cu)
+void ctx_set_time_scheme(Ctx *c, const zb_time_scheme *ts);
+void ctx_time_state(Ctx *c, double *dt, double *prev_err, int64_t *rejected, double *flow_time);
+void ctx_get_element_dt(Ctx *c, double *out);
+void ctx_step_scheme(Ctx *c, int n);  // zb_step with the context's time scheme
+// CFL limits of the upwinded advection and LDG diffusion operators per order
+// (reference get_cfl_limit_adv / get_cfl_limit_diff, src/funcs.cpp:435-560)
+double cfl_limit_adv(int order);
+double cfl_limit_diff(int order, double beta);
 void ctx_norms(Ctx *c, double *out);
 void ctx_sync(Ctx *c);
 int64_t ctx_launches(const Ctx *c);

@@ -81,9 +81,22 @@ struct Ctx
   double *pbar = nullptr;
   double *mbar = nullptr, *gbar = nullptr, *nbx = nullptr;  // geometry adjoint
   double *mbar_acc = nullptr, *gbar_acc = nullptr;          // its device-side sums
+  // time integration (zb_set_time_scheme; time_scheme.cu); the RK54 and CFL
+  // buffers are allocated on first use
+  zb_time_scheme ts{ZB_RK44, 0, 1, 1.0, 0, 1e-5, 1e-5, 0.7, 0.4, 0.8, 2.5, 0.3, 100.0};
+  double prev_err = 1.0, flow_time = 0.0;
+  int64_t rejected = 0;
+  double *d_dt = nullptr;     // [0] CFL step (global minimum), [1] error maximum, [2] flow time of CFL steps
+  double *dt_ele = nullptr;   // [ntiles * TW] per-element CFL step
+  double *h_ref = nullptr;    // [ntiles][Fp][TW] CFL_type 2 line lengths
+  double *evol = nullptr;     // [ntiles * TW] element volumes
+  double *dfw = nullptr;      // face-point quadrature weights [Fp / faces]
+  void *U_til = nullptr, *rk_err = nullptr;
+  bool use_dt_dev = false, use_dt_ele = false;  // stage kernels read the step from d_dt / dt_ele
   void (*launch_extrap)(Ctx &) = nullptr;
   void (*launch_stage)(Ctx &, const StageCfg &) = nullptr;
   void (*launch_vjp)(Ctx &, bool, bool) = nullptr;
+  void (*launch_dt)(Ctx &) = nullptr;  // CFL estimate from the current traces
 };
 
 static cudaEvent_t take_event(Ctx &c)
@@ -217,6 +230,8 @@ static Args<T, A> make_args(Ctx &c, const StageCfg &sc)
   a.U_ini = (T *)c.U_ini;
   a.Ucomp = nullptr;
   a.dt = (A)c.dt;
+  a.dt_dev = c.use_dt_dev ? c.d_dt : nullptr;
+  a.dt_ele = c.use_dt_ele ? c.dt_ele : nullptr;
   a.ntiles = c.ntiles;
   a.dU_out = sc.want_dU ? (T *)c.dU : nullptr;
   a.dops = (const A *)c.dops;

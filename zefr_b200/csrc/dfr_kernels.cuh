@@ -56,6 +56,8 @@ struct Args
   A *divF_vol;       // NS: volume part of the residual (arithmetic type: it cancels
                      // against the surface part)
   T *Fvn;            // NS: viscous normal flux at own flux points
+  const double *dt_dev;  // optional: the step as computed on the device (CFL, global)
+  const double *dt_ele;  // optional: per-element step [tile * TW + lane] (CFL, local)
   T *Fcom;           // NS hexahedra, LDG beta = +-1/2, optional: common flux (convective
                      // + viscous, not dA-scaled) at the flux points whose side supplies
                      // the LDG normal flux; the partner reads it from there
@@ -275,6 +277,15 @@ __device__ __forceinline__ void conv_common(const Args<T, A> &a, const A Uo[D + 
     rusanov<A, D>(UL, UR, n, F, a.ph);
 }
 
+// time step of element (tile, lane): per element, device-computed or fixed
+template <typename T, typename A>
+__device__ __forceinline__ A step_dt(const Args<T, A> &a, int64_t tile, int l)
+{
+  if (a.dt_ele) return (A)a.dt_ele[tile * TW + l];
+  if (a.dt_dev) return (A)a.dt_dev[0];
+  return a.dt;
+}
+
 // ---------------------------------------------------------------------------
 // Store the residual of one point and apply the optional RK update
 // (src/solver.cpp:2916-2937, 3040-3094).
@@ -288,6 +299,7 @@ __device__ __forceinline__ void store_rk(const Args<T, A> &a, int64_t tile, int 
   for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
   if (a.rk_mode == 0) return;
   const A detJ = a.mets[((tile * S + s) * NM + D * D) * TW + l];
+  const A dtv = step_dt(a, tile, l);
 #pragma unroll
   for (int v = 0; v < V; v++)
   {
@@ -302,7 +314,7 @@ __device__ __forceinline__ void store_rk(const Args<T, A> &a, int64_t tile, int 
       u_ini = a.U_ini[idx];
     A unew;
     if (a.rk_mode == 1)
-      unew = u_ini - a.rk_coef[0] * a.dt / detJ * res[v];
+      unew = u_ini - a.rk_coef[0] * dtv / detJ * res[v];
     else
     {
       if (a.Ucomp)
@@ -310,8 +322,8 @@ __device__ __forceinline__ void store_rk(const Args<T, A> &a, int64_t tile, int 
         // Kahan-compensated accumulation of the step increment; the
         // remainder includes the rounding of the stored state
         A delta = A(0);
-        for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * a.dt / detJ * (A)a.divF_prev[st][idx];
-        delta -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
+        for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * dtv / detJ * (A)a.divF_prev[st][idx];
+        delta -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
         const A c = a.Ucomp[idx];
         const A y = delta - c;
         unew = (A)(T)(u_ini + y);
@@ -321,8 +333,8 @@ __device__ __forceinline__ void store_rk(const Args<T, A> &a, int64_t tile, int 
       {
         // reference order: U = U_ini; U -= b_s dt/|J| divF_s for s = 0..
         unew = u_ini;
-        for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * a.dt / detJ * a.divF_prev[st][idx];
-        unew -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
+        for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * dtv / detJ * a.divF_prev[st][idx];
+        unew -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
       }
     }
     a.Uout[idx] = unew;

@@ -296,6 +296,7 @@ __device__ __forceinline__ void hex_finish(const Args<T, A> &a, int64_t tile, in
   for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
   if (a.rk_mode == 0) return;
   const A detJ = a.mets[((tile * H::S + s) * NM + 9) * TW + l];
+  const A dtv = step_dt(a, tile, l);
 #pragma unroll
   for (int v = 0; v < V; v++)
   {
@@ -310,14 +311,14 @@ __device__ __forceinline__ void hex_finish(const Args<T, A> &a, int64_t tile, in
       u_ini = a.U_ini[idx];
     A unew;
     if (a.rk_mode == 1)
-      unew = u_ini - a.rk_coef[0] * a.dt / detJ * res[v];
+      unew = u_ini - a.rk_coef[0] * dtv / detJ * res[v];
     else if (a.Ucomp)
     {
       // Kahan-compensated step increment; the remainder includes the
       // rounding of the stored state
       A delta = A(0);
-      for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * a.dt / detJ * (A)a.divF_prev[st][idx];
-      delta -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
+      for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * dtv / detJ * (A)a.divF_prev[st][idx];
+      delta -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
       const A c = a.Ucomp[idx];
       const A y = delta - c;
       unew = (A)(T)(u_ini + y);
@@ -326,8 +327,8 @@ __device__ __forceinline__ void hex_finish(const Args<T, A> &a, int64_t tile, in
     else
     {
       unew = u_ini;
-      for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * a.dt / detJ * a.divF_prev[st][idx];
-      unew -= a.rk_coef[a.nprev] * a.dt / detJ * res[v];
+      for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * dtv / detJ * a.divF_prev[st][idx];
+      unew -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
     }
     a.Uout[idx] = unew;
     if (sUnew) sUnew[(s * V + v) * TW + l] = (A)(T)unew;  // the state as stored

@@ -245,6 +245,41 @@ class FRSolver:
     def set_dt(self, dt: float) -> None:
         check(lib().zb_set_dt(self.h, dt))
 
+    def set_time_scheme(self, dt_scheme: str = "RK44", **kw) -> None:
+        """Time integration with the reference deck's keys (src/input.cpp:72-127):
+        ``dt_scheme`` "RK44" or "RK54"; ``dt_type`` 0/1/2, ``CFL``, ``CFL_type``;
+        ``adapt_dt`` and ``err_atol``, ``err_rtol``, ``pi_alpha``, ``pi_beta``,
+        ``safety_factor``, ``max_factor``, ``min_factor``, ``max_dt``.  Keys not
+        given keep the deck defaults."""
+        ts = _lib.ZbTimeScheme()
+        lib().zb_time_scheme_defaults(ctypes.byref(ts))
+        schemes = {"RK44": _lib.ZB_RK44, "RK54": _lib.ZB_RK54}
+        if dt_scheme not in schemes:
+            raise ValueError(f"dt_scheme must be one of {sorted(schemes)}")
+        ts.scheme = schemes[dt_scheme]
+        keys = {"dt_type": "dt_type", "CFL": "cfl", "CFL_type": "cfl_type", "adapt_dt": "adapt_dt",
+                "err_atol": "atol", "err_rtol": "rtol", "pi_alpha": "pi_alpha", "pi_beta": "pi_beta",
+                "safety_factor": "safety", "max_factor": "max_factor", "min_factor": "min_factor", "max_dt": "max_dt"}
+        for k, v in kw.items():
+            if k not in keys:
+                raise ValueError(f"unknown time-scheme key {k!r}")
+            setattr(ts, keys[k], type(getattr(ts, keys[k]))(v))
+        check(lib().zb_set_time_scheme(self.h, ctypes.byref(ts)))
+
+    def time_state(self) -> Dict[str, float]:
+        """dt the next step starts from, last accepted error estimate, rejected
+        steps and flow time."""
+        dt, err, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        rej = ctypes.c_int64()
+        check(lib().zb_time_state(self.h, ctypes.byref(dt), ctypes.byref(err), ctypes.byref(rej), ctypes.byref(t)))
+        return {"dt": dt.value, "prev_err": err.value, "rejected": int(rej.value), "flow_time": t.value}
+
+    def element_dt(self) -> np.ndarray:
+        """Per-element step of the last CFL estimate, [n_eles]."""
+        out = np.zeros(self.info.n_eles)
+        check(lib().zb_get_element_dt(self.h, out.ctypes.data_as(_DP)))
+        return out
+
     def set_freestream(self, rho_fs: float, V_fs, P_fs: float) -> None:
         """Free-stream state of the far-field / characteristic boundaries."""
         v = np.zeros(3)
