@@ -244,7 +244,7 @@ __device__ __forceinline__ void hex_gather_common(const Args<T, A> &a, int64_t t
   using H = HexIdx<N>;
   constexpr int V = 5;
   const int supplier = a.ph.ldg_b == A(0.5) ? 0 : 1;  // slot whose normal flux LDG takes
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < 6 / ZS; k++)
   {
     const int q = own_face<ZS>(zs, k);
@@ -634,7 +634,13 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
       // hex_common_flux with the partner's normal flux zero)
       const A tau = a.ph.ldg_tau;
       A Un[V], UL[V], UR[V], UB[V], Fc[V];
-      if (code >= 0) gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
+      // with beta = +-1/2 the supplying side's common solution is the
+      // partner's trace, already in shared memory
+      if (code >= 0)
+      {
+#pragma unroll
+        for (int v = 0; v < V; v++) Un[v] = sUC[(fq * V + v) * TW + l];
+      }
       conv_common<T, A, 3>(a, Uf, Un, code, n, UL, UR, UB, Fc);
       T *fc = a.Fcom + (tile * Fp + fq) * (int64_t)V * TW + l;
 #pragma unroll
