@@ -495,8 +495,9 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
         sU[(s * V + v) * TW + l] = Ut[(s * V + v) * TW + l];
       }
   }
-  // common solution at own flux points (LDG, flip_beta = 1)
-#pragma unroll 1
+  // common solution at own flux points (LDG, flip_beta = 1); unrolled so the
+  // partner gathers of all points are in flight together
+#pragma unroll
   for (int kq = 0; kq < 6 / ZS; kq++)
   {
     const int q = own_face<ZS>(zs, kq);
