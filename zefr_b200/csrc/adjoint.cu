@@ -29,7 +29,10 @@ static void launch_adj_kernels(Ctx &c, const dev::AdjArgs &a, const LineOpsT<dou
     CK(cudaGetLastError());
     return;
   }
-  const size_t smem1 = (size_t)(2 * S * V + Fp * V + 2 * D * S * V) * TW * sizeof(double);
+  // the state adjoint's staged face inputs: [Fp][3V + D][TW]
+  const size_t smem1 = (size_t)(GEO ? 2 * S * V + Fp * V + 2 * D * S * V
+                                    : S * V + Fp * V + D * S * V + Fp * (3 * V + D)) *
+                       TW * sizeof(double);
   set_smem(dev::k_adj_ns1<D, N, GEO>, smem1);
   {
     ProfScope ps(c, ZB_K_ADJ_VOL);
@@ -61,6 +64,7 @@ static void launch_vjp_impl(Ctx &c, bool params, bool geo)
   a.Lfp = c.Lfp;
   a.Ubfp = c.Ubfp;
   a.dUbfp = c.dUbfp;
+  a.Ubx = c.Ubx;
   a.UCb = c.UCb;
   a.Ubar = c.Ubar;
   a.pbar = params ? c.pbar : nullptr;

@@ -279,26 +279,28 @@ ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double 
   const double g = ph.gamma;
   // ---- forward recomputation ----
   const double rL = UL[0], rR = UR[0];
+  // reciprocals formed once: the FP64 division is a multi-instruction sequence
+  const double irL = 1.0 / rL, irR = 1.0 / rR;
   double m2L = 0.0, m2R = 0.0;
   for (int d = 0; d < D; d++)
   {
     m2L += UL[d + 1] * UL[d + 1];
     m2R += UR[d + 1] * UR[d + 1];
   }
-  const double PL = (g - 1.0) * (UL[V - 1] - 0.5 * m2L / rL);
-  const double PR = (g - 1.0) * (UR[V - 1] - 0.5 * m2R / rR);
+  const double PL = (g - 1.0) * (UL[V - 1] - 0.5 * m2L * irL);
+  const double PR = (g - 1.0) * (UR[V - 1] - 0.5 * m2R * irR);
   const double sL = sqrt(rL), sR = sqrt(rR);
   const double inv = 1.0 / (sL + sR);
   double uL[D], uR[D], u[D], unL = 0.0, unR = 0.0;
   for (int d = 0; d < D; d++)
   {
-    uL[d] = UL[d + 1] / rL;
-    uR[d] = UR[d + 1] / rR;
+    uL[d] = UL[d + 1] * irL;
+    uR[d] = UR[d + 1] * irR;
     u[d] = (sL * uL[d] + sR * uR[d]) * inv;
     unL += uL[d] * n[d];
     unR += uR[d] * n[d];
   }
-  const double HL = (UL[V - 1] + PL) / rL, HR = (UR[V - 1] + PR) / rR;
+  const double HL = (UL[V - 1] + PL) * irL, HR = (UR[V - 1] + PR) * irR;
   const double H = (sL * HL + sR * HR) * inv;
   double q2 = 0.0, un = 0.0;
   for (int d = 0; d < D; d++)
@@ -310,21 +312,23 @@ ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double 
   const bool clamped = !(c2 > 1e-30);
   if (clamped) c2 = 1e-30;
   const double a = sqrt(c2);
+  const double ic2 = 1.0 / c2, ia = 1.0 / a;
   const double rho = sL * sR;
   const double dp = PR - PL, dr = rR - rL, dun = unR - unL;
-  const double t2 = 1.0 / (2.0 * c2);
+  const double t2 = 0.5 * ic2;
   const double a1 = (dp - rho * a * dun) * t2;
   const double a3 = (dp + rho * a * dun) * t2;
-  const double a2w = dr - dp / c2;
+  const double a2w = dr - dp * ic2;
   const double x[3] = {un - a, un, un + a};
   const double delta = 0.1 * (fabs(un) + a);
+  const double idelta = 1.0 / delta;
   double l[3];
   bool fixed[3];
   for (int i = 0; i < 3; i++)
   {
     const double ax = fabs(x[i]);
     fixed[i] = ax < delta;
-    l[i] = fixed[i] ? (ax * ax + delta * delta) / (2.0 * delta) : ax;
+    l[i] = fixed[i] ? (ax * ax + delta * delta) * (0.5 * idelta) : ax;
   }
   double dvt[D], udvt = 0.0;
   for (int d = 0; d < D; d++)
@@ -400,8 +404,8 @@ ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double 
     double axb = lb[i];
     if (fixed[i])
     {
-      axb = lb[i] * ax / delta;
-      deltab += lb[i] * (delta * delta - ax * ax) / (2.0 * delta * delta);
+      axb = lb[i] * ax * idelta;
+      deltab += lb[i] * (delta * delta - ax * ax) * (0.5 * idelta * idelta);
     }
     const double xb = (x[i] < 0.0) ? -axb : axb;
     unb += xb;
@@ -416,16 +420,16 @@ ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double 
   rhob -= a1b * a * dun * t2;
   ab -= a1b * rho * dun * t2;
   dunb -= a1b * rho * a * t2;
-  c2b -= a1b * a1 / c2;
+  c2b -= a1b * a1 * ic2;
   dpb += a3b * t2;
   rhob += a3b * a * dun * t2;
   ab += a3b * rho * dun * t2;
   dunb += a3b * rho * a * t2;
-  c2b -= a3b * a3 / c2;
+  c2b -= a3b * a3 * ic2;
   drb += a2wb;
-  dpb -= a2wb / c2;
-  c2b += a2wb * dp / (c2 * c2);
-  c2b += ab / (2.0 * a);
+  dpb -= a2wb * ic2;
+  c2b += a2wb * dp * (ic2 * ic2);
+  c2b += ab * (0.5 * ia);
   if (!clamped)
   {
     Hb += (g - 1.0) * c2b;
@@ -442,12 +446,12 @@ ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double 
     sLb += Hb * HL * inv;
     sRb += Hb * HR * inv;
     invb += Hb * (sL * HL + sR * HR);
-    UbL[V - 1] += HLb / rL;
-    PLb += HLb / rL;
-    rLb -= HLb * HL / rL;
-    UbR[V - 1] += HRb / rR;
-    PRb += HRb / rR;
-    rRb -= HRb * HR / rR;
+    UbL[V - 1] += HLb * irL;
+    PLb += HLb * irL;
+    rLb -= HLb * HL * irL;
+    UbR[V - 1] += HRb * irR;
+    PRb += HRb * irR;
+    rRb -= HRb * HR * irR;
   }
   for (int d = 0; d < D; d++)
   {
@@ -461,13 +465,13 @@ ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double 
   sRb -= invb * inv * inv;
   for (int d = 0; d < D; d++)
   {
-    UbL[d + 1] += uLb[d] / rL;
-    rLb -= uLb[d] * uL[d] / rL;
-    UbR[d + 1] += uRb[d] / rR;
-    rRb -= uRb[d] * uR[d] / rR;
+    UbL[d + 1] += uLb[d] * irL;
+    rLb -= uLb[d] * uL[d] * irL;
+    UbR[d + 1] += uRb[d] * irR;
+    rRb -= uRb[d] * uR[d] * irR;
   }
-  rLb += sLb / (2.0 * sL);
-  rRb += sRb / (2.0 * sR);
+  rLb += sLb * (0.5 * sL * irL);  // d sqrt(r) / dr = 1 / (2 sqrt(r)) = sqrt(r) / (2 r)
+  rRb += sRb * (0.5 * sR * irR);
   UbL[0] += rLb;
   UbR[0] += rRb;
   pressure_vjp<D>(UL, PLb, g, UbL);
@@ -782,6 +786,8 @@ struct AdjArgs
   double *Lfp;         // [tile][Fp][V][TW] weight on the own-side surface flux
   double *Ubfp;        // [tile][Fp][V][TW] adjoint of the own trace U_fpts
   double *dUbfp;       // NS: [tile][Fp][V][D][TW] adjoint of the own gradient trace
+  double *Ubx;         // NS: [tile][Fp][V][TW] Riemann-flux adjoint of a right side's trace,
+                       // written by its left partner, added in the trace pass
   double *UCb;         // NS: [tile][Fp][V][TW] adjoint of the own common solution
   double *Ubar;        // [tile][S][V][TW] result
   double *pbar;        // [ntiles][5] per-tile free-stream adjoint (nullptr: off)
@@ -1134,18 +1140,44 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_euler(const __grid_cons
 // the volume flux, of the face fluxes and of the gradient; writes the partial
 // solution-point result, the trace adjoint and the common-solution adjoint.
 // ---------------------------------------------------------------------------
+// Item order of the face pass: face pairs in turn, with the pair's two faces
+// swapped on every other pair, so the items a thread takes (stride NT) mix
+// both sides of the faces -- the Riemann VJP runs on the left side only,
+// usually the + face -- and each warp's lanes stay on one face.
+template <int D, int N>
+__device__ __forceinline__ void face_item(int it, int &f, int &l)
+{
+  constexpr int NF = Shape<D, N>::NF;
+  const int pair = it / (2 * NF * TW), within = it % (2 * NF * TW);
+  const int face = 2 * pair + ((within / (NF * TW)) ^ (pair & 1));
+  const int rest = within % (NF * TW);
+  f = face * NF + rest / TW;
+  l = rest % TW;
+}
+
 template <int D, int N, bool GEO>
 __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_constant__ AdjArgs a,
-                                                             const __grid_constant__ LineOpsT<double, N> ops)
+                                                                           const __grid_constant__ LineOpsT<double, N> ops)
 {
   using G = Shape<D, N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, NM = G::NM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *sU = reinterpret_cast<double *>(smem_raw);  // [S][V][TW]
   double *sUC = sU + S * V * TW;                       // [Fp][V][TW]
-  double *sUb = sUC + Fp * V * TW;                     // [S][V][TW]
-  double *sdU = sUb + S * V * TW;                      // [D][S][V][TW] physical gradient
-  double *sG = sdU + D * S * V * TW;                   // [D][S][V][TW] its adjoint, then tdU's
+  double *sdU = sUC + Fp * V * TW;                     // [D][S][V][TW] physical gradient
+  // The state adjoint reuses the common solution's array for the volume
+  // flux's U adjoint [S][V][TW] and the gradient's for the gradient adjoint
+  // [D][S][V][TW] (each dead by then), which leaves more of the SM's L1 to
+  // cache the gathers; the geometry variant reads both again later and keeps
+  // all five apart.
+  double *sUb = GEO ? sdU + D * S * V * TW : sUC;
+  double *sG = GEO ? sUb + S * V * TW : sdU;
+  // State adjoint: the face pass's inputs per own flux point -- weight w,
+  // own and partner traces, normal -- gathered once in the common-solution
+  // pass, where the same traces are loaded, so the register-heavy face pass
+  // runs on shared-memory reads ([Fp][FK][TW]; FK = 3V + D).
+  constexpr int FK = 3 * V + D;
+  double *sFace = sdU + D * S * V * TW;
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
   const double beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
@@ -1163,10 +1195,29 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
     const double *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
+    if (!GEO)
+    {
+      double n[D], w[V];
+      face_weight<D, N>(a, tile, f, l, code, n, w);
+      double *sf = sFace + f * FK * TW + l;
+#pragma unroll
+      for (int v = 0; v < V; v++)
+      {
+        sf[v * TW] = w[v];
+        sf[(V + v) * TW] = Uo[v];
+      }
+#pragma unroll
+      for (int d = 0; d < D; d++) sf[(3 * V + d) * TW] = n[d];
+    }
     if (code >= 0)
     {
       double Un[V];
       gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
+      if (!GEO)
+      {
+#pragma unroll
+        for (int v = 0; v < V; v++) sFace[(f * FK + 2 * V + v) * TW + l] = Un[v];
+      }
       const int slot = code & 1;
 #pragma unroll
       for (int v = 0; v < V; v++)
@@ -1230,6 +1281,97 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
       }
   }
   __syncthreads();
+  // adjoint of the face fluxes at own flux points
+  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  {
+    int f, l;
+    face_item<D, N>(it, f, l);
+    const int code = a.nbr[(tile * Fp + f) * (int64_t)TW + l];
+    double n[D], w[V], Uo[V], dUo[V][D], Ub[V], dUb[V][D];
+    const double *sf = sFace + f * FK * TW + l;
+    if (GEO)
+      face_weight<D, N>(a, tile, f, l, code, n, w);
+    else
+    {
+#pragma unroll
+      for (int v = 0; v < V; v++) w[v] = sf[v * TW];
+#pragma unroll
+      for (int d = 0; d < D; d++) n[d] = sf[(3 * V + d) * TW];
+    }
+    const double *uo = GEO ? a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l : sf + V * TW;
+    SOps<double, N> o(reinterpret_cast<const double *>(&ops));
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      Uo[v] = uo[v * TW];
+      Ub[v] = 0.0;
+#pragma unroll
+      for (int d = 0; d < D; d++)
+      {
+        dUo[v][d] = extrap_smem<double, D, N>(sdU + d * S * V * TW, o, f, v, l, V);
+        dUb[v][d] = 0.0;
+      }
+    }
+    if (code >= 0)
+    {
+      const bool own_left = !(code & 1);
+      if (own_left)
+      {
+        // one reverse sweep of the shared Riemann flux gives both sides'
+        // adjoints (the right side forms the same weight w bitwise): keep
+        // the left's, leave the right's at the partner's flux point
+        double Un[V], bL[V], bR[V];
+        if (GEO)
+          gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
+        else
+        {
+#pragma unroll
+          for (int v = 0; v < V; v++) Un[v] = sf[(2 * V + v) * TW];
+        }
+#pragma unroll
+        for (int v = 0; v < V; v++) bL[v] = bR[v] = 0.0;
+        if (a.ph.fconv == 2)
+          roe_vjp<D>(Uo, Un, n, w, a.ph, bL, bR);
+        else
+          rusanov_vjp<D>(Uo, Un, n, w, a.ph, bL, bR);
+        const int pidx = code >> 1;
+        double *px = a.Ubx + (int64_t)(pidx / TW) * V * TW + pidx % TW;
+#pragma unroll
+        for (int v = 0; v < V; v++)
+        {
+          Ub[v] += bL[v];
+          px[v * TW] = bR[v];
+        }
+      }
+      // LDG: (1/2 + beta) FnL + (1/2 - beta) FnR + tau (UL - UR)
+      const double c = own_left ? 0.5 + beta : 0.5 - beta;
+      if (c != 0.0)
+      {
+        double wc[V];
+#pragma unroll
+        for (int v = 0; v < V; v++) wc[v] = c * w[v];
+        visc_normal_vjp<D>(Uo, dUo, n, wc, a.ph, Ub, dUb);
+      }
+#pragma unroll
+      for (int v = 0; v < V; v++) Ub[v] += own_left ? tau * w[v] : -tau * w[v];
+    }
+    else
+    {
+      bnd_face_vjp<D, true>(-code - 1, Uo, dUo, n, w, dual_phys(a.ph), Ub, dUb);
+      if (a.pbar) bnd_face_param_vjp<D, true>(-code - 1, Uo, dUo, n, w, dual_phys(a.ph), pb);
+    }
+    if (GEO && a.gbar) geo_face_ns<D, N>(a, tile, f, l, code, n, w, Uo, dUo);
+    double *ub = a.Ubfp + (tile * Fp + f) * (int64_t)V * TW + l;
+    double *dub = a.dUbfp + (tile * Fp + f) * (int64_t)V * D * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++)
+    {
+      ub[v * TW] = Ub[v];
+#pragma unroll
+      for (int d = 0; d < D; d++) dub[(v * D + d) * TW] = dUb[v][d];
+    }
+  }
+  __syncthreads();  // the face pass reads sdU, which the volume pass may overwrite
   // adjoint of the volume flux: U and gradient parts
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
   {
@@ -1264,61 +1406,6 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
       flux_conv<double, D>(U, F, P, a.ph.gamma);
       flux_visc_add<double, D>(U, dU, F, a.ph);
       geo_adj_bar<D>(a, tile, s, l, Ft, F, S);
-    }
-  }
-  // adjoint of the face fluxes at own flux points
-  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
-  {
-    const int f = it / TW, l = it % TW;
-    const int code = a.nbr[(tile * Fp + f) * (int64_t)TW + l];
-    double n[D], w[V], Uo[V], dUo[V][D], Ub[V], dUb[V][D];
-    face_weight<D, N>(a, tile, f, l, code, n, w);
-    const double *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
-    SOps<double, N> o(reinterpret_cast<const double *>(&ops));
-#pragma unroll
-    for (int v = 0; v < V; v++)
-    {
-      Uo[v] = uo[v * TW];
-      Ub[v] = 0.0;
-#pragma unroll
-      for (int d = 0; d < D; d++)
-      {
-        dUo[v][d] = extrap_smem<double, D, N>(sdU + d * S * V * TW, o, f, v, l, V);
-        dUb[v][d] = 0.0;
-      }
-    }
-    if (code >= 0)
-    {
-      double Un[V];
-      gather_fpt<double, double, V>(a.Ufp, code >> 1, Un);
-      const bool own_left = !(code & 1);
-      conv_face_vjp_side<D>(own_left ? Uo : Un, own_left ? Un : Uo, n, w, own_left, a.ph, Ub);
-      // LDG: (1/2 + beta) FnL + (1/2 - beta) FnR + tau (UL - UR)
-      const double c = own_left ? 0.5 + beta : 0.5 - beta;
-      if (c != 0.0)
-      {
-        double wc[V];
-#pragma unroll
-        for (int v = 0; v < V; v++) wc[v] = c * w[v];
-        visc_normal_vjp<D>(Uo, dUo, n, wc, a.ph, Ub, dUb);
-      }
-#pragma unroll
-      for (int v = 0; v < V; v++) Ub[v] += own_left ? tau * w[v] : -tau * w[v];
-    }
-    else
-    {
-      bnd_face_vjp<D, true>(-code - 1, Uo, dUo, n, w, dual_phys(a.ph), Ub, dUb);
-      if (a.pbar) bnd_face_param_vjp<D, true>(-code - 1, Uo, dUo, n, w, dual_phys(a.ph), pb);
-    }
-    if (GEO && a.gbar) geo_face_ns<D, N>(a, tile, f, l, code, n, w, Uo, dUo);
-    double *ub = a.Ubfp + (tile * Fp + f) * (int64_t)V * TW + l;
-    double *dub = a.dUbfp + (tile * Fp + f) * (int64_t)V * D * TW + l;
-#pragma unroll
-    for (int v = 0; v < V; v++)
-    {
-      ub[v * TW] = Ub[v];
-#pragma unroll
-      for (int d = 0; d < D; d++) dub[(v * D + d) * TW] = dUb[v][d];
     }
   }
   __syncthreads();
@@ -1499,6 +1586,13 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns2(const __grid_consta
     double Ub[V];
 #pragma unroll
     for (int v = 0; v < V; v++) Ub[v] = ub[v * TW];
+    if (code >= 0 && (code & 1))
+    {
+      // the Riemann-flux adjoint the left partner formed for this trace
+      const double *ux = a.Ubx + (tile * Fp + f) * (int64_t)V * TW + l;
+#pragma unroll
+      for (int v = 0; v < V; v++) Ub[v] += ux[v * TW];
+    }
     if (GEO && a.gbar && code >= 0 && !(code & 1))
     {
       // collect the right side's viscous part of this face's normal adjoint

@@ -503,7 +503,7 @@ static void free_all(Ctx *c)
 {
   void *bufs[] = {c->U, c->U_ini, c->divF[0], c->divF[1], c->divF[2], c->divF[3], c->divF_vol, c->Ufp[0],
                   c->Ufp[1], c->Fvn, c->Fcom, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
-                  c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubar, c->pbar, c->dops, c->dwall,
+                  c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubx, c->Ubar, c->pbar, c->dops, c->dwall,
                   c->mbar, c->gbar, c->nbx, c->mbar_acc, c->gbar_acc, c->d_dt, c->dt_ele, c->h_ref, c->evol,
                   c->dfw, c->U_til, c->rk_err};
   for (void *b : bufs)
@@ -1002,6 +1002,7 @@ void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, in
     {
       c->dUbfp = (double *)dalloc(nF * c->D * sizeof(double));
       c->UCb = (double *)dalloc(nF * sizeof(double));
+      c->Ubx = (double *)dalloc(nF * sizeof(double));
     }
   }
   const size_t ext = extent(c, ss, vs, es, c->S);

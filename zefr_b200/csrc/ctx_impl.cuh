@@ -78,6 +78,7 @@ struct Ctx
   int64_t prof_n[ZB_NKERNELS] = {0};
   // adjoint (plain FP64 form), allocated on first use
   double *lam = nullptr, *Lfp = nullptr, *Ubfp = nullptr, *dUbfp = nullptr, *UCb = nullptr, *Ubar = nullptr;
+  double *Ubx = nullptr;  // NS: Riemann-flux adjoint a left side leaves at its right partner
   double *pbar = nullptr;
   double *mbar = nullptr, *gbar = nullptr, *nbx = nullptr;  // geometry adjoint
   double *mbar_acc = nullptr, *gbar_acc = nullptr;          // its device-side sums
