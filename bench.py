@@ -299,10 +299,12 @@ def batched_side(steps: int = 5, ncases: int = 512, seed: int = 4):
     cfg = bt.autotune(steps=2)
     bt.step(2)
     bt.synchronize()
+    n0 = bt.launch_count()
     t0 = time.perf_counter()
     bt.step(steps)
     bt.synchronize()
     ms_batch = (time.perf_counter() - t0) * 1e3 / steps
+    batch_launches = (bt.launch_count() - n0) // steps
     # one launch per case and stage, every case on its own context stream
     for c in cases:
         c.step(1)
@@ -333,7 +335,8 @@ def batched_side(steps: int = 5, ncases: int = 512, seed: int = 4):
     out = {"workload": "batched_vortex_512_quads_n8-96_P1-5_euler", "cases": ncases, "dof": dof,
            "setup_s": setup_s, "autotuned": cfg,
            "batched": {"gdof_s": dof * res_per_step / (ms_batch * 1e-3) / 1e9, "ms_per_step": ms_batch,
-                       "launches_per_step": 4},
+                       "launches_per_step": batch_launches,
+                       "kernels": "one persistent kernel per order present and stage, concurrent streams"},
            "one_launch_per_case": {"gdof_s": dof * res_per_step / (ms_single * 1e-3) / 1e9,
                                    "ms_per_step": ms_single, "launches_per_step": 4 * ncases,
                                    "streams": "one per case (concurrent)"},

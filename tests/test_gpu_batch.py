@@ -82,13 +82,14 @@ def test_autotune_keeps_state_and_picks_a_shape():
         assert _same(s1.get_state(), s2.get_state(), "mixed")
 
 
-def test_graph_is_one_replay_of_four_launches():
+def test_graph_is_one_replay_of_one_launch_per_order_and_stage():
     cases = zbatch.vortex_cases(4, 1, n_range=(3, 5), precision="mixed")
+    orders = len({c.info.order for c in cases})
     bt = zbatch.Batch(cases)
     n0 = bt.launch_count()
     bt.step(5)
     bt.synchronize()
-    assert bt.launch_count() - n0 == 20
+    assert bt.launch_count() - n0 == 5 * 4 * orders
 
 
 def test_batch_rejects_viscous_and_hex():

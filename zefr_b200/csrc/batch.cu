@@ -41,12 +41,14 @@ constexpr size_t batch_desc_bytes()
   return (sizeof(BatchCase<T, A>) + 15) / 16 * 16;
 }
 
-// A CTA holds blockDim.x / gsz independent groups of gsz threads (whole warps);
-// each group walks its own share of the work items with its own named barrier,
-// so low-order tiles do not leave most of a large CTA idle.
-template <typename T, typename A>
+// One persistent kernel per order present, each compiled for that order
+// (registers, shared memory) and walking that order's work items
+// [begin, end).  A CTA holds blockDim.x / gsz independent groups of gsz
+// threads (whole warps); each group walks its own share of the items with its
+// own named barrier, so low-order tiles do not leave most of a large CTA idle.
+template <typename T, typename A, int NN>
 __global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__restrict__ cases,
-                                                     const int2 *__restrict__ items, int nitems, int gsz,
+                                                     const int2 *__restrict__ items, int begin, int end, int gsz,
                                                      int gstride, int chunk)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -60,9 +62,9 @@ __global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__re
   int have = -1;  // case whose descriptor the group holds
   // a group takes chunks of `chunk` consecutive items; consecutive items of
   // one case reuse the shared descriptor
-  for (int c0 = gid * chunk; c0 < nitems; c0 += ngroups * chunk)
+  for (int c0 = begin + gid * chunk; c0 < end; c0 += ngroups * chunk)
   {
-    const int c1 = min(c0 + chunk, nitems);
+    const int c1 = min(c0 + chunk, end);
     for (int it = c0; it < c1; it++)
     {
       const int2 w = items[it];
@@ -75,17 +77,8 @@ __global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__re
         have = w.x;
       }
       dev::group_sync(bar, gsz);
-      switch (sbc->N)
-      {
-#define ZB_BATCH_N(NN)                                                                                            \
-  case NN:                                                                                                        \
-    dev::euler_tile<T, A, 2, NN>(sbc->a, *reinterpret_cast<const LineOpsT<A, NN> *>(sbc->ops), w.y, tsm, tid, gsz, \
-                                 bar);                                                                            \
-    break;
-        ZB_BATCH_N(2) ZB_BATCH_N(3) ZB_BATCH_N(4) ZB_BATCH_N(5) ZB_BATCH_N(6)
-#undef ZB_BATCH_N
-        default: break;
-      }
+      dev::euler_tile<T, A, 2, NN>(sbc->a, *reinterpret_cast<const LineOpsT<A, NN> *>(sbc->ops), w.y, tsm, tid, gsz,
+                                   bar);
     }
   }
 }
@@ -111,9 +104,12 @@ struct Batch
   void *cases[4] = {nullptr, nullptr, nullptr, nullptr};  // BatchCase arrays, one per stage
   int2 *items = nullptr;
   int nitems = 0;
+  int obeg[kBatchMaxN + 1] = {0}, oend[kBatchMaxN + 1] = {0};  // items of order N: [obeg[N], oend[N])
+  int norders = 0;  // orders present: kernels per stage
   std::vector<int> parity;  // Ufp parity of every case the descriptors assume
-  size_t smem = 0;     // tile arrays of one group (largest order)
-  size_t gstride = 0;  // one group's shared memory: descriptor + tile arrays
+  size_t gstride[kBatchMaxN + 1] = {0};  // one group's shared memory per order: descriptor + tile arrays
+  cudaStream_t ost[kBatchMaxN + 1] = {nullptr};  // one stream per order, forked from and joined to `stream`
+  cudaEvent_t efork = nullptr, ejoin[kBatchMaxN + 1] = {nullptr};
   int sms = 148;
   zb_batch_config cfg{256, 4, 0, 0.0, 64, 1};
   cudaGraph_t graph = nullptr;
@@ -163,20 +159,22 @@ static void build_cases(Batch &b)
   }
 }
 
-// Work order 0: items sorted by order (costliest first), cases interleaved
-// within an order; order 1: case-major.
+// Items grouped by order (one kernel each); within an order, work order 0
+// interleaves the cases tile by tile, order 1 is case-major.
 static void build_items(Batch &b, int order)
 {
   std::vector<int2> it;
   const int n = (int)b.ctx.size();
-  if (order == 1)
+  for (int N = kBatchMaxN; N >= 2; N--)
   {
-    for (int i = 0; i < n; i++)
-      for (int64_t t = 0; t < b.ctx[i]->ntiles; t++) it.push_back(make_int2(i, (int)t));
-  }
-  else
-  {
-    for (int N = kBatchMaxN; N >= 2; N--)
+    b.obeg[N] = (int)it.size();
+    if (order == 1)
+    {
+      for (int i = 0; i < n; i++)
+        if (b.ctx[i]->N == N)
+          for (int64_t t = 0; t < b.ctx[i]->ntiles; t++) it.push_back(make_int2(i, (int)t));
+    }
+    else
     {
       int64_t maxt = 0;
       for (int i = 0; i < n; i++)
@@ -185,7 +183,10 @@ static void build_items(Batch &b, int order)
         for (int i = 0; i < n; i++)
           if (b.ctx[i]->N == N && t < b.ctx[i]->ntiles) it.push_back(make_int2(i, (int)t));
     }
+    b.oend[N] = (int)it.size();
   }
+  b.norders = 0;
+  for (int N = 2; N <= kBatchMaxN; N++) b.norders += b.oend[N] > b.obeg[N];
   if (it.size() > (size_t)INT32_MAX) ZB_THROW(ZB_ERR_UNSUPPORTED, "batch too large");
   if (b.items) cudaFree(b.items);
   b.items = nullptr;
@@ -194,16 +195,35 @@ static void build_items(Batch &b, int order)
   b.nitems = (int)it.size();
 }
 
+template <typename T, typename A, int NN>
+static void launch_order(Batch &b, unsigned st)
+{
+  const int n = b.oend[NN] - b.obeg[NN];
+  if (n == 0) return;
+  const int ng = b.cfg.threads / b.cfg.group;
+  const int blocks =
+      std::max(1, std::min((n + ng * b.cfg.chunk - 1) / (ng * b.cfg.chunk), b.cfg.blocks_per_sm * b.sms));
+  CK(cudaStreamWaitEvent(b.ost[NN], b.efork, 0));
+  k_batch_euler<T, A, NN><<<blocks, b.cfg.threads, ng * b.gstride[NN], b.ost[NN]>>>(
+      (const BatchCase<T, A> *)b.cases[st], b.items, b.obeg[NN], b.oend[NN], b.cfg.group, (int)b.gstride[NN],
+      b.cfg.chunk);
+  b.launches++;
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(b.ejoin[NN], b.ost[NN]));
+  CK(cudaStreamWaitEvent(b.stream, b.ejoin[NN], 0));
+}
+
+// one stage: the per-order kernels run concurrently on their own streams,
+// forked from and joined back to the batch stream (also under graph capture)
 template <typename T, typename A>
 static void launch_stage_t(Batch &b, unsigned st)
 {
-  const int ng = b.cfg.threads / b.cfg.group;
-  const int blocks = std::max(1, std::min((b.nitems + ng * b.cfg.chunk - 1) / (ng * b.cfg.chunk),
-                                          b.cfg.blocks_per_sm * b.sms));
-  k_batch_euler<T, A><<<blocks, b.cfg.threads, ng * b.gstride, b.stream>>>(
-      (const BatchCase<T, A> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride, b.cfg.chunk);
-  b.launches++;
-  CK(cudaGetLastError());
+  CK(cudaEventRecord(b.efork, b.stream));
+  launch_order<T, A, 6>(b, st);
+  launch_order<T, A, 5>(b, st);
+  launch_order<T, A, 4>(b, st);
+  launch_order<T, A, 3>(b, st);
+  launch_order<T, A, 2>(b, st);
 }
 
 static void launch_stage(Batch &b, unsigned st)
@@ -226,20 +246,9 @@ static void build_graph(Batch &b)
 {
   drop_graph(b);
   CK(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
-  for (unsigned st = 0; st < 4; st++)
-  {
-    const int ng = b.cfg.threads / b.cfg.group;
-    const int blocks = std::max(1, std::min((b.nitems + ng * b.cfg.chunk - 1) / (ng * b.cfg.chunk),
-                                            b.cfg.blocks_per_sm * b.sms));
-    if (b.prec == ZB_FP64)
-      k_batch_euler<double, double><<<blocks, b.cfg.threads, ng * b.gstride, b.stream>>>(
-          (const BatchCase<double, double> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride,
-          b.cfg.chunk);
-    else
-      k_batch_euler<float, float><<<blocks, b.cfg.threads, ng * b.gstride, b.stream>>>(
-          (const BatchCase<float, float> *)b.cases[st], b.items, b.nitems, b.cfg.group, (int)b.gstride,
-          b.cfg.chunk);
-  }
+  const int64_t l0 = b.launches;
+  for (unsigned st = 0; st < 4; st++) launch_stage(b, st);
+  b.launches = l0;  // counted when the graph is replayed
   cudaError_t e = cudaStreamEndCapture(b.stream, &b.graph);
   if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
   CK(cudaGraphInstantiate(&b.exec, b.graph, 0));
@@ -272,6 +281,16 @@ static void prepare(Batch &b, unsigned first)
   drop_graph(b);
 }
 
+template <typename T, typename A>
+static void set_batch_smem(Batch &b)
+{
+  CK(cudaFuncSetAttribute(k_batch_euler<T, A, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * b.gstride[2])));
+  CK(cudaFuncSetAttribute(k_batch_euler<T, A, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * b.gstride[3])));
+  CK(cudaFuncSetAttribute(k_batch_euler<T, A, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * b.gstride[4])));
+  CK(cudaFuncSetAttribute(k_batch_euler<T, A, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * b.gstride[5])));
+  CK(cudaFuncSetAttribute(k_batch_euler<T, A, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * b.gstride[6])));
+}
+
 Batch *batch_create(Ctx *const *ctxs, int n)
 {
   if (n <= 0 || !ctxs) ZB_THROW(ZB_ERR_ARG, "empty batch");
@@ -294,18 +313,21 @@ Batch *batch_create(Ctx *const *ctxs, int n)
     b->ctx.push_back(c);
   }
   b->asz = (b->prec == ZB_FP64) ? sizeof(double) : sizeof(float);
-  int maxN = 2;
-  for (Ctx *c : b->ctx) maxN = std::max(maxN, c->N);
-  b->smem = euler_smem_bytes(maxN, b->asz);
-  b->gstride = (b->prec == ZB_FP64 ? batch_desc_bytes<double, double>() : batch_desc_bytes<float, float>()) +
-               (b->smem + 15) / 16 * 16;
+  const size_t desc = b->prec == ZB_FP64 ? batch_desc_bytes<double, double>() : batch_desc_bytes<float, float>();
+  for (int N = 2; N <= kBatchMaxN; N++) b->gstride[N] = desc + (euler_smem_bytes(N, b->asz) + 15) / 16 * 16;
   CK(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev0));
   CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  const int max_smem = (int)(4 * b->gstride);  // up to four groups per CTA
+  CK(cudaEventCreateWithFlags(&b->efork, cudaEventDisableTiming));
+  for (int N = 2; N <= kBatchMaxN; N++)
+  {
+    CK(cudaStreamCreateWithFlags(&b->ost[N], cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&b->ejoin[N], cudaEventDisableTiming));
+  }
+  // up to four groups per CTA
   if (b->prec == ZB_FP64)
-    CK(cudaFuncSetAttribute(k_batch_euler<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    set_batch_smem<double, double>(*b);
   else
-    CK(cudaFuncSetAttribute(k_batch_euler<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    set_batch_smem<float, float>(*b);
   build_items(*b, b->cfg.order);
   return b.release();
 }
@@ -318,6 +340,12 @@ void batch_destroy(Batch *b)
   for (void *p : b->cases)
     if (p) cudaFree(p);
   if (b->items) cudaFree(b->items);
+  for (int N = 2; N <= kBatchMaxN; N++)
+  {
+    if (b->ost[N]) cudaStreamDestroy(b->ost[N]);
+    if (b->ejoin[N]) cudaEventDestroy(b->ejoin[N]);
+  }
+  if (b->efork) cudaEventDestroy(b->efork);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -342,7 +370,7 @@ void batch_step(Batch *b, int nsteps, int use_graph)
     if (use_graph)
     {
       CK(cudaGraphLaunch(b->exec, b->stream));
-      b->launches += 4;
+      b->launches += 4 * b->norders;
     }
     else
       for (unsigned st = 0; st < 4; st++) launch_stage(*b, st);
