@@ -511,20 +511,30 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
     for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
     if (code >= 0)
     {
-      A Un[V];
-      gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
       const int slot = code & 1;
-#pragma unroll
-      for (int v = 0; v < V; v++)
+      if ((beta == A(0.5) && slot) || (beta == A(-0.5) && !slot))
       {
-        const A ul = slot ? Un[v] : Uo[v];
-        const A ur = slot ? Uo[v] : Un[v];
-        if (beta == A(0.5))
-          UC[v] = ur;
-        else if (beta == A(-0.5))
-          UC[v] = ul;
-        else
-          UC[v] = A(0.5) * (ul + ur) - beta * (ul - ur);
+        // beta = +1/2 (-1/2) takes the right (left) trace: this side's own,
+        // no partner gather
+#pragma unroll
+        for (int v = 0; v < V; v++) UC[v] = Uo[v];
+      }
+      else
+      {
+        A Un[V];
+        gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
+#pragma unroll
+        for (int v = 0; v < V; v++)
+        {
+          const A ul = slot ? Un[v] : Uo[v];
+          const A ur = slot ? Uo[v] : Un[v];
+          if (beta == A(0.5))
+            UC[v] = ur;
+          else if (beta == A(-0.5))
+            UC[v] = ul;
+          else
+            UC[v] = A(0.5) * (ul + ur) - beta * (ul - ur);
+        }
       }
     }
     else
