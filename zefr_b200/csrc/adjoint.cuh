@@ -1177,6 +1177,7 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
   // pass, where the same traces are loaded, so the register-heavy face pass
   // runs on shared-memory reads ([Fp][FK][TW]; FK = 3V + D).
   constexpr int FK = 3 * V + D;
+  static_assert(FK >= V * D, "staging slots hold the gradient-trace adjoint");
   double *sFace = sdU + D * S * V * TW;
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
@@ -1362,7 +1363,10 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
     }
     if (GEO && a.gbar) geo_face_ns<D, N>(a, tile, f, l, code, n, w, Uo, dUo);
     double *ub = a.Ubfp + (tile * Fp + f) * (int64_t)V * TW + l;
-    double *dub = a.dUbfp + (tile * Fp + f) * (int64_t)V * D * TW + l;
+    // the gradient-trace adjoint stays in this tile: the state adjoint keeps
+    // it in the item's staging slots (read above, FK >= V D), the geometry
+    // variant in global memory
+    double *dub = GEO ? a.dUbfp + (tile * Fp + f) * (int64_t)V * D * TW + l : sFace + f * FK * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++)
     {
@@ -1424,8 +1428,8 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
     {
       int i, fm, fp;
       spt_ends<D, N>(s, dl, i, fm, fp);
-      const double *bm = a.dUbfp + (tile * Fp + fm) * (int64_t)V * D * TW + l;
-      const double *bp = a.dUbfp + (tile * Fp + fp) * (int64_t)V * D * TW + l;
+      const double *bm = GEO ? a.dUbfp + (tile * Fp + fm) * (int64_t)V * D * TW + l : sFace + fm * FK * TW + l;
+      const double *bp = GEO ? a.dUbfp + (tile * Fp + fp) * (int64_t)V * D * TW + l : sFace + fp * FK * TW + l;
 #pragma unroll
       for (int v = 0; v < V; v++)
 #pragma unroll
