@@ -99,3 +99,23 @@ def test_time_scheme_errors():
     with pytest.raises(ZbError):
         st.set_time_scheme("RK44", dt_type=1)
     st.close()
+
+
+@pytest.mark.parametrize("name", ["rk54_adapt_quad_p3_vortex", "cfl2_global_hex_p2_ns"])
+def test_from_deck_reproduces_reference_trajectory(name, tmp_path):
+    """The same deck file the reference ran, read by FRSolver.from_deck."""
+    from oracle import refcpu
+    g = gc.load_time(name)
+    meshgen.write_gmsh(g.mesh, str(tmp_path / "m.msh"))
+    deck = refcpu.write_deck(str(tmp_path / "case.deck"), "m.msh", g.meta["ndims"], g.order, g.viscous, g.bounds,
+                             g.deck)
+    s = FRSolver.from_deck(deck)
+    s.set_state(g.U0)
+    dts = []
+    for _ in range(g.meta["nsteps"]):
+        s.update()
+        dts.append(s.time_state()["dt"])
+    tol = 1e-10 if g.deck.get("adapt_dt") else 1e-12
+    assert np.max(np.abs(np.array(dts) - g.dt0) / g.dt0) < tol
+    assert gc.rel_err(s.get_state(), g.Un) < tol
+    s.close()

@@ -156,6 +156,18 @@ class FRSolver:
         self.ndims, self.nstages = self.info.ndims, self.info.nstages
 
     # -- lifetime --
+    @classmethod
+    def from_deck(cls, path: str, precision: str = "fp64") -> "FRSolver":
+        """Solver for a reference input deck (mesh file, parameters, mesh_bound
+        lines, time scheme; see ``zefr_b200.deck``)."""
+        from .deck import read_deck
+        d = read_deck(path)
+        p = params_from_deck(precision={"fp64": 0, "mixed": 1}[precision], **d.params)
+        s = cls(d.meshfile, p, d.bounds)
+        if d.dt_scheme != "RK44" or d.time_scheme:
+            s.set_time_scheme(d.dt_scheme, **d.time_scheme)
+        return s
+
     def close(self):
         if getattr(self, "h", None):
             lib().zb_destroy(self.h)
