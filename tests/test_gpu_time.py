@@ -119,3 +119,21 @@ def test_from_deck_reproduces_reference_trajectory(name, tmp_path):
     assert np.max(np.abs(np.array(dts) - g.dt0) / g.dt0) < tol
     assert gc.rel_err(s.get_state(), g.Un) < tol
     s.close()
+
+
+def test_checkpoint_resume_is_exact(tmp_path):
+    """save_state / load_state: a resumed run continues bitwise like the
+    uninterrupted one (plain FP64, RK54 at the fixed dt)."""
+    from zefr_b200.output import load_state, save_state
+    g = gc.load_time("rk54_quad_p3_vortex")
+    a = _solver(g)
+    a.update()
+    save_state(str(tmp_path / "ck"), a)
+    a.update()
+    b = _solver(g)
+    meta = load_state(str(tmp_path / "ck.npz"), b)
+    assert meta["nspts"] == a.nspts and meta["time"]["flow_time"] > 0
+    b.update()
+    assert np.array_equal(a.get_state(), b.get_state())
+    a.close()
+    b.close()
