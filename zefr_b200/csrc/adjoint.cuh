@@ -116,12 +116,14 @@ ZB_HD void flux_visc_vjp(const double U[D + 2], const double dU[D + 2][D], const
   }
   double div = 0.0;
   for (int d = 0; d < D; d++) div += dvel[d][d];
-  const double diag = div / 3.0;
+  // constant reciprocals: an FP64 division is a multi-instruction sequence
+  const double third = 1.0 / 3.0, ipr = 1.0 / ph.prandtl;
+  const double diag = div * third;
   double tau[D][D];
   for (int i = 0; i < D; i++)
     for (int j = 0; j < D; j++)
       tau[i][j] = (i == j) ? 2.0 * mu * (dvel[i][i] - diag) : mu * (dvel[i][j] + dvel[j][i]);
-  const double kappa = (mu / ph.prandtl) * g;
+  const double kappa = (mu * ipr) * g;
   // reverse
   double taub[D][D], velb[D], dvelb[D][D], deb[D];
   double mub = 0.0, kappab = 0.0, diagb = 0.0, irb = 0.0, rhob = 0.0, e_intb = 0.0, vsqb = 0.0;
@@ -140,7 +142,7 @@ ZB_HD void flux_visc_vjp(const double U[D + 2], const double dU[D + 2][D], const
     kappab -= Fb[V - 1][j] * de[j];
     deb[j] = -Fb[V - 1][j] * kappa;
   }
-  mub += kappab * g / ph.prandtl;
+  mub += kappab * g * ipr;
   for (int i = 0; i < D; i++)
     for (int j = 0; j < D; j++)
     {
@@ -157,7 +159,7 @@ ZB_HD void flux_visc_vjp(const double U[D + 2], const double dU[D + 2][D], const
         dvelb[j][i] += mu * taub[i][j];
       }
     }
-  for (int d = 0; d < D; d++) dvelb[d][d] += diagb / 3.0;
+  for (int d = 0; d < D; d++) dvelb[d][d] += diagb * third;
   for (int j = 0; j < D; j++)
   {
     const double X = dU[V - 1][j] - dke[j] - dU[0][j] * e_int;
