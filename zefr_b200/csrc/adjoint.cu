@@ -52,7 +52,7 @@ template <int D, int N>
 static void launch_vjp_impl(Ctx &c, bool params, bool geo)
 {
   using G = Shape<D, N>;
-  constexpr int S = G::S, Fp = G::Fp, V = G::V, NT = G::NT;
+  constexpr int Fp = G::Fp;
   dev::AdjArgs a;
   std::memset(&a, 0, sizeof(a));
   a.U = (const double *)c.U;

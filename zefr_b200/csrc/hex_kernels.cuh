@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_euler(const __grid_constant_
                                                           const __grid_constant__ LineOpsT<A, N> ops)
 {
   using H = HexIdx<N>;
-  constexpr int S = H::S, Fp = H::Fp, V = 5;
+  constexpr int S = H::S, V = 5;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sU = reinterpret_cast<A *>(smem_raw);   // [S][V][TW] state, then new state
   A *sF = sU + S * V * TW;                   // [3][S][V][TW] transformed flux
