@@ -128,6 +128,30 @@ class TrajectoryAdjoint:
         return Ubar0
 
     @staticmethod
+    def _obj_grad_batch(objective: Callable, Us: torch.Tensor, geo=None):
+        """Objective gradients for a stack of states Us [M,S,V,E] in one
+        vectorised evaluation (torch.func.vmap of the gradient): the state
+        gradients per state and, with ``geo``, the geometry gradient summed
+        over the stack.  Falls back to one autograd call per state when the
+        objective cannot be vectorised."""
+        try:
+            from torch.func import grad, vmap
+            if geo is None:
+                gU = vmap(grad(objective))(Us)
+                return gU, None
+            leaves = {k: v.detach() for k, v in geo.items()}
+            gU, gG = vmap(grad(objective, argnums=(0, 1)), in_dims=(0, None))(Us, leaves)
+            return gU, {k: v.sum(dim=0) for k, v in gG.items()}
+        except Exception:  # noqa: BLE001 -- objective not vmap-able: per-state autograd
+            gUs, gsum = [], None
+            for U in Us:
+                _, gU, gG = TrajectoryAdjoint._obj_grad(objective, U, geo)
+                gUs.append(gU)
+                if gG is not None:
+                    gsum = gG if gsum is None else {k: gsum[k] + gG[k] for k in gsum}
+            return torch.stack(gUs), gsum
+
+    @staticmethod
     def _obj_grad(objective: Callable, U: torch.Tensor, geo=None):
         x = U.detach().clone().requires_grad_(True)
         if geo is None:
@@ -150,6 +174,7 @@ class TrajectoryAdjoint:
         U = torch.as_tensor(U0, dtype=torch.float64).cuda().contiguous()
         checkpoints = {0: U.clone()}
         obj = objective if geometry is None else (lambda x, geo=geometry: objective(x, geo))
+        obj_grad_fn = objective
         J = 0.0
         with torch.no_grad():
             for k in range(1, nsteps + 1):
@@ -173,16 +198,21 @@ class TrajectoryAdjoint:
             states = [checkpoints[k0]]
             for _ in range(k0 + 1, k1):
                 states.append(self._step(states[-1]))
-            for m in range(k1 - k0 - 1, -1, -1):
-                if m + 1 < len(states):
-                    Unext = states[m + 1]
-                else:
-                    Unext = checkpoints[k1] if k1 in checkpoints else self._step(states[m])
-                _, gU, gG = self._obj_grad(objective, Unext, geometry)
-                Ubar = Ubar + gU / nsteps
-                if gG is not None:
+            last = checkpoints[k1] if k1 in checkpoints else self._step(states[-1])
+            # the objective's gradients at U_{k0+1..k1} do not depend on the
+            # adjoint: vectorised evaluations over the segment, in chunks of
+            # about 1 GiB of states
+            nexts = states[1:] + [last]
+            chunk = max(1, (1 << 30) // max(1, last.numel() * last.element_size()))
+            gUs = []
+            for c0 in range(0, len(nexts), chunk):
+                gU, gGsum = self._obj_grad_batch(obj_grad_fn, torch.stack(nexts[c0:c0 + chunk]), geometry)
+                gUs.extend(gU.unbind(0))
+                if gGsum is not None:
                     for k in gbar:
-                        gbar[k] += gG[k] / nsteps
+                        gbar[k] += gGsum[k] / nsteps
+            for m in range(k1 - k0 - 1, -1, -1):
+                Ubar = Ubar + gUs[m] / nsteps
                 Ubar = self._step_adjoint(states[m], Ubar, pbar, gbar)
         out = {"J": J, "dJ_dU0": Ubar, "dJ_dfreestream": pbar}
         if gbar is not None:

@@ -92,7 +92,7 @@ class CylinderDrag:
 
         def objective(U, geo):
             F = wf.force(U, geo)
-            if not U.requires_grad:
+            if not torch.is_grad_enabled():  # the forward sweep (no_grad), not a gradient evaluation
                 forces.append(F.detach())
             return (F * e).sum()
 

@@ -154,6 +154,7 @@ class FRSolver:
         check(lib().zb_info_get(self.h, ctypes.byref(self.info)))
         self.nspts, self.nvars, self.neles = self.info.nspts, self.info.nvars, int(self.info.n_eles)
         self.ndims, self.nstages = self.info.ndims, self.info.nstages
+        self._stream = None  # caller stream given to set_stream
 
     # -- lifetime --
     @classmethod
@@ -188,12 +189,25 @@ class FRSolver:
         return (self.nvars * E, E, 1)
 
     # -- state --
-    @staticmethod
-    def _torch_ready():
+    def _torch_ready(self):
         """The library runs on its own stream: wait for torch's queued work
-        on a tensor before the library reads it."""
+        on a tensor before the library reads it (nothing to wait for when the
+        library was put on torch's current stream with set_stream)."""
         import torch
-        torch.cuda.current_stream().synchronize()
+        if not self._on_torch_stream():
+            torch.cuda.current_stream().synchronize()
+
+    def _on_torch_stream(self) -> bool:
+        if self._stream is None:
+            return False
+        import torch
+        return self._stream == torch.cuda.current_stream().cuda_stream
+
+    def _device_done(self) -> None:
+        """Device outputs complete for torch: a full wait only when the
+        library and torch use different streams."""
+        if not self._on_torch_stream():
+            self.synchronize()
 
     def set_state(self, U) -> None:
         if hasattr(U, "is_cuda") and U.is_cuda:
@@ -218,7 +232,7 @@ class FRSolver:
         """Copy the state into a contiguous float64 CUDA tensor of state_shape
         (complete on return)."""
         check(lib().zb_get_state(self.h, ctypes.cast(out.data_ptr(), _DP), *self._strides(), _lib.ZB_DEVICE))
-        self.synchronize()
+        self._device_done()
 
     # -- residual --
     def compute_residual(self, stage: int = 0) -> None:
@@ -237,7 +251,7 @@ class FRSolver:
         (complete on return)."""
         check(lib().zb_get_residual(self.h, stage, ctypes.cast(out.data_ptr(), _DP), *self._strides(),
                                     _lib.ZB_DEVICE))
-        self.synchronize()
+        self._device_done()
 
     def residual(self, U, stage: int = 0) -> np.ndarray:
         self.set_state(U)
@@ -327,7 +341,7 @@ class FRSolver:
             self._torch_ready()
             check(lib().zb_vjp(self.h, ctypes.cast(lam.data_ptr(), _DP), ctypes.cast(out.data_ptr(), _DP),
                                *self._strides(), _lib.ZB_DEVICE, pptr))
-            self.synchronize()
+            self._device_done()
         else:
             lam = np.ascontiguousarray(lam, dtype=np.float64)
             if lam.shape != self.state_shape:
@@ -377,7 +391,7 @@ class FRSolver:
         check(lib().zb_vjp_geometry_accumulate(self.h, ctypes.cast(lam.data_ptr(), _DP),
                                                ctypes.cast(out.data_ptr(), _DP), *self._strides(), _lib.ZB_DEVICE,
                                                pbar.ctypes.data_as(_DP)))
-        self.synchronize()
+        self._device_done()
         return out, pbar
 
     def geometry_adjoint(self, reset: bool = True) -> Dict[str, np.ndarray]:
@@ -393,6 +407,7 @@ class FRSolver:
 
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().zb_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+        self._stream = stream_ptr
 
     def synchronize(self) -> None:
         check(lib().zb_synchronize(self.h))
