@@ -95,7 +95,13 @@ class TrajectoryAdjoint:
         return (Us, Unew, Rs) if with_residuals else (Us, Unew)
 
     def _step(self, U: torch.Tensor) -> torch.Tensor:
-        return self._stages(U)[1]
+        """One RK44 step by the library's fused stages (the stepping the
+        forward objective runs use), back as a torch tensor."""
+        self.s.set_state(U)
+        self.s.step(1)
+        out = torch.empty_like(U)
+        self.s.get_state_device(out)
+        return out
 
     # -- reverse pieces --
     def _vjp(self, U: torch.Tensor, lam: torch.Tensor, pbar: np.ndarray, gbar=None) -> torch.Tensor:
