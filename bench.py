@@ -364,7 +364,8 @@ def cylinder_adjoint_side(nsteps: int = 500, every: int = 50):
     coef = np.zeros(16)
     coef[:4] = (0.01, -0.005, 0.003, 0.002)
     alpha = 0.05
-    prob.drag(coef, alpha, 2)  # warm-up
+    prob.drag(coef, alpha, 2)  # warm-ups of both paths (library, torch.func and allocator set-up)
+    prob.gradient(coef, alpha, 2)
     t0 = time.perf_counter()
     J = prob.drag(coef, alpha, nsteps)
     t_fwd = time.perf_counter() - t0

@@ -135,27 +135,28 @@ class TrajectoryAdjoint:
 
     @staticmethod
     def _obj_grad_batch(objective: Callable, Us: torch.Tensor, geo=None):
-        """Objective gradients for a stack of states Us [M,S,V,E] in one
-        vectorised evaluation (torch.func.vmap of the gradient): the state
-        gradients per state and, with ``geo``, the geometry gradient summed
-        over the stack.  Falls back to one autograd call per state when the
-        objective cannot be vectorised."""
+        """Objective values and gradients for a stack of states Us [M,S,V,E]
+        in one vectorised evaluation (torch.func.vmap of grad_and_value): the
+        sum of the values, the state gradients per state and, with ``geo``,
+        the geometry gradient summed over the stack.  Falls back to one
+        autograd call per state when the objective cannot be vectorised."""
         try:
-            from torch.func import grad, vmap
+            from torch.func import grad_and_value, vmap
             if geo is None:
-                gU = vmap(grad(objective))(Us)
-                return gU, None
+                gU, j = vmap(grad_and_value(objective))(Us)
+                return float(j.sum()), gU, None
             leaves = {k: v.detach() for k, v in geo.items()}
-            gU, gG = vmap(grad(objective, argnums=(0, 1)), in_dims=(0, None))(Us, leaves)
-            return gU, {k: v.sum(dim=0) for k, v in gG.items()}
+            (gU, gG), j = vmap(grad_and_value(objective, argnums=(0, 1)), in_dims=(0, None))(Us, leaves)
+            return float(j.sum()), gU, {k: v.sum(dim=0) for k, v in gG.items()}
         except Exception:  # noqa: BLE001 -- objective not vmap-able: per-state autograd
-            gUs, gsum = [], None
+            gUs, gsum, jsum = [], None, 0.0
             for U in Us:
-                _, gU, gG = TrajectoryAdjoint._obj_grad(objective, U, geo)
+                j, gU, gG = TrajectoryAdjoint._obj_grad(objective, U, geo)
+                jsum += j
                 gUs.append(gU)
                 if gG is not None:
                     gsum = gG if gsum is None else {k: gsum[k] + gG[k] for k in gsum}
-            return torch.stack(gUs), gsum
+            return jsum, torch.stack(gUs), gsum
 
     @staticmethod
     def _obj_grad(objective: Callable, U: torch.Tensor, geo=None):
@@ -169,26 +170,32 @@ class TrajectoryAdjoint:
         grads = torch.autograd.grad(j, [x] + list(leaves.values()))
         return float(j.detach()), grads[0], dict(zip(leaves, grads[1:]))
 
-    def run(self, U0, nsteps: int, objective: Callable, geometry=None) -> Dict[str, object]:
+    def run(self, U0, nsteps: int, objective: Callable, geometry=None,
+            observe: Optional[Callable] = None) -> Dict[str, object]:
         """Returns J, dJ/dU0 (CUDA tensor) and dJ/d(rho_fs, V_fs[0..2], P_fs).
 
         With ``geometry`` (a dict of the current metric tensors, as
         ``geometry.GeometryMap.metrics`` returns them), ``objective(U, geo)``
         also takes the metrics and the result adds ``dJ_dgeometry``: the
         gradient with respect to inv_jaco, jaco_det, norm and dA, summed over
-        the residual's adjoint, the RK update's 1/|J| and the objective."""
+        the residual's adjoint, the RK update's 1/|J| and the objective.
+
+        The forward sweep only steps (the library's fused RK44) and keeps
+        checkpoints; the objective is evaluated, with its gradients, on the
+        states the reverse sweep recomputes, a segment at a time.
+        ``observe(k, U)``, if given, sees every forward state U_k while the
+        solver holds it."""
         U = torch.as_tensor(U0, dtype=torch.float64).cuda().contiguous()
         checkpoints = {0: U.clone()}
-        obj = objective if geometry is None else (lambda x, geo=geometry: objective(x, geo))
         obj_grad_fn = objective
         J = 0.0
         with torch.no_grad():
             for k in range(1, nsteps + 1):
                 U = self._step(U)
-                J += float(obj(U))
+                if observe is not None:
+                    observe(k, U)
                 if k % self.every == 0:
                     checkpoints[k] = U.clone()
-        J /= nsteps
         # reverse sweep, one checkpointed segment at a time from the end
         Ubar = torch.zeros_like(U)
         pbar = np.zeros(5)
@@ -212,7 +219,8 @@ class TrajectoryAdjoint:
             chunk = max(1, (1 << 30) // max(1, last.numel() * last.element_size()))
             gUs = []
             for c0 in range(0, len(nexts), chunk):
-                gU, gGsum = self._obj_grad_batch(obj_grad_fn, torch.stack(nexts[c0:c0 + chunk]), geometry)
+                jsum, gU, gGsum = self._obj_grad_batch(obj_grad_fn, torch.stack(nexts[c0:c0 + chunk]), geometry)
+                J += jsum / nsteps
                 gUs.extend(gU.unbind(0))
                 if gGsum is not None:
                     for k in gbar:

@@ -91,14 +91,16 @@ class CylinderDrag:
         forces = []
 
         def objective(U, geo):
-            F = wf.force(U, geo)
-            if not torch.is_grad_enabled():  # the forward sweep (no_grad), not a gradient evaluation
-                forces.append(F.detach())
-            return (F * e).sum()
+            return (wf.force(U, geo) * e).sum()
+
+        def observe(k, U):
+            # the force of each step's state (held by the solver), for the drag
+            # direction's share of the angle derivative
+            forces.append(s.wall_force()["force"][:2])
 
         traj = TrajectoryAdjoint(s, self.dt, checkpoint_every=self.every)
         U0 = self.initial_state(s, alpha)
-        out = traj.run(U0, nsteps, objective, geometry=geo0)
+        out = traj.run(U0, nsteps, objective, geometry=geo0, observe=observe)
         # metrics -> nodes -> wall coefficients
         X = gm.nodes0.clone().requires_grad_(True)
         m = gm.metrics(X)
@@ -122,7 +124,7 @@ class CylinderDrag:
         dU0[:, 1, :] = dV[0]  # rho = 1
         dU0[:, 2, :] = dV[1]
         dalpha += float((gU0 * dU0).sum())
-        Fm = torch.stack(forces).mean(dim=0).cpu().numpy()
+        Fm = np.mean(forces, axis=0)
         dalpha += float(Fm[0] * -sn + Fm[1] * c)
         s.close()
         return {"J": out["J"], "dJ_dcoef": dcoef, "dJ_dalpha": dalpha}
