@@ -322,7 +322,8 @@ typedef struct zb_batch_config {
   double ms_per_step; /* autotuner: measured time of one RK44 step */
   int group;          /* threads per tile group (64, 128 or 256, dividing threads): a CTA
                          runs threads/group tiles at once */
-  int chunk;          /* consecutive work items a group takes at a time */
+  int chunk;          /* consecutive work items a group takes at a time; 0: one
+                         contiguous run per group */
 } zb_batch_config;
 
 zb_status zb_batch_create(zb_ctx *const *ctxs, int n, zb_batch **out);

@@ -37,7 +37,7 @@ def test_batch_matches_cases_stepped_alone(precision, graph):
         assert _same(s1.get_state(), s2.get_state(), precision)
 
 
-@pytest.mark.parametrize("shape", [(256, 256, 1), (128, 64, 1), (64, 64, 1), (256, 64, 8), (128, 128, 32)])
+@pytest.mark.parametrize("shape", [(256, 256, 1), (128, 64, 1), (64, 64, 1), (256, 64, 8), (128, 128, 32), (256, 64, 0)])
 def test_batch_launch_shapes_agree(shape):
     """Whole-CTA tiles (one group) and several tile groups per CTA (named
     barriers) compute the same stages."""

@@ -201,12 +201,22 @@ static void launch_order(Batch &b, unsigned st)
   const int n = b.oend[NN] - b.obeg[NN];
   if (n == 0) return;
   const int ng = b.cfg.threads / b.cfg.group;
-  const int blocks =
-      std::max(1, std::min((n + ng * b.cfg.chunk - 1) / (ng * b.cfg.chunk), b.cfg.blocks_per_sm * b.sms));
+  int chunk = b.cfg.chunk;
+  int blocks;
+  if (chunk == 0)
+  {
+    // contiguous: every group takes one run of consecutive items (the items
+    // of one order cost the same, so equal runs balance), which keeps a
+    // group's descriptor for a whole case
+    blocks = std::max(1, std::min((n + ng - 1) / ng, b.cfg.blocks_per_sm * b.sms));
+    chunk = (n + blocks * ng - 1) / (blocks * ng);
+  }
+  else
+    blocks = std::max(1, std::min((n + ng * chunk - 1) / (ng * chunk), b.cfg.blocks_per_sm * b.sms));
   CK(cudaStreamWaitEvent(b.ost[NN], b.efork, 0));
   k_batch_euler<T, A, NN><<<blocks, b.cfg.threads, ng * b.gstride[NN], b.ost[NN]>>>(
       (const BatchCase<T, A> *)b.cases[st], b.items, b.obeg[NN], b.oend[NN], b.cfg.group, (int)b.gstride[NN],
-      b.cfg.chunk);
+      chunk);
   b.launches++;
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ejoin[NN], b.ost[NN]));
@@ -407,7 +417,7 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
   const int shapes[][2] = {{64, 64}, {128, 64}, {128, 128}, {256, 64}, {256, 128}, {256, 256}};
   const int bps[] = {2, 4, 8, 16};
   const int orders[] = {0, 1};
-  const int chunks[] = {1, 8, 32};
+  const int chunks[] = {0, 1, 8, 32};  // 0: one contiguous run per group
   zb_batch_config best{0, 0, 0, 1e300, 0, 1};
   for (int order : orders)
   {
@@ -464,7 +474,7 @@ void batch_config(Batch *b, const zb_batch_config *cfg)
     ZB_THROW(ZB_ERR_ARG, "group must be a multiple of 32, at least 64, dividing threads");
   if (cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 64) ZB_THROW(ZB_ERR_ARG, "blocks_per_sm out of range");
   if (cfg->order != 0 && cfg->order != 1) ZB_THROW(ZB_ERR_ARG, "order must be 0 or 1");
-  if (cfg->chunk < 1) ZB_THROW(ZB_ERR_ARG, "chunk must be at least 1");
+  if (cfg->chunk < 0) ZB_THROW(ZB_ERR_ARG, "chunk must be 0 (contiguous runs) or positive");
   CK(cudaStreamSynchronize(b->stream));
   b->cfg = *cfg;
   build_items(*b, cfg->order);
