@@ -302,6 +302,20 @@ zb_status zb_vjp_geometry(zb_ctx *ctx, const double *lam, double *Ubar, int64_t 
  * (for unsteady adjoints, one call per RK stage without host copies);
  * zb_geometry_adjoint_get copies the sums out in the zb_vjp_geometry layouts
  * and, with reset != 0, clears them.  No reference counterpart. */
+/* Reverse of one RK44 step U1 = step(U0) of FRSolver::step_RK (plain FP64
+ * form), for unsteady adjoints: given the step's start state U0 and the
+ * adjoint Ubar1 of its end state, Ubar0 = (d U1 / d U0)^T Ubar1, with the
+ * four stage states and residuals recomputed on the device (RK44 tables of
+ * src/solver.cpp:722-735).  param_bar (host,
+ * 5 values, may be NULL) gets the free-stream adjoint added; with geometry
+ * != 0 the metric adjoint of the stage residuals and of the update's 1/|J|
+ * is added to the device sums zb_geometry_adjoint_get reads.  Uses the
+ * context's fixed dt (zb_set_dt; ZB_ERR_UNSUPPORTED under RK54 or a CFL
+ * step); leaves the context's state undefined.  No reference
+ * counterpart. */
+zb_status zb_rk_step_vjp(zb_ctx *ctx, const double *U0, const double *Ubar1, double *Ubar0, int64_t spt_stride,
+                         int64_t var_stride, int64_t ele_stride, int where, double *param_bar, int geometry);
+
 zb_status zb_vjp_geometry_accumulate(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride,
                                      int64_t var_stride, int64_t ele_stride, int where, double *param_bar);
 zb_status zb_geometry_adjoint_get(zb_ctx *ctx, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar,

@@ -32,6 +32,43 @@ def test_residual_backward_is_the_library_adjoint():
     assert np.array_equal(U.grad.cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "cyl_p3_ns_char_adi"])
+def test_rk_step_vjp_equals_composed_stage_adjoints(name):
+    """zb_rk_step_vjp against the RK44 transpose written out here from the
+    residual adjoint (zb_vjp) and the stage tables of src/solver.cpp:722-735:
+    U_{s+1} = U_0 - a_s dt/|J| R(U_s), U_new = U_0 - dt/|J| sum_s b_s R(U_s).
+    Same kernels in a different order of sums: 1e-12 relative."""
+    g = gc.load(name)
+    s = solver_for(g)
+    dt = 1e-3 if "vortex" in name else 2e-4
+    s.set_dt(dt)
+    S, V, E = s.state_shape
+    inv_det = torch.from_numpy(1.0 / s.plan.get("jaco_det_spts").reshape(S, 1, E)).cuda()
+    alpha, beta = (0.5, 0.5, 1.0), (1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0)
+    U0 = torch.from_numpy(g.U0).cuda()
+    Us = [U0]
+    for a in alpha:
+        Us.append(U0 - a * dt * inv_det * zag.residual(Us[-1], s))
+    rng = np.random.default_rng(11)
+    ub = torch.from_numpy(rng.standard_normal(g.U0.shape)).cuda()
+    ub0, ub_next, pref = ub.clone(), None, np.zeros(5)
+    for st in range(3, -1, -1):
+        lam = -beta[st] * dt * inv_det * ub
+        if ub_next is not None:
+            lam = lam - alpha[st] * dt * inv_det * ub_next
+        s.set_state(Us[st])
+        ubs, p = s.vjp(lam.contiguous(), params=True)
+        pref += p
+        ub0 = ub0 + ubs
+        ub_next = ubs
+    pbar = np.zeros(5)
+    got = s.rk_step_vjp(U0, ub, pbar)
+    ref = ub0.cpu().numpy()
+    err = np.abs(got.cpu().numpy() - ref).max() / np.abs(ref).max()
+    assert err <= 1e-12, err
+    assert np.allclose(pbar, pref, rtol=1e-12, atol=1e-12 * np.abs(pref).max())
+
+
 def _fd_objective(traj, U0, v, h, nsteps, obj):
     vals = []
     for sgn in (1.0, -1.0):

@@ -5,8 +5,10 @@ library's hand-written adjoint (``zb_vjp``), never a PyTorch trace of the
 kernels.  ``TrajectoryAdjoint`` differentiates a time-averaged objective over
 RK44 steps (``FRSolver::step_RK`` with the RK44 tables of src/solver.cpp:
 722-735) with respect to the initial state and the free-stream state, storing
-a checkpoint every ``checkpoint_every`` steps and recomputing the stage states
-of each segment during the reverse sweep.
+a checkpoint every ``checkpoint_every`` steps and recomputing the states of
+each segment during the reverse sweep; each step's transpose is one library
+call (``zb_rk_step_vjp``) that re-runs the four stages and applies their
+adjoints on the device.
 
 Everything is plain FP64 on the device: the adjoint exists for ZB_FP64
 contexts only.
@@ -19,11 +21,6 @@ import numpy as np
 import torch
 
 from .solver import FRSolver
-
-# RK44 of FRSolver::step_RK: stage states U_{s+1} = U_0 - a_s dt/|J| R_s,
-# update U_new = U_0 - dt/|J| sum_s b_s R_s
-RK_ALPHA = (0.5, 0.5, 1.0)
-RK_BETA = (1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0)
 
 
 class _Residual(torch.autograd.Function):
@@ -69,31 +66,9 @@ class TrajectoryAdjoint:
         self.s = solver
         self.dt = float(dt)
         self.every = int(checkpoint_every)
-        S, V, E = solver.state_shape
-        self.inv_det = (1.0 / _device_array(solver, "jaco_det_spts", (S, E))).reshape(S, 1, E)
         solver.set_dt(self.dt)
 
     # -- forward pieces --
-    def _residual(self, U: torch.Tensor) -> torch.Tensor:
-        self.s.set_state(U)
-        self.s.compute_residual(0)
-        R = torch.empty_like(U)
-        self.s.get_residual_device(R, 0)
-        return R
-
-    def _stages(self, U0: torch.Tensor, with_residuals: bool = False):
-        """Stage states U^(0..3) of one RK44 step and the updated state (and
-        the stage residuals)."""
-        Us, Rs = [U0], []
-        for s in range(4):
-            Rs.append(self._residual(Us[s]))
-            if s < 3:
-                Us.append(U0 - RK_ALPHA[s] * self.dt * self.inv_det * Rs[s])
-        Unew = U0.clone()
-        for s in range(4):
-            Unew = Unew - RK_BETA[s] * self.dt * self.inv_det * Rs[s]
-        return (Us, Unew, Rs) if with_residuals else (Us, Unew)
-
     def _step(self, U: torch.Tensor) -> torch.Tensor:
         """One RK44 step by the library's fused stages (the stepping the
         forward objective runs use), back as a torch tensor."""
@@ -104,34 +79,13 @@ class TrajectoryAdjoint:
         return out
 
     # -- reverse pieces --
-    def _vjp(self, U: torch.Tensor, lam: torch.Tensor, pbar: np.ndarray, gbar=None) -> torch.Tensor:
-        self.s.set_state(U)
-        if gbar is None:
-            g, p = self.s.vjp(lam.contiguous(), params=True)
-            pbar += p
-            return g
-        # geometry adjoint summed on the device by the library
-        g, p = self.s.vjp_geometry_accumulate(lam)
-        pbar += p
-        return g
-
     def _step_adjoint(self, U0: torch.Tensor, Ubar_new: torch.Tensor, pbar: np.ndarray, gbar=None) -> torch.Tensor:
-        Us, _, Rs = self._stages(U0, with_residuals=True)
-        Ubar0 = Ubar_new.clone()
-        Rbar = [-RK_BETA[s] * self.dt * self.inv_det * Ubar_new for s in range(4)]
-        inv2 = (self.inv_det * self.inv_det)[:, 0, :]
-        for s in range(3, 0, -1):
-            Ubar_s = self._vjp(Us[s], Rbar[s], pbar, gbar)
-            Ubar0 += Ubar_s
-            Rbar[s - 1] = Rbar[s - 1] - RK_ALPHA[s - 1] * self.dt * self.inv_det * Ubar_s
-            if gbar is not None:
-                # U^(s) = U0 - a dt R_{s-1} / |J|
-                gbar["jaco_det"] += RK_ALPHA[s - 1] * self.dt * (Ubar_s * Rs[s - 1]).sum(dim=1) * inv2
-        Ubar0 += self._vjp(Us[0], Rbar[0], pbar, gbar)
-        if gbar is not None:
-            Rsum = sum(RK_BETA[s] * Rs[s] for s in range(4))
-            gbar["jaco_det"] += self.dt * (Ubar_new * Rsum).sum(dim=1) * inv2
-        return Ubar0
+        """(dU1/dU0)^T Ubar_new for the RK44 step from U0: one library call
+        (zb_rk_step_vjp) that recomputes the four stages and applies the four
+        stage adjoints with the RK weights on the device; with ``gbar`` the
+        metric adjoint (residuals and the update's 1/|J|) goes to the
+        library's device-side sums."""
+        return self.s.rk_step_vjp(U0, Ubar_new, pbar, geometry=gbar is not None)
 
     @staticmethod
     def _obj_grad_batch(objective: Callable, Us: torch.Tensor, geo=None):

@@ -341,6 +341,16 @@ zb_status zb_get_element_dt(zb_ctx *ctx, double *out)
   })
 }
 
+zb_status zb_rk_step_vjp(zb_ctx *ctx, const double *U0, const double *Ubar1, double *Ubar0, int64_t spt_stride,
+                         int64_t var_stride, int64_t ele_stride, int where, double *param_bar, int geometry)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_rk_step_vjp(ctx->impl, U0, Ubar1, Ubar0, spt_stride, var_stride, ele_stride, where, param_bar,
+                        geometry != 0);
+  })
+}
+
 zb_status zb_residual_norms(zb_ctx *ctx, double *out)
 {
   ZB_GUARD({

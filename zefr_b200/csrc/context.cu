@@ -505,7 +505,7 @@ static void free_all(Ctx *c)
                   c->Ufp[1], c->Fvn, c->Fcom, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
                   c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubx, c->Ubar, c->pbar, c->dops, c->dwall,
                   c->mbar, c->gbar, c->nbx, c->mbar_acc, c->gbar_acc, c->d_dt, c->dt_ele, c->h_ref, c->evol,
-                  c->dfw, c->U_til, c->rk_err};
+                  c->dfw, c->U_til, c->rk_err, c->rkv};
   for (void *b : bufs)
     if (b) cudaFree(b);
   for (auto &r : c->recs)
@@ -977,18 +977,11 @@ void ctx_geometry_adjoint_get(Ctx *c, double *inv_jaco_bar, double *jaco_det_bar
   }
 }
 
-void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, int64_t es, int where,
-             double *param_bar, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar, double *dA_bar,
-             bool accumulate)
+static void ensure_adjoint_buffers(Ctx *c)
 {
-  const bool geo_out = inv_jaco_bar || jaco_det_bar || norm_bar || dA_bar;
-  if (geo_out && !(inv_jaco_bar && jaco_det_bar && norm_bar && dA_bar))
-    ZB_THROW(ZB_ERR_ARG, "the geometry adjoint needs all four output arrays");
-  const bool geo = geo_out || accumulate;
   if (c->prec != ZB_FP64) ZB_THROW(ZB_ERR_UNSUPPORTED, "the adjoint is built for the plain FP64 form only");
   if (!c->launch_vjp)
     ZB_THROW(ZB_ERR_UNSUPPORTED, "no adjoint kernels for ndims=" + std::to_string(c->D) + " P=" + std::to_string(c->N - 1));
-  if (!lam || !Ubar) ZB_THROW(ZB_ERR_ARG, "null adjoint buffer");
   const size_t nU = (size_t)c->ntiles * c->S * c->V * TW;
   const size_t nF = (size_t)c->ntiles * c->Fp * c->V * TW;
   if (!c->lam)
@@ -1005,16 +998,14 @@ void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, in
       c->Ubx = (double *)dalloc(nF * sizeof(double));
     }
   }
-  const size_t ext = extent(c, ss, vs, es, c->S);
-  const double *src = stage_in(c, lam, ext, where);
-  {
-    const int64_t work = c->ntiles * c->S * c->V * TW;
-    ProfScope ps(*c, ZB_K_TO_TILES);
-    k_to_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>(src, c->lam, nullptr, nullptr, c->plan.neles,
-                                                                     c->ntiles, c->S, c->V, ss, vs, es);
-    c->launches++;
-    CK(cudaGetLastError());
-  }
+}
+
+// The adjoint of the residual at the context's current state for the weight
+// already in c->lam (tile layout), into c->Ubar; optionally the free-stream
+// adjoint (host, summed over tiles) and the geometry adjoint (c->mbar /
+// c->gbar, added to the device sums with `accumulate`).
+static void vjp_tiles(Ctx *c, double *param_bar, bool geo, bool accumulate)
+{
   // linearisation point: the current state and its traces
   c->ufp_valid = false;
   ensure_ufp(c);
@@ -1036,7 +1027,6 @@ void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, in
     }
   }
   c->launch_vjp(*c, param_bar != nullptr, geo);
-  from_tiles(c, c->Ubar, nullptr, nullptr, Ubar, ss, vs, es, where);
   if (accumulate)
   {
     const size_t nm = (size_t)c->ntiles * c->S * NM * TW, ng = (size_t)c->ntiles * c->Fp * (c->D + 1) * TW;
@@ -1052,7 +1042,6 @@ void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, in
     c->launches += 2;
     CK(cudaGetLastError());
   }
-  if (geo_out) geo_to_reference(c, c->mbar, c->gbar, inv_jaco_bar, jaco_det_bar, norm_bar, dA_bar);
   if (param_bar)
   {
     std::vector<double> h((size_t)c->ntiles * 5);
@@ -1063,6 +1052,192 @@ void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, in
     for (int64_t t = 0; t < c->ntiles; t++)
       for (int k = 0; k < 5; k++) param_bar[k] += h[(size_t)t * 5 + k];
   }
+}
+
+void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, int64_t es, int where,
+             double *param_bar, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar, double *dA_bar,
+             bool accumulate)
+{
+  const bool geo_out = inv_jaco_bar || jaco_det_bar || norm_bar || dA_bar;
+  if (geo_out && !(inv_jaco_bar && jaco_det_bar && norm_bar && dA_bar))
+    ZB_THROW(ZB_ERR_ARG, "the geometry adjoint needs all four output arrays");
+  const bool geo = geo_out || accumulate;
+  ensure_adjoint_buffers(c);
+  if (!lam || !Ubar) ZB_THROW(ZB_ERR_ARG, "null adjoint buffer");
+  const size_t ext = extent(c, ss, vs, es, c->S);
+  const double *src = stage_in(c, lam, ext, where);
+  {
+    const int64_t work = c->ntiles * c->S * c->V * TW;
+    ProfScope ps(*c, ZB_K_TO_TILES);
+    k_to_tiles<double><<<grid_for(work, 256), 256, 0, c->stream>>>(src, c->lam, nullptr, nullptr, c->plan.neles,
+                                                                     c->ntiles, c->S, c->V, ss, vs, es);
+    c->launches++;
+    CK(cudaGetLastError());
+  }
+  vjp_tiles(c, param_bar, geo, accumulate);
+  from_tiles(c, c->Ubar, nullptr, nullptr, Ubar, ss, vs, es, where);
+  if (geo_out) geo_to_reference(c, c->mbar, c->gbar, inv_jaco_bar, jaco_det_bar, norm_bar, dA_bar);
+}
+
+// ---------------------------------------------------------------------------
+// reverse of one RK44 step (tile layout, FP64)
+// ---------------------------------------------------------------------------
+
+// out = a - (c * (1/|J|)) * r per point (the RK stage update)
+__global__ void k_stage_state(double *__restrict__ out, const double *__restrict__ a, const double *__restrict__ r,
+                              const double *__restrict__ mets, double c, int64_t ntiles, int S, int V, int NM, int DD)
+{
+  const int64_t total = ntiles * S * V * TW;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int l = (int)(i % TW);
+    const int64_t ps = i / ((int64_t)TW * V);
+    const double inv = 1.0 / mets[(ps * NM + DD) * TW + l];
+    out[i] = a[i] - c * inv * r[i];
+  }
+}
+
+// lam = cb * (1/|J|) * ubar1 [+ ca * (1/|J|) * ubs]: the stage residual's
+// adjoint weight (cb = -b_s dt, ca = -a_s dt)
+__global__ void k_stage_weight(double *__restrict__ lam, const double *__restrict__ ubar1,
+                               const double *__restrict__ ubs, const double *__restrict__ mets, double cb, double ca,
+                               int64_t ntiles, int S, int V, int NM, int DD)
+{
+  const int64_t total = ntiles * S * V * TW;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int l = (int)(i % TW);
+    const int64_t ps = i / ((int64_t)TW * V);
+    const double inv = 1.0 / mets[(ps * NM + DD) * TW + l];
+    double w = cb * inv * ubar1[i];
+    if (ubs) w = w + ca * inv * ubs[i];
+    lam[i] = w;
+  }
+}
+
+// |J| part of the geometry adjoint from the update's 1/|J|:
+// acc(|J|) += c * sum_v x_v y_v / |J|^2, and acc(U) += u (state adjoint sum)
+__global__ void k_det_adjoint(double *__restrict__ mbar_acc, const double *__restrict__ x,
+                              const double *__restrict__ y, const double *__restrict__ mets, double c, int64_t ntiles,
+                              int S, int V, int NM, int DD)
+{
+  const int64_t total = ntiles * S * TW;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+  {
+    const int l = (int)(i % TW);
+    const int64_t ps = i / TW;  // tile * S + s
+    const double det = mets[(ps * NM + DD) * TW + l];
+    const double inv = 1.0 / det;
+    double acc = 0.0;
+    for (int v = 0; v < V; v++) acc += x[(ps * V + v) * TW + l] * y[(ps * V + v) * TW + l];
+    mbar_acc[(ps * NM + DD) * TW + l] += c * acc * (inv * inv);
+  }
+}
+
+__global__ void k_add(double *__restrict__ a, const double *__restrict__ b, int64_t n)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    a[i] += b[i];
+}
+
+void ctx_rk_step_vjp(Ctx *c, const double *U0, const double *Ubar1, double *Ubar0, int64_t ss, int64_t vs,
+                     int64_t es, int where, double *param_bar, bool geometry)
+{
+  if (!U0 || !Ubar1 || !Ubar0) ZB_THROW(ZB_ERR_ARG, "null state or adjoint buffer");
+  if (c->nstages != 4) ZB_THROW(ZB_ERR_UNSUPPORTED, "the step adjoint is built for RK44");
+  if (c->use_dt_dev || c->use_dt_ele)
+    ZB_THROW(ZB_ERR_UNSUPPORTED, "the step adjoint takes the fixed step of set_dt (dt_type 0)");
+  ensure_adjoint_buffers(c);
+  const int64_t nU = c->ntiles * c->S * c->V * TW;
+  const int S = c->S, V = c->V, NM = c->D * c->D + 1, DD = c->D * c->D;
+  const unsigned grid = grid_for(nU, 256);
+  if (!c->rkv)
+  {
+    // stage states 0..3, stage residuals 0..3, the end state's adjoint, one
+    // stage adjoint and the running result, in the tile layout
+    c->rkv = (double *)dalloc((size_t)11 * nU * sizeof(double));
+  }
+  double *Us[4], *Rs[4];
+  for (int s = 0; s < 4; s++)
+  {
+    Us[s] = c->rkv + (size_t)s * nU;
+    Rs[s] = c->rkv + (size_t)(4 + s) * nU;
+  }
+  double *ub1 = c->rkv + (size_t)8 * nU, *ubs = c->rkv + (size_t)9 * nU, *ub0 = c->rkv + (size_t)10 * nU;
+  const double dt = c->dt;
+  // inputs to the tile layout
+  {
+    const size_t ext = extent(c, ss, vs, es, c->S);
+    const double *src = stage_in(c, U0, ext, where);
+    k_to_tiles<double><<<grid, 256, 0, c->stream>>>(src, Us[0], nullptr, nullptr, c->plan.neles, c->ntiles, S, V, ss,
+                                                    vs, es);
+    src = stage_in(c, Ubar1, ext, where);
+    k_to_tiles<double><<<grid, 256, 0, c->stream>>>(src, ub1, nullptr, nullptr, c->plan.neles, c->ntiles, S, V, ss,
+                                                    vs, es);
+    c->launches += 2;
+    CK(cudaGetLastError());
+  }
+  // forward: the stage states and residuals (FRSolver::step_RK's stages)
+  for (int s = 0; s < 4; s++)
+  {
+    CK(cudaMemcpyAsync(c->U, Us[s], (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    c->ufp_valid = false;
+    ensure_ufp(c);
+    StageCfg sc{0, 0, 0, 0};
+    c->launch_stage(*c, sc);
+    CK(cudaMemcpyAsync(Rs[s], c->divF[0], (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    if (s < 3)
+    {
+      k_stage_state<<<grid, 256, 0, c->stream>>>(Us[s + 1], Us[0], Rs[s], (const double *)c->mets, kRkAlpha[s] * dt,
+                                                 c->ntiles, S, V, NM, DD);
+      c->launches++;
+      CK(cudaGetLastError());
+    }
+  }
+  // reverse: Ubar0 = Ubar1 + sum_s (dR_s/dU_s)^T lam_s with the stage weights
+  // lam_s = -b_s dt/|J| Ubar1 - a_s dt/|J| Ubar_{s+1}
+  CK(cudaMemcpyAsync(ub0, ub1, (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  double pacc[5] = {0, 0, 0, 0, 0};
+  for (int s = 3; s >= 0; s--)
+  {
+    k_stage_weight<<<grid, 256, 0, c->stream>>>(c->lam, ub1, s < 3 ? ubs : nullptr, (const double *)c->mets,
+                                                -kRkBeta[s] * dt, s < 3 ? -kRkAlpha[s] * dt : 0.0, c->ntiles, S, V,
+                                                NM, DD);
+    c->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->U, Us[s], (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    double pb[5];
+    vjp_tiles(c, param_bar ? pb : nullptr, geometry, geometry);
+    if (param_bar)
+      for (int k = 0; k < 5; k++) pacc[k] += pb[k];
+    CK(cudaMemcpyAsync(ubs, c->Ubar, (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    k_add<<<grid, 256, 0, c->stream>>>(ub0, ubs, nU);
+    c->launches++;
+    CK(cudaGetLastError());
+    if (geometry && s > 0)
+    {
+      // U_s = U_0 - a_{s-1} dt R_{s-1} / |J|
+      k_det_adjoint<<<grid_for(c->ntiles * S * TW, 256), 256, 0, c->stream>>>(
+          c->mbar_acc, ubs, Rs[s - 1], (const double *)c->mets, kRkAlpha[s - 1] * dt, c->ntiles, S, V, NM, DD);
+      c->launches++;
+      CK(cudaGetLastError());
+    }
+  }
+  if (geometry)
+  {
+    // U_1 = U_0 - dt sum_s b_s R_s / |J|
+    for (int s = 0; s < 4; s++)
+    {
+      k_det_adjoint<<<grid_for(c->ntiles * S * TW, 256), 256, 0, c->stream>>>(
+          c->mbar_acc, ub1, Rs[s], (const double *)c->mets, kRkBeta[s] * dt, c->ntiles, S, V, NM, DD);
+      c->launches++;
+      CK(cudaGetLastError());
+    }
+  }
+  if (param_bar)
+    for (int k = 0; k < 5; k++) param_bar[k] += pacc[k];
+  from_tiles(c, ub0, nullptr, nullptr, Ubar0, ss, vs, es, where);
+  c->ufp_valid = false;
 }
 
 void ctx_wall_force(Ctx *c, double *out)

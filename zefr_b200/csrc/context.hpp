@@ -46,6 +46,9 @@ void ctx_wall_force(Ctx *c, double *out);
 void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, int64_t es, int where,
              double *param_bar, double *inv_jaco_bar = nullptr, double *jaco_det_bar = nullptr,
              double *norm_bar = nullptr, double *dA_bar = nullptr, bool accumulate = false);
+// reverse of one RK44 step with recomputed stages (zb_rk_step_vjp)
+void ctx_rk_step_vjp(Ctx *c, const double *U0, const double *Ubar1, double *Ubar0, int64_t ss, int64_t vs,
+                     int64_t es, int where, double *param_bar, bool geometry);
 void ctx_geometry_adjoint_get(Ctx *c, double *inv_jaco_bar, double *jaco_det_bar, double *norm_bar, double *dA_bar,
                               int reset);
 void ctx_profile_read(Ctx *c, double *ms, int64_t *count);

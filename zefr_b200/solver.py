@@ -394,6 +394,27 @@ class FRSolver:
         self._device_done()
         return out, pbar
 
+    def rk_step_vjp(self, U0, Ubar1, pbar: Optional[np.ndarray] = None, geometry: bool = False):
+        """Reverse of one RK44 step from U0 (CUDA tensors of state_shape):
+        returns (dU1/dU0)^T Ubar1, adds the free-stream adjoint to ``pbar``
+        (5 values) and, with ``geometry``, the metric adjoint to the
+        device-side sums of :meth:`geometry_adjoint`.  Stage states and
+        residuals are recomputed in the library (zb_rk_step_vjp)."""
+        import torch
+        U0 = U0.to(torch.float64).contiguous()
+        Ubar1 = Ubar1.to(torch.float64).contiguous()
+        assert tuple(U0.shape) == self.state_shape and tuple(Ubar1.shape) == self.state_shape
+        out = torch.empty_like(U0)
+        p = np.zeros(5)
+        self._torch_ready()
+        check(lib().zb_rk_step_vjp(self.h, ctypes.cast(U0.data_ptr(), _DP), ctypes.cast(Ubar1.data_ptr(), _DP),
+                                   ctypes.cast(out.data_ptr(), _DP), *self._strides(), _lib.ZB_DEVICE,
+                                   p.ctypes.data_as(_DP), 1 if geometry else 0))
+        self._device_done()
+        if pbar is not None:
+            pbar += p
+        return out
+
     def geometry_adjoint(self, reset: bool = True) -> Dict[str, np.ndarray]:
         """The summed geometry adjoint of vjp_geometry_accumulate (host arrays)."""
         S, V, E = self.state_shape
