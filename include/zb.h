@@ -179,8 +179,9 @@ zb_status zb_plan_info(const zb_plan *plan, zb_info *out);
  * fpt_slot, fpt_norm (left-element normal per element fpt [fpt][dim][ele]),
  * fpt_dA, coord_fpts, weights_spts, loc_spts, loc_fpts, tnorm ([fpt][dim]
  * reference normals), dshape_spts [dim][spt][node], dshape_fpts
- * [dim][fpt][node], shape_fpts [fpt][node] (shape functions, gmsh node order;
- * for geometry derivatives).  With out == NULL, *n receives the element count. */
+ * [dim][fpt][node], shape_fpts [fpt][node], shape_spts [spt][node] (shape
+ * functions, gmsh node order; for geometry derivatives), nodes
+ * [node][dim][ele] (element node coordinates, Elements::nodes).  With out == NULL, *n receives the element count. */
 zb_status zb_plan_get(const zb_plan *plan, const char *name, double *out, int64_t *n);
 
 /* Create a device context from a plan on the current device. */
@@ -315,6 +316,32 @@ zb_status zb_vjp_geometry(zb_ctx *ctx, const double *lam, double *Ubar, int64_t 
  * counterpart. */
 zb_status zb_rk_step_vjp(zb_ctx *ctx, const double *U0, const double *Ubar1, double *Ubar0, int64_t spt_stride,
                          int64_t var_stride, int64_t ele_stride, int where, double *param_bar, int geometry);
+
+/* Element geometry from element node coordinates, on the device: the set-up's
+ * calc_transforms and calc_normals (src/elements.cpp:845-996; GPU forms
+ * src/elements_kernels.cu:1649-1737, 1896-1950).  nodes[nNodes][D][E] is the
+ * reference's Elements::nodes layout (zb_plan_get "nodes"); outputs in the
+ * zb_vjp_geometry layouts: inv_jaco[D][S][D][E] (adjugate), jaco_det[S][E],
+ * norm[Fp][D][E] (the left element's unit normal on both sides of a face),
+ * dA[Fp][E] (each side's own).  For the context's own nodes the results
+ * equal the set-up's bit for bit.  Every pointer is host or device memory as
+ * `where` says.  No reference counterpart as an entry point. */
+zb_status zb_geometry_eval(zb_ctx *ctx, const double *nodes, double *inv_jaco, double *jaco_det, double *norm,
+                           double *dA, int where);
+/* Adjoint of zb_geometry_eval at `nodes`: nodes_bar[nNodes][D][E] from the
+ * adjoints of the four arrays (as zb_vjp_geometry / zb_geometry_adjoint_get
+ * return them; a NULL adjoint counts as zero).  Deterministic. */
+zb_status zb_geometry_eval_vjp(zb_ctx *ctx, const double *nodes, const double *inv_jaco_bar,
+                               const double *jaco_det_bar, const double *norm_bar, const double *dA_bar,
+                               double *nodes_bar, int where);
+/* Moves the context's mesh: new element node coordinates (same layout) give
+ * new metrics on the device in the context's precision form, with the
+ * coordinates, volumes and CFL line lengths that depend on them; the state,
+ * the connectivity and the plan handle are unchanged.  The role of the
+ * reference's moving-grid metric updates (update_transforms_rigid_wrapper,
+ * src/elements_kernels.cu:1840-1895) for arbitrary node motion.
+ * ZB_ERR_MESH (context unchanged) if a solution point's |J| turns negative. */
+zb_status zb_set_nodes(zb_ctx *ctx, const double *nodes, int where);
 
 zb_status zb_vjp_geometry_accumulate(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride,
                                      int64_t var_stride, int64_t ele_stride, int where, double *param_bar);

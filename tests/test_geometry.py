@@ -1,6 +1,7 @@
 """Torch restatements used by the shape adjoint, on the CPU: the set-up
-metrics as functions of the node coordinates must reproduce the plan's, and
-the wall force must equal the oracle's compute_moments restatement."""
+metrics as functions of the node coordinates (the checker of the library's
+geometry kernels) must reproduce the plan's, and the wall force must equal
+the oracle's compute_moments restatement."""
 import numpy as np
 import pytest
 
@@ -11,6 +12,7 @@ from zefr_b200.solver import Plan, make_params
 torch = pytest.importorskip("torch")
 
 from zefr_b200 import geometry  # noqa: E402
+from geometry_restatement import GeometryRestatement  # noqa: E402
 
 
 class _PlanView:
@@ -27,7 +29,7 @@ class _PlanView:
 def test_geometry_map_reproduces_plan_metrics(name):
     g = gc.load(name)
     v = _PlanView(g)
-    gm = geometry.GeometryMap(v, g.mesh, device="cpu")
+    gm = GeometryRestatement(v, g.mesh, device="cpu")
     m = gm.metrics(gm.nodes0)
     for key, arr in (("inv_jaco", "inv_jaco_spts"), ("jaco_det", "jaco_det_spts"), ("norm", "fpt_norm"),
                      ("dA", "fpt_dA")):
@@ -40,7 +42,7 @@ def test_geometry_map_reproduces_plan_metrics(name):
 def test_torch_wall_force_matches_oracle(name):
     g = gc.load(name)
     v = _PlanView(g)
-    gm = geometry.GeometryMap(v, g.mesh, device="cpu")
+    gm = GeometryRestatement(v, g.mesh, device="cpu")
     wf = geometry.WallForce(v, g.params, device="cpu")
     F = wf.force(torch.from_numpy(g.U0), gm.metrics(gm.nodes0)).numpy()
     st = g.setup()

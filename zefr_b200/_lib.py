@@ -38,6 +38,7 @@ EXPORTED = [
     "zb_batch_create", "zb_batch_destroy", "zb_batch_autotune", "zb_batch_set_config", "zb_batch_step",
     "zb_batch_stage", "zb_batch_synchronize", "zb_batch_launch_count",
     "zb_time_scheme_defaults", "zb_set_time_scheme", "zb_time_state", "zb_get_element_dt", "zb_rk_step_vjp",
+    "zb_geometry_eval", "zb_geometry_eval_vjp", "zb_set_nodes",
 ]
 ZB_RK44, ZB_RK54 = 0, 1
 ZB_NKERNELS = 11
@@ -169,6 +170,9 @@ def lib() -> ctypes.CDLL:
         L.zb_time_state.argtypes = [vp, dp, dp, ctypes.POINTER(i64), dp]
         L.zb_get_element_dt.argtypes = [vp, dp]
         L.zb_rk_step_vjp.argtypes = [vp, dp, dp, dp, i64, i64, i64, ctypes.c_int, dp, ctypes.c_int]
+        L.zb_geometry_eval.argtypes = [vp, dp, dp, dp, dp, dp, ctypes.c_int]
+        L.zb_geometry_eval_vjp.argtypes = [vp, dp, dp, dp, dp, dp, dp, ctypes.c_int]
+        L.zb_set_nodes.argtypes = [vp, dp, ctypes.c_int]
         _lib = L
     return _lib
 

@@ -163,6 +163,8 @@ zb_status zb_plan_get(const zb_plan *plan, const char *name, double *out, int64_
     else if (nm == "dshape_spts") put(p.dshape_spts);
     else if (nm == "dshape_fpts") put(p.dshape_fpts);
     else if (nm == "shape_fpts") put(p.shape_fpts);
+    else if (nm == "shape_spts") put(p.shape_spts);
+    else if (nm == "nodes") put(p.nodes);
     else if (nm == "fpt_partner")
     {
       tmp.assign(p.partner.begin(), p.partner.end());
@@ -348,6 +350,33 @@ zb_status zb_rk_step_vjp(zb_ctx *ctx, const double *U0, const double *Ubar1, dou
     ZB_REQUIRE(ctx, "null context");
     zb::ctx_rk_step_vjp(ctx->impl, U0, Ubar1, Ubar0, spt_stride, var_stride, ele_stride, where, param_bar,
                         geometry != 0);
+  })
+}
+
+zb_status zb_geometry_eval(zb_ctx *ctx, const double *nodes, double *inv_jaco, double *jaco_det, double *norm,
+                           double *dA, int where)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_geometry_eval(ctx->impl, nodes, inv_jaco, jaco_det, norm, dA, where);
+  })
+}
+
+zb_status zb_geometry_eval_vjp(zb_ctx *ctx, const double *nodes, const double *inv_jaco_bar,
+                               const double *jaco_det_bar, const double *norm_bar, const double *dA_bar,
+                               double *nodes_bar, int where)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_geometry_eval_vjp(ctx->impl, nodes, inv_jaco_bar, jaco_det_bar, norm_bar, dA_bar, nodes_bar, where);
+  })
+}
+
+zb_status zb_set_nodes(zb_ctx *ctx, const double *nodes, int where)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_set_nodes(ctx->impl, nodes, where);
   })
 }
 

@@ -505,7 +505,7 @@ static void free_all(Ctx *c)
                   c->Ufp[1], c->Fvn, c->Fcom, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
                   c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubx, c->Ubar, c->pbar, c->dops, c->dwall,
                   c->mbar, c->gbar, c->nbx, c->mbar_acc, c->gbar_acc, c->d_dt, c->dt_ele, c->h_ref, c->evol,
-                  c->dfw, c->U_til, c->rk_err, c->rkv};
+                  c->dfw, c->U_til, c->rk_err, c->rkv, c->geo_tab, c->geo_pair, c->geo_work};
   for (void *b : bufs)
     if (b) cudaFree(b);
   for (auto &r : c->recs)

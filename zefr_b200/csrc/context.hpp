@@ -33,6 +33,13 @@ void ctx_set_time_scheme(Ctx *c, const zb_time_scheme *ts);
 void ctx_time_state(Ctx *c, double *dt, double *prev_err, int64_t *rejected, double *flow_time);
 void ctx_get_element_dt(Ctx *c, double *out);
 void ctx_step_scheme(Ctx *c, int n);  // zb_step with the context's time scheme
+void ctx_refresh_cfl_geometry(Ctx *c);  // after the mesh moved
+// geometry from element node coordinates (geometry.cu)
+void ctx_geometry_eval(Ctx *c, const double *nodes, double *inv_jaco, double *jaco_det, double *norm, double *dA,
+                       int where);
+void ctx_geometry_eval_vjp(Ctx *c, const double *nodes, const double *inv_jaco_bar, const double *jaco_det_bar,
+                           const double *norm_bar, const double *dA_bar, double *nodes_bar, int where);
+void ctx_set_nodes(Ctx *c, const double *nodes, int where);
 // CFL limits of the upwinded advection and LDG diffusion operators per order
 // (reference get_cfl_limit_adv / get_cfl_limit_diff, src/funcs.cpp:435-560)
 double cfl_limit_adv(int order);

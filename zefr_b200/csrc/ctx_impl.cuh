@@ -83,6 +83,11 @@ struct Ctx
   double *mbar = nullptr, *gbar = nullptr, *nbx = nullptr;  // geometry adjoint
   double *mbar_acc = nullptr, *gbar_acc = nullptr;          // its device-side sums
   double *rkv = nullptr;  // step adjoint: stage states, residuals and adjoints (tile layout)
+  // geometry from node coordinates (geometry.cu): shape tables, face pairing, scratch
+  double *geo_tab = nullptr;
+  int64_t *geo_pair = nullptr;
+  double *geo_work = nullptr;
+  size_t geo_work_bytes = 0;
   // time integration (zb_set_time_scheme; time_scheme.cu); the RK54 and CFL
   // buffers are allocated on first use
   zb_time_scheme ts{ZB_RK44, 0, 1, 1.0, 0, 1e-5, 1e-5, 0.7, 0.4, 0.8, 2.5, 0.3, 100.0};

@@ -504,6 +504,7 @@ void build_plan(const zb_mesh &mesh, const zb_params &params, Plan &p)
   p.dshape_spts = shs.dval;
   p.dshape_fpts = shf.dval;
   p.shape_fpts = shf.val;
+  p.shape_spts = shs.val;
   p.coord_spts.assign((size_t)S * D * E, 0.0);
   p.coord_fpts.assign((size_t)Fp * D * E, 0.0);
   p.jaco_det_spts.assign((size_t)S * E, 0.0);

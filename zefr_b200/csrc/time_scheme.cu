@@ -192,6 +192,19 @@ static void upload_cfl_geometry(Ctx *c)
   if (!c->dt_ele) c->dt_ele = (double *)talloc((size_t)nt * TW * sizeof(double));
 }
 
+// volumes and line lengths again from the (moved) geometry
+void ctx_refresh_cfl_geometry(Ctx *c)
+{
+  double **bufs[] = {&c->evol, &c->dfw, &c->h_ref};
+  for (double **b : bufs)
+    if (*b)
+    {
+      cudaFree(*b);
+      *b = nullptr;
+    }
+  if (c->ts.dt_type != 0) upload_cfl_geometry(c);
+}
+
 void ctx_set_time_scheme(Ctx *c, const zb_time_scheme *ts)
 {
   if (!ts) ZB_THROW(ZB_ERR_ARG, "null time scheme");

@@ -72,6 +72,7 @@ struct Plan
   std::vector<double> dshape_spts;   // [D][S][nNodes] shape-function derivatives (geometry adjoint)
   std::vector<double> dshape_fpts;   // [D][Fp][nNodes]
   std::vector<double> shape_fpts;    // [Fp][nNodes]
+  std::vector<double> shape_spts;    // [S][nNodes]
 
   // Face connectivity per element flux point
   std::vector<int64_t> partner;  // [Fp][E]: e'*Fp + f' (interior) or -1-bc (boundary)

@@ -426,6 +426,79 @@ class FRSolver:
                                             g["dA"].ctypes.data_as(_DP), 1 if reset else 0))
         return g
 
+    # -- geometry from element nodes (zb_geometry_eval, zb_set_nodes) --
+    @property
+    def nodes_shape(self):
+        """(nNodes, ndims, neles): the element node layout Elements::nodes."""
+        if getattr(self, "_nodes_shape", None) is None:
+            n = self.plan.get("nodes").size
+            self._nodes_shape = (n // (self.ndims * self.neles), self.ndims, self.neles)
+        return self._nodes_shape
+
+    def _geometry_shapes(self):
+        S, D, E, Fp = self.nspts, self.ndims, self.neles, self.info.nfpts
+        return {"inv_jaco": (D, S, D, E), "jaco_det": (S, E), "norm": (Fp, D, E), "dA": (Fp, E)}
+
+    def geometry_eval(self, nodes):
+        """Set-up metrics of element nodes [nNodes][D][E] (float64 CUDA
+        tensor), computed on the device by zb_geometry_eval: a dict of CUDA
+        tensors inv_jaco [D,S,D,E], jaco_det [S,E], norm [Fp,D,E], dA [Fp,E]."""
+        import torch
+        nodes = nodes.to(torch.float64).contiguous()
+        if tuple(nodes.shape) != self.nodes_shape or not nodes.is_cuda:
+            raise ValueError(f"nodes must be a CUDA tensor of shape {self.nodes_shape}")
+        out = {k: torch.empty(s, dtype=torch.float64, device=nodes.device) for k, s in self._geometry_shapes().items()}
+        self._torch_ready()
+        check(lib().zb_geometry_eval(self.h, ctypes.cast(nodes.data_ptr(), _DP),
+                                     *(ctypes.cast(out[k].data_ptr(), _DP) for k in ("inv_jaco", "jaco_det", "norm", "dA")),
+                                     _lib.ZB_DEVICE))
+        self._device_done()
+        return out
+
+    def geometry_eval_vjp(self, nodes, bars: Dict[str, object]):
+        """Adjoint of :meth:`geometry_eval` at ``nodes``: the node adjoint
+        [nNodes][D][E] (CUDA tensor) of metric adjoints ``bars`` (keys as
+        geometry_eval's; missing keys count as zero)."""
+        import torch
+        nodes = nodes.to(torch.float64).contiguous()
+        if tuple(nodes.shape) != self.nodes_shape or not nodes.is_cuda:
+            raise ValueError(f"nodes must be a CUDA tensor of shape {self.nodes_shape}")
+        shapes = self._geometry_shapes()
+        held, ptrs = [], []
+        for k in ("inv_jaco", "jaco_det", "norm", "dA"):
+            b = bars.get(k)
+            if b is None:
+                ptrs.append(None)
+                continue
+            b = torch.as_tensor(b, dtype=torch.float64, device=nodes.device).contiguous()
+            if tuple(b.shape) != shapes[k]:
+                raise ValueError(f"{k} adjoint must have shape {shapes[k]}")
+            held.append(b)
+            ptrs.append(ctypes.cast(b.data_ptr(), _DP))
+        out = torch.empty_like(nodes)
+        self._torch_ready()
+        check(lib().zb_geometry_eval_vjp(self.h, ctypes.cast(nodes.data_ptr(), _DP), *ptrs,
+                                         ctypes.cast(out.data_ptr(), _DP), _lib.ZB_DEVICE))
+        self._device_done()
+        return out
+
+    def set_nodes(self, nodes) -> None:
+        """Move the mesh (zb_set_nodes): new element nodes [nNodes][D][E], a
+        numpy array or a CUDA tensor; metrics are recomputed on the device."""
+        if hasattr(nodes, "is_cuda") and nodes.is_cuda:
+            import torch
+            nodes = nodes.to(torch.float64).contiguous()
+            if tuple(nodes.shape) != self.nodes_shape:
+                raise ValueError(f"nodes must have shape {self.nodes_shape}")
+            self._torch_ready()
+            check(lib().zb_set_nodes(self.h, ctypes.cast(nodes.data_ptr(), _DP), _lib.ZB_DEVICE))
+            self._device_done()
+        else:
+            nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+            if nodes.shape != self.nodes_shape:
+                raise ValueError(f"nodes must have shape {self.nodes_shape}")
+            check(lib().zb_set_nodes(self.h, nodes.ctypes.data_as(_DP), _lib.ZB_HOST))
+
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().zb_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
         self._stream = stream_ptr
