@@ -243,26 +243,37 @@ def time_e2e(s, U, K: int, W: int, world: int):
     return max_over_ranks(ms, world), Un.nbytes, Rn.nbytes
 
 
-def triangle_side(K: int, W: int):
+def triangle_solver(form: str, mesh=None):
     """Triangle workload: 128 x 128 quads on periodic [0,1]^2 split along seeded
     diagonals (32,768 triangles), interior nodes jittered 15% of h, P4
     (15 Williams-Shunn points), Roe + LDG (beta 0.5, tau 0.1), Ma 0.2, Re 1000,
-    Pr 0.71, double shear layer with seeded 1e-3 velocity noise.  GDOF/s per
-    residual of both forms and the mixed form's relative L2 error."""
+    Pr 0.71, double shear layer with seeded 1e-3 velocity noise; the solver of
+    one form on torch's current stream, with the state set."""
     import torch
     from zefr_b200 import ics, meshgen
     from zefr_b200.solver import FRSolver, params_from_deck
+    if mesh is None:
+        mesh = meshgen.box_tris(128, seed=2024, jitter=0.15)
+    p = params_from_deck(ndims=2, order=4, viscous=1, disable_nondim=1, fix_vis=1, mach_fs=0.2, Re_fs=1000.0,
+                         prandtl=0.71, P_fs=1.0, rho_fs=1.0, L_fs=1.0, ldg_b=0.5, ldg_tau=0.1, fconv=2,
+                         precision={"mixed": 1, "fp64": 0}[form], gamma=1.4, dt=1e-4)
+    s = FRSolver(mesh, p, {"PERIODIC": "periodic"})
+    s.set_stream(torch.cuda.current_stream().cuda_stream)
+    X = s.plan.get("coord_spts").reshape(s.nspts, 2, s.neles)
+    s.set_state(ics.double_shear_layer(X, mach=0.2, noise=1e-3, seed=7))
+    return s
+
+
+def triangle_side(K: int, W: int):
+    """The triangle workload (triangle_solver): GDOF/s per residual of both
+    forms and the mixed form's relative L2 error."""
+    import torch
+    from zefr_b200 import meshgen
     mesh = meshgen.box_tris(128, seed=2024, jitter=0.15)
     out = {"workload": "triangles_128x128x2_P4_navier_stokes_roe_ldg", "elements": int(mesh.n_elements)}
     R = {}
     for form in ("mixed", "fp64"):
-        p = params_from_deck(ndims=2, order=4, viscous=1, disable_nondim=1, fix_vis=1, mach_fs=0.2, Re_fs=1000.0,
-                             prandtl=0.71, P_fs=1.0, rho_fs=1.0, L_fs=1.0, ldg_b=0.5, ldg_tau=0.1, fconv=2,
-                             precision={"mixed": 1, "fp64": 0}[form], gamma=1.4, dt=1e-4)
-        s = FRSolver(mesh, p, {"PERIODIC": "periodic"})
-        s.set_stream(torch.cuda.current_stream().cuda_stream)
-        X = s.plan.get("coord_spts").reshape(s.nspts, 2, s.neles)
-        s.set_state(ics.double_shear_layer(X, mach=0.2, noise=1e-3, seed=7))
+        s = triangle_solver(form, mesh)
         for i in range(W):
             s.compute_residual(i % 4)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -573,8 +584,11 @@ def profile_run(args):
     import torch
     torch.cuda.set_device(0)
     adj = args.profile_form == "adjoint"
-    s, U = build_solver("fp64" if adj else args.profile_form, args.cells)
-    s.set_state(U)
+    if args.profile_form.startswith("tri-"):
+        s = triangle_solver(args.profile_form[4:])
+    else:
+        s, U = build_solver("fp64" if adj else args.profile_form, args.cells)
+        s.set_state(U)
     lam = torch.ones(s.state_shape, dtype=torch.float64, device="cuda") if adj else None
     for i in range(args.warmup + args.steps):
         if adj:
@@ -638,7 +652,7 @@ def main():
     ap.add_argument("--ref-cells", type=int, default=20, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-side", action="store_true", help="skip the triangle and batched side workloads")
-    ap.add_argument("--profile-form", choices=["mixed", "fp64", "adjoint"], default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--profile-form", choices=["mixed", "fp64", "adjoint", "tri-mixed", "tri-fp64"], default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
