@@ -505,7 +505,7 @@ static void free_all(Ctx *c)
                   c->Ufp[1], c->Fvn, c->Fcom, c->mets, c->fgeo, c->Ucomp, c->nbr, c->dtmp, c->dred, c->dref,
                   c->dU, c->dweights, c->dfun, c->lam, c->Lfp, c->Ubfp, c->dUbfp, c->UCb, c->Ubx, c->Ubar, c->pbar, c->dops, c->dwall,
                   c->mbar, c->gbar, c->nbx, c->mbar_acc, c->gbar_acc, c->d_dt, c->dt_ele, c->h_ref, c->evol,
-                  c->dfw, c->U_til, c->rk_err, c->rkv, c->geo_tab, c->geo_pair, c->geo_work};
+                  c->dfw, c->U_til, c->rk_err, c->rkv, c->rkfvn, c->geo_tab, c->geo_pair, c->geo_work};
   for (void *b : bufs)
     if (b) cudaFree(b);
   for (auto &r : c->recs)
@@ -1002,9 +1002,12 @@ static void ensure_adjoint_buffers(Ctx *c)
 
 // The adjoint of the residual at the context's current state for the weight
 // already in c->lam (tile layout), into c->Ubar; optionally the free-stream
-// adjoint (host, summed over tiles) and the geometry adjoint (c->mbar /
-// c->gbar, added to the device sums with `accumulate`).
-static void vjp_tiles(Ctx *c, double *param_bar, bool geo, bool accumulate)
+// adjoint (`params`: per tile in c->pbar, and with param_bar also summed over
+// tiles on the host) and the geometry adjoint (c->mbar / c->gbar, added to
+// the device sums with `accumulate`).  The geometry adjoint of the viscous
+// form reads this state's forward viscous normal flux from c->Fvn: computed
+// here unless `fvn_ready` says the caller has put it there.
+static void vjp_tiles(Ctx *c, bool params, double *param_bar, bool geo, bool accumulate, bool fvn_ready = false)
 {
   // linearisation point: the current state and its traces
   c->ufp_valid = false;
@@ -1020,13 +1023,13 @@ static void vjp_tiles(Ctx *c, double *param_bar, bool geo, bool accumulate)
     }
     // the face values need the forward viscous normal fluxes of this state
     // (residual register 0 is overwritten with this state's residual)
-    if (c->plan.params.viscous)
+    if (c->plan.params.viscous && !fvn_ready)
     {
       StageCfg sc{0, 0, 0, 0};
       c->launch_stage(*c, sc);
     }
   }
-  c->launch_vjp(*c, param_bar != nullptr, geo);
+  c->launch_vjp(*c, params || param_bar, geo);
   if (accumulate)
   {
     const size_t nm = (size_t)c->ntiles * c->S * NM * TW, ng = (size_t)c->ntiles * c->Fp * (c->D + 1) * TW;
@@ -1074,7 +1077,7 @@ void ctx_vjp(Ctx *c, const double *lam, double *Ubar, int64_t ss, int64_t vs, in
     c->launches++;
     CK(cudaGetLastError());
   }
-  vjp_tiles(c, param_bar, geo, accumulate);
+  vjp_tiles(c, param_bar != nullptr, param_bar, geo, accumulate);
   from_tiles(c, c->Ubar, nullptr, nullptr, Ubar, ss, vs, es, where);
   if (geo_out) geo_to_reference(c, c->mbar, c->gbar, inv_jaco_bar, jaco_det_bar, norm_bar, dA_bar);
 }
@@ -1154,9 +1157,16 @@ void ctx_rk_step_vjp(Ctx *c, const double *U0, const double *Ubar1, double *Ubar
   if (!c->rkv)
   {
     // stage states 0..3, stage residuals 0..3, the end state's adjoint, one
-    // stage adjoint and the running result, in the tile layout
-    c->rkv = (double *)dalloc((size_t)11 * nU * sizeof(double));
+    // stage adjoint and the running result, in the tile layout; the
+    // free-stream adjoint per tile summed over the stages
+    c->rkv = (double *)dalloc(((size_t)11 * nU + (size_t)c->ntiles * 5) * sizeof(double));
   }
+  double *pb_acc = c->rkv + (size_t)11 * nU;
+  // the geometry adjoint of the viscous form needs each stage's forward
+  // viscous normal flux: kept from the forward sweep
+  const bool keep_fvn = geometry && c->plan.params.viscous;
+  const size_t nF = (size_t)c->ntiles * c->Fp * V * TW;
+  if (keep_fvn && !c->rkfvn) c->rkfvn = (double *)dalloc(4 * nF * sizeof(double));
   double *Us[4], *Rs[4];
   for (int s = 0; s < 4; s++)
   {
@@ -1186,6 +1196,8 @@ void ctx_rk_step_vjp(Ctx *c, const double *U0, const double *Ubar1, double *Ubar
     StageCfg sc{0, 0, 0, 0};
     c->launch_stage(*c, sc);
     CK(cudaMemcpyAsync(Rs[s], c->divF[0], (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    if (keep_fvn)
+      CK(cudaMemcpyAsync(c->rkfvn + s * nF, c->Fvn, nF * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     if (s < 3)
     {
       k_stage_state<<<grid, 256, 0, c->stream>>>(Us[s + 1], Us[0], Rs[s], (const double *)c->mets, kRkAlpha[s] * dt,
@@ -1197,7 +1209,7 @@ void ctx_rk_step_vjp(Ctx *c, const double *U0, const double *Ubar1, double *Ubar
   // reverse: Ubar0 = Ubar1 + sum_s (dR_s/dU_s)^T lam_s with the stage weights
   // lam_s = -b_s dt/|J| Ubar1 - a_s dt/|J| Ubar_{s+1}
   CK(cudaMemcpyAsync(ub0, ub1, (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  double pacc[5] = {0, 0, 0, 0, 0};
+  if (param_bar) CK(cudaMemsetAsync(pb_acc, 0, (size_t)c->ntiles * 5 * sizeof(double), c->stream));
   for (int s = 3; s >= 0; s--)
   {
     k_stage_weight<<<grid, 256, 0, c->stream>>>(c->lam, ub1, s < 3 ? ubs : nullptr, (const double *)c->mets,
@@ -1206,10 +1218,15 @@ void ctx_rk_step_vjp(Ctx *c, const double *U0, const double *Ubar1, double *Ubar
     c->launches++;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->U, Us[s], (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    double pb[5];
-    vjp_tiles(c, param_bar ? pb : nullptr, geometry, geometry);
+    if (keep_fvn)
+      CK(cudaMemcpyAsync(c->Fvn, c->rkfvn + s * nF, nF * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    vjp_tiles(c, param_bar != nullptr, nullptr, geometry, geometry, keep_fvn);
     if (param_bar)
-      for (int k = 0; k < 5; k++) pacc[k] += pb[k];
+    {
+      k_accumulate<<<grid_for(c->ntiles * 5, 256), 256, 0, c->stream>>>(pb_acc, c->pbar, c->ntiles * 5);
+      c->launches++;
+      CK(cudaGetLastError());
+    }
     CK(cudaMemcpyAsync(ubs, c->Ubar, (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     k_add<<<grid, 256, 0, c->stream>>>(ub0, ubs, nU);
     c->launches++;
@@ -1235,7 +1252,16 @@ void ctx_rk_step_vjp(Ctx *c, const double *U0, const double *Ubar1, double *Ubar
     }
   }
   if (param_bar)
+  {
+    // one read of the stage-summed tiles, summed over tiles in a fixed order
+    std::vector<double> h((size_t)c->ntiles * 5);
+    CK(cudaMemcpyAsync(h.data(), pb_acc, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double pacc[5] = {0, 0, 0, 0, 0};
+    for (int64_t t = 0; t < c->ntiles; t++)
+      for (int k = 0; k < 5; k++) pacc[k] += h[(size_t)t * 5 + k];
     for (int k = 0; k < 5; k++) param_bar[k] += pacc[k];
+  }
   from_tiles(c, ub0, nullptr, nullptr, Ubar0, ss, vs, es, where);
   c->ufp_valid = false;
 }

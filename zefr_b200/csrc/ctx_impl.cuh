@@ -83,6 +83,7 @@ struct Ctx
   double *mbar = nullptr, *gbar = nullptr, *nbx = nullptr;  // geometry adjoint
   double *mbar_acc = nullptr, *gbar_acc = nullptr;          // its device-side sums
   double *rkv = nullptr;  // step adjoint: stage states, residuals and adjoints (tile layout)
+  double *rkfvn = nullptr;  // step adjoint: the four stages' forward viscous normal fluxes
   // geometry from node coordinates (geometry.cu): shape tables, face pairing, scratch
   double *geo_tab = nullptr;
   int64_t *geo_pair = nullptr;
