@@ -36,7 +36,7 @@ def _interior_nodes(mesh):
 
 
 @pytest.mark.parametrize("name", ["cyl_p3_ns_char_adi", "cyl_p3_euler_slip_char", "quad_p2_ns_jitter",
-                                  "hex_p2_euler_jitter", "cyl_p2_ns_iso_farfield_b03"])
+                                  "hex_p2_euler_jitter", "cyl_p2_ns_iso_farfield_b03", "hex_p1_ns", "hex_p3_ns_tgv"])
 def test_geometry_adjoint_matches_central_differences(name):
     g = gc.load(name)
     D = g.meta["ndims"]
@@ -54,6 +54,18 @@ def test_geometry_adjoint_matches_central_differences(name):
         # have kinks there and a difference quotient has no derivative to
         # match.  Turn the stream by 0.5 rad to move off them.
         c, sn = np.cos(0.5), np.sin(0.5)
+        mx, my = U[:, 1].copy(), U[:, 2].copy()
+        U[:, 1], U[:, 2] = c * mx - sn * my, sn * mx + c * my
+    elif D == 3:
+        # The hexahedral fixtures hold Taylor-Green-like states with w = 0
+        # everywhere, so the normal velocity at every z-face point is exactly
+        # zero: the Rusanov flux's |Vn| has its kink there and the residual
+        # has no derivative with respect to the face normal (central
+        # differences then differ from the adjoint by a constant, whatever
+        # the step).  Turn the velocity by 0.5 rad about x, then about z.
+        c, sn = np.cos(0.5), np.sin(0.5)
+        my, mz = U[:, 2].copy(), U[:, 3].copy()
+        U[:, 2], U[:, 3] = c * my - sn * mz, sn * my + c * mz
         mx, my = U[:, 1].copy(), U[:, 2].copy()
         U[:, 1], U[:, 2] = c * mx - sn * my, sn * mx + c * my
     s = FRSolver(g.mesh, p, g.bounds)
