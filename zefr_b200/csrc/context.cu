@@ -419,7 +419,7 @@ static void launch_stage_tri(Ctx &c, const StageCfg &sc)
   using G = dev::TriShape<N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, D = 2;
   const Args<T, A> a = make_args<T, A>(c, sc);
-  const size_t ops = (size_t)((G::NOPS + 1) / 2) * 2;
+  const size_t ops = (size_t)G::OPS_PAD;
   if (!c.plan.params.viscous)
   {
     const size_t smem = (ops + (size_t)(S * V + D * S * V + Fp * V) * TW) * sizeof(A);

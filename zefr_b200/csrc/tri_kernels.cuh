@@ -25,7 +25,77 @@ struct TriShape
   // oppDiv [S][D*S], oppDiv_fpts [S][Fp]
   static constexpr int OE = 0, OD = OE + Fp * S, ODF = OD + D * S * S, ODV = ODF + D * S * Fp,
                        ODVF = ODV + S * D * S, NOPS = ODVF + S * Fp;
+  // the tile arrays that follow the operator block in shared memory start on
+  // a 16-byte boundary
+  static constexpr int OPS_PAD = ((NOPS + 3) / 4) * 4;
+  static_assert(V == 4, "the shared tile arrays hold four variables per point");
 };
+
+// Shared-memory tile arrays of these kernels (states, common solutions,
+// gradients, fluxes) keep the four variables of one (point, element)
+// together, [P][TW][4]: one 16-byte load (FP32) or two (FP64) fetch a point's
+// variables where the global [P][V][TW] order would take four loads, and the
+// eight elements of a warp's point cover 128 contiguous bytes.
+__device__ __forceinline__ int tvl(int p, int l) { return (p * TW + l) * 4; }
+
+__device__ __forceinline__ void ld4(const float *p, float x[4])
+{
+  const float4 q = *reinterpret_cast<const float4 *>(p);
+  x[0] = q.x;
+  x[1] = q.y;
+  x[2] = q.z;
+  x[3] = q.w;
+}
+
+__device__ __forceinline__ void ld4(const double *p, double x[4])
+{
+  const double2 a = *reinterpret_cast<const double2 *>(p);
+  const double2 b = *reinterpret_cast<const double2 *>(p + 2);
+  x[0] = a.x;
+  x[1] = a.y;
+  x[2] = b.x;
+  x[3] = b.y;
+}
+
+__device__ __forceinline__ void st4(float *p, const float x[4])
+{
+  *reinterpret_cast<float4 *>(p) = make_float4(x[0], x[1], x[2], x[3]);
+}
+
+__device__ __forceinline__ void st4(double *p, const double x[4])
+{
+  *reinterpret_cast<double2 *>(p) = make_double2(x[0], x[1]);
+  *reinterpret_cast<double2 *>(p + 2) = make_double2(x[2], x[3]);
+}
+
+// global [S][V][TW] tile -> shared [S][TW][4]
+template <typename T, typename A, int S>
+__device__ __forceinline__ void load_tile_vl(const T *__restrict__ src, A *dst)
+{
+  for (int i = threadIdx.x; i < S * 4 * TW; i += blockDim.x)
+  {
+    const int l = i % TW, v = (i / TW) % 4, p = i / (4 * TW);
+    dst[tvl(p, l) + v] = src[i];
+  }
+}
+
+// X_v(f) = sum_s E[f][s] Y_v(s) for the four variables of a [S][TW][4] array
+template <typename A, int N>
+__device__ __forceinline__ void tri_extrap4(const A *sY, const A *E, int f, int l, A out[4])
+{
+  constexpr int S = TriShape<N>::S;
+#pragma unroll
+  for (int v = 0; v < 4; v++) out[v] = A(0);
+#pragma unroll
+  for (int t = 0; t < S; t++)
+  {
+    A x[4];
+    ld4(sY + tvl(t, l), x);
+    const A e = E[f * S + t];
+#pragma unroll
+    for (int v = 0; v < 4; v++) out[v] += e * x[v];
+  }
+}
 
 template <typename A, int N>
 __device__ __forceinline__ void load_tri_ops(A *sops, const A *g)
@@ -34,6 +104,7 @@ __device__ __forceinline__ void load_tri_ops(A *sops, const A *g)
 }
 
 // X(f) = sum_s E[f][s] Y(s) for component v of a tile array in smem [S][nv][TW]
+// (the RK-updated state, as store_rk leaves it)
 template <typename A, int N>
 __device__ __forceinline__ A tri_extrap(const A *sY, const A *E, int f, int v, int l, int nv)
 {
@@ -86,7 +157,7 @@ __device__ __forceinline__ void tri_extrap_next(const Args<T, A> &a, int64_t til
   }
 }
 
-// transformed flux F~_d = adj[d][.] . F at solution point s into sF [D][S][V][TW]
+// transformed flux F~_d = adj[d][.] . F at solution point s into sF [D*S][TW][4]
 template <typename T, typename A>
 __device__ __forceinline__ void tri_transform(const Args<T, A> &a, int64_t tile, int s, int l, const A F[4][2],
                                               A *sF, int S)
@@ -98,9 +169,13 @@ __device__ __forceinline__ void tri_transform(const Args<T, A> &a, int64_t tile,
 #pragma unroll
     for (int d2 = 0; d2 < 2; d2++) adj[d1][d2] = m[(d1 * 2 + d2) * TW];
 #pragma unroll
-  for (int v = 0; v < 4; v++)
+  for (int d1 = 0; d1 < 2; d1++)
+  {
+    A Ft[4];
 #pragma unroll
-    for (int d1 = 0; d1 < 2; d1++) sF[((d1 * S + s) * 4 + v) * TW + l] = F[v][0] * adj[d1][0] + F[v][1] * adj[d1][1];
+    for (int v = 0; v < 4; v++) Ft[v] = F[v][0] * adj[d1][0] + F[v][1] * adj[d1][1];
+    st4(sF + tvl(d1 * S + s, l), Ft);
+  }
 }
 
 // divF(s) = sum_k oppDiv[s][k] F~(k) + sum_f oppDiv_fpts[s][f] Fc(f), then store / RK
@@ -127,14 +202,22 @@ __device__ __forceinline__ void tri_finish(const Args<T, A> &a, int64_t tile, in
     const A *Dv = ops + G::ODV + s * D * S;
 #pragma unroll
     for (int k = 0; k < D * S; k++)
+    {
+      A x[4];
+      ld4(sF + tvl(k, l), x);
 #pragma unroll
-      for (int v = 0; v < V; v++) vol[v] += Dv[k] * sF[(k * V + v) * TW + l];
+      for (int v = 0; v < V; v++) vol[v] += Dv[k] * x[v];
+    }
   }
   const A *Dvf = ops + G::ODVF + s * Fp;
 #pragma unroll
   for (int f = 0; f < Fp; f++)
+  {
+    A x[4];
+    ld4(sFc + tvl(f, l), x);
 #pragma unroll
-    for (int v = 0; v < V; v++) surf[v] += Dvf[f] * sFc[(f * V + v) * TW + l];
+    for (int v = 0; v < V; v++) surf[v] += Dvf[f] * x[v];
+  }
   A res[V];
 #pragma unroll
   for (int v = 0; v < V; v++) res[v] = vol[v] + surf[v];
@@ -151,23 +234,19 @@ __global__ void __launch_bounds__(128) k_tri_euler(const __grid_constant__ Args<
   constexpr int S = G::S, Fp = G::Fp, V = G::V, D = 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sops = reinterpret_cast<A *>(smem_raw);
-  A *sU = sops + ((G::NOPS + 1) / 2) * 2;
+  A *sU = sops + G::OPS_PAD;  // [S][TW][4]; then the RK-updated state as store_rk writes it
   A *sF = sU + S * V * TW;
   A *sFc = sF + D * S * V * TW;
   load_tri_ops<A, N>(sops, a.dops);
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
-  {
-    const T *src = a.U + tile * (int64_t)S * V * TW;
-    for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
-  }
+  load_tile_vl<T, A, S>(a.U + tile * (int64_t)S * V * TW, sU);
   __syncthreads();
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
   {
     const int s = it / TW, l = it % TW;
     A U[V], F[V][D], P, Pp;
-#pragma unroll
-    for (int v = 0; v < V; v++) U[v] = sU[(s * V + v) * TW + l];
+    ld4(sU + tvl(s, l), U);
     flux_conv_stored<A, D>(U, F, P, Pp, a.ph);
     tri_transform<T, A>(a, tile, s, l, F, sF, S);
   }
@@ -187,8 +266,10 @@ __global__ void __launch_bounds__(128) k_tri_euler(const __grid_constant__ Args<
     if (code >= 0) gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
     conv_common<T, A, D>(a, Uo, Un, code, n, UL, UR, UB, Fc);
     const bool right = (code >= 0) && (code & 1);
+    A out[V];
 #pragma unroll
-    for (int v = 0; v < V; v++) sFc[(f * V + v) * TW + l] = right ? -Fc[v] * dA : Fc[v] * dA;
+    for (int v = 0; v < V; v++) out[v] = right ? -Fc[v] * dA : Fc[v] * dA;
+    st4(sFc + tvl(f, l), out);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
@@ -214,16 +295,13 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
   constexpr int S = G::S, Fp = G::Fp, V = G::V, D = 2, NM = 5;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sops = reinterpret_cast<A *>(smem_raw);
-  A *sU = sops + ((G::NOPS + 1) / 2) * 2;
-  A *sUC = sU + S * V * TW;
-  A *sdU = sUC + Fp * V * TW;  // [D][S][V][TW]: physical gradient, then F~
+  A *sU = sops + G::OPS_PAD;    // [S][TW][4]
+  A *sUC = sU + S * V * TW;      // [Fp][TW][4]
+  A *sdU = sUC + Fp * V * TW;    // [D*S][TW][4]: physical gradient, then F~
   load_tri_ops<A, N>(sops, a.dops);
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
-  {
-    const T *src = a.U + tile * (int64_t)S * V * TW;
-    for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
-  }
+  load_tile_vl<T, A, S>(a.U + tile * (int64_t)S * V * TW, sU);
   const A beta = a.ph.ldg_b;
   for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
   {
@@ -261,8 +339,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
       ghost_state<A, D>(-code - 1, Ua, n, URa, UBa, a.ph);
       to_stored<A, D>(UBa, UC, a.ph);
     }
-#pragma unroll
-    for (int v = 0; v < V; v++) sUC[(f * V + v) * TW + l] = UC[v];
+    st4(sUC + tvl(f, l), UC);
   }
   __syncthreads();
   // gradient: oppD U + oppD_fpts Ucomm, then physical
@@ -275,16 +352,31 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
     {
       const A *Dd = sops + G::OD + (d * S + s) * S;
       const A *Df = sops + G::ODF + (d * S + s) * Fp;
+      A acc[V], cor[V];
 #pragma unroll
       for (int v = 0; v < V; v++)
       {
-        A acc = A(0), cor = A(0);
-#pragma unroll
-        for (int t = 0; t < S; t++) acc += Dd[t] * sU[(t * V + v) * TW + l];
-#pragma unroll
-        for (int f = 0; f < Fp; f++) cor += Df[f] * sUC[(f * V + v) * TW + l];
-        tdU[v][d] = acc + cor;
+        acc[v] = A(0);
+        cor[v] = A(0);
       }
+#pragma unroll
+      for (int t = 0; t < S; t++)
+      {
+        A x[4];
+        ld4(sU + tvl(t, l), x);
+#pragma unroll
+        for (int v = 0; v < V; v++) acc[v] += Dd[t] * x[v];
+      }
+#pragma unroll
+      for (int f = 0; f < Fp; f++)
+      {
+        A x[4];
+        ld4(sUC + tvl(f, l), x);
+#pragma unroll
+        for (int v = 0; v < V; v++) cor[v] += Df[f] * x[v];
+      }
+#pragma unroll
+      for (int v = 0; v < V; v++) tdU[v][d] = acc[v] + cor[v];
     }
     const T *m = a.mets + (tile * S + s) * (int64_t)NM * TW + l;
     A adj[D][D];
@@ -294,16 +386,24 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
       for (int d2 = 0; d2 < D; d2++) adj[d1][d2] = m[(d1 * D + d2) * TW];
     const A inv_det = A(1) / m[D * D * TW];
 #pragma unroll
-    for (int v = 0; v < V; v++)
+    for (int d1 = 0; d1 < D; d1++)
+    {
+      A g[V];
 #pragma unroll
-      for (int d1 = 0; d1 < D; d1++)
-        sdU[((d1 * S + s) * V + v) * TW + l] = (tdU[v][0] * adj[0][d1] + tdU[v][1] * adj[1][d1]) * inv_det;
+      for (int v = 0; v < V; v++) g[v] = (tdU[v][0] * adj[0][d1] + tdU[v][1] * adj[1][d1]) * inv_det;
+      st4(sdU + tvl(d1 * S + s, l), g);
+    }
   }
   __syncthreads();
   if (a.dU_out)
   {
+    // back to the global [D][S][V][TW] order
     T *g = a.dU_out + tile * (int64_t)D * S * V * TW;
-    for (int i = threadIdx.x; i < D * S * V * TW; i += blockDim.x) g[i] = (T)sdU[i];
+    for (int i = threadIdx.x; i < D * S * V * TW; i += blockDim.x)
+    {
+      const int l = i % TW, v = (i / TW) % V, p = i / (V * TW);
+      g[i] = (T)sdU[tvl(p, l) + v];
+    }
   }
   // own viscous normal flux at flux points
   for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
@@ -318,11 +418,14 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
     A Uf[V], dUf[V][D], Fn[V];
     const T *uo = a.Ufp + (tile * Fp + f) * (int64_t)V * TW + l;
 #pragma unroll
-    for (int v = 0; v < V; v++)
-    {
-      Uf[v] = uo[v * TW];
+    for (int v = 0; v < V; v++) Uf[v] = uo[v * TW];
 #pragma unroll
-      for (int d = 0; d < D; d++) dUf[v][d] = tri_extrap<A, N>(sdU + d * S * V * TW, sops + G::OE, f, v, l, V);
+    for (int d = 0; d < D; d++)
+    {
+      A x[V];
+      tri_extrap4<A, N>(sdU + d * S * V * TW, sops + G::OE, f, l, x);
+#pragma unroll
+      for (int v = 0; v < V; v++) dUf[v][d] = x[v];
     }
     A Ua[V];
     to_abs<A, D>(Uf, Ua, a.ph);
@@ -344,12 +447,14 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
   {
     const int s = it / TW, l = it % TW;
     A U[V], dU[V][D], F[V][D], P, Pp, Ua[V];
+    ld4(sU + tvl(s, l), U);
 #pragma unroll
-    for (int v = 0; v < V; v++)
+    for (int d = 0; d < D; d++)
     {
-      U[v] = sU[(s * V + v) * TW + l];
+      A x[V];
+      ld4(sdU + tvl(d * S + s, l), x);
 #pragma unroll
-      for (int d = 0; d < D; d++) dU[v][d] = sdU[((d * S + s) * V + v) * TW + l];
+      for (int v = 0; v < V; v++) dU[v][d] = x[v];
     }
     flux_conv_stored<A, D>(U, F, P, Pp, a.ph);
     to_abs<A, D>(U, Ua, a.ph);
@@ -367,8 +472,12 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
     const A *Dv = sops + G::ODV + s * D * S;
 #pragma unroll
     for (int k = 0; k < D * S; k++)
+    {
+      A x[V];
+      ld4(sdU + tvl(k, l), x);
 #pragma unroll
-      for (int v = 0; v < V; v++) vol[v] += Dv[k] * sdU[(k * V + v) * TW + l];
+      for (int v = 0; v < V; v++) vol[v] += Dv[k] * x[v];
+    }
     A *out = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
 #pragma unroll
     for (int v = 0; v < V; v++) out[v * TW] = vol[v];
@@ -385,8 +494,8 @@ __global__ void __launch_bounds__(128) k_tri_ns_face(const __grid_constant__ Arg
   constexpr int S = G::S, Fp = G::Fp, V = G::V, D = 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sops = reinterpret_cast<A *>(smem_raw);
-  A *sFc = sops + ((G::NOPS + 1) / 2) * 2;
-  A *sUnew = sFc + Fp * V * TW;
+  A *sFc = sops + G::OPS_PAD;   // [Fp][TW][4]
+  A *sUnew = sFc + Fp * V * TW;  // RK-updated state as store_rk writes it, [S][V][TW]
   load_tri_ops<A, N>(sops, a.dops);
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
@@ -458,6 +567,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_face(const __grid_constant__ Arg
       for (int v = 0; v < V; v++) Fv[v] = fvo[v * TW] + tau * (UL[v] - UB[v]);
     }
     const bool right = (code >= 0) && (code & 1);
+    A out[V];
 #pragma unroll
     for (int v = 0; v < V; v++)
     {
@@ -466,8 +576,9 @@ __global__ void __launch_bounds__(128) k_tri_ns_face(const __grid_constant__ Arg
         acc -= Fv[v] * dA;
       else
         acc += Fv[v] * dA;
-      sFc[(f * V + v) * TW + l] = acc;
+      out[v] = acc;
     }
+    st4(sFc + tvl(f, l), out);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
