@@ -32,11 +32,31 @@ struct TriShape
 };
 
 // Shared-memory tile arrays of these kernels (states, common solutions,
-// gradients, fluxes) keep the four variables of one (point, element)
-// together, [P][TW][4]: one 16-byte load (FP32) or two (FP64) fetch a point's
-// variables where the global [P][V][TW] order would take four loads, and the
-// eight elements of a warp's point cover 128 contiguous bytes.
-__device__ __forceinline__ int tvl(int p, int l) { return (p * TW + l) * 4; }
+// gradients, fluxes) keep the variables of one (point, element) in 16-byte
+// groups, [P][4/W][TW][W] with W = 16 / sizeof(A): FP32 holds all four
+// variables in one group, FP64 two groups of two.  One 16-byte load per group
+// fetches a point's variables where the global [P][V][TW] order takes four
+// loads, and the eight elements of a warp's point read 128 contiguous bytes
+// per group (no bank conflicts).
+template <typename A>
+struct TVec
+{
+  static constexpr int W = 16 / (int)sizeof(A), G = 4 / W;
+};
+
+// offset of (point p, element l, variable v)
+template <typename A>
+__device__ __forceinline__ int tix(int p, int l, int v)
+{
+  return ((p * TVec<A>::G + v / TVec<A>::W) * TW + l) * TVec<A>::W + v % TVec<A>::W;
+}
+
+// offset of (point p, element l)'s first group
+template <typename A>
+__device__ __forceinline__ int tvl(int p, int l)
+{
+  return tix<A>(p, l, 0);
+}
 
 __device__ __forceinline__ void ld4(const float *p, float x[4])
 {
@@ -47,10 +67,11 @@ __device__ __forceinline__ void ld4(const float *p, float x[4])
   x[3] = q.w;
 }
 
+// the second group of two doubles sits TW groups further on
 __device__ __forceinline__ void ld4(const double *p, double x[4])
 {
   const double2 a = *reinterpret_cast<const double2 *>(p);
-  const double2 b = *reinterpret_cast<const double2 *>(p + 2);
+  const double2 b = *reinterpret_cast<const double2 *>(p + 2 * TW);
   x[0] = a.x;
   x[1] = a.y;
   x[2] = b.x;
@@ -65,21 +86,21 @@ __device__ __forceinline__ void st4(float *p, const float x[4])
 __device__ __forceinline__ void st4(double *p, const double x[4])
 {
   *reinterpret_cast<double2 *>(p) = make_double2(x[0], x[1]);
-  *reinterpret_cast<double2 *>(p + 2) = make_double2(x[2], x[3]);
+  *reinterpret_cast<double2 *>(p + 2 * TW) = make_double2(x[2], x[3]);
 }
 
-// global [S][V][TW] tile -> shared [S][TW][4]
+// global [S][V][TW] tile -> the shared layout above
 template <typename T, typename A, int S>
 __device__ __forceinline__ void load_tile_vl(const T *__restrict__ src, A *dst)
 {
   for (int i = threadIdx.x; i < S * 4 * TW; i += blockDim.x)
   {
     const int l = i % TW, v = (i / TW) % 4, p = i / (4 * TW);
-    dst[tvl(p, l) + v] = src[i];
+    dst[tix<A>(p, l, v)] = src[i];
   }
 }
 
-// X_v(f) = sum_s E[f][s] Y_v(s) for the four variables of a [S][TW][4] array
+// X_v(f) = sum_s E[f][s] Y_v(s) for the four variables of a shared tile array
 template <typename A, int N>
 __device__ __forceinline__ void tri_extrap4(const A *sY, const A *E, int f, int l, A out[4])
 {
@@ -90,7 +111,7 @@ __device__ __forceinline__ void tri_extrap4(const A *sY, const A *E, int f, int 
   for (int t = 0; t < S; t++)
   {
     A x[4];
-    ld4(sY + tvl(t, l), x);
+    ld4(sY + tvl<A>(t, l), x);
     const A e = E[f * S + t];
 #pragma unroll
     for (int v = 0; v < 4; v++) out[v] += e * x[v];
@@ -157,7 +178,7 @@ __device__ __forceinline__ void tri_extrap_next(const Args<T, A> &a, int64_t til
   }
 }
 
-// transformed flux F~_d = adj[d][.] . F at solution point s into sF [D*S][TW][4]
+// transformed flux F~_d = adj[d][.] . F at solution point s into sF [D*S] points
 template <typename T, typename A>
 __device__ __forceinline__ void tri_transform(const Args<T, A> &a, int64_t tile, int s, int l, const A F[4][2],
                                               A *sF, int S)
@@ -174,7 +195,7 @@ __device__ __forceinline__ void tri_transform(const Args<T, A> &a, int64_t tile,
     A Ft[4];
 #pragma unroll
     for (int v = 0; v < 4; v++) Ft[v] = F[v][0] * adj[d1][0] + F[v][1] * adj[d1][1];
-    st4(sF + tvl(d1 * S + s, l), Ft);
+    st4(sF + tvl<A>(d1 * S + s, l), Ft);
   }
 }
 
@@ -204,7 +225,7 @@ __device__ __forceinline__ void tri_finish(const Args<T, A> &a, int64_t tile, in
     for (int k = 0; k < D * S; k++)
     {
       A x[4];
-      ld4(sF + tvl(k, l), x);
+      ld4(sF + tvl<A>(k, l), x);
 #pragma unroll
       for (int v = 0; v < V; v++) vol[v] += Dv[k] * x[v];
     }
@@ -214,7 +235,7 @@ __device__ __forceinline__ void tri_finish(const Args<T, A> &a, int64_t tile, in
   for (int f = 0; f < Fp; f++)
   {
     A x[4];
-    ld4(sFc + tvl(f, l), x);
+    ld4(sFc + tvl<A>(f, l), x);
 #pragma unroll
     for (int v = 0; v < V; v++) surf[v] += Dvf[f] * x[v];
   }
@@ -234,7 +255,7 @@ __global__ void __launch_bounds__(128) k_tri_euler(const __grid_constant__ Args<
   constexpr int S = G::S, Fp = G::Fp, V = G::V, D = 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sops = reinterpret_cast<A *>(smem_raw);
-  A *sU = sops + G::OPS_PAD;  // [S][TW][4]; then the RK-updated state as store_rk writes it
+  A *sU = sops + G::OPS_PAD;  // [S] points; then the RK-updated state as store_rk writes it
   A *sF = sU + S * V * TW;
   A *sFc = sF + D * S * V * TW;
   load_tri_ops<A, N>(sops, a.dops);
@@ -246,7 +267,7 @@ __global__ void __launch_bounds__(128) k_tri_euler(const __grid_constant__ Args<
   {
     const int s = it / TW, l = it % TW;
     A U[V], F[V][D], P, Pp;
-    ld4(sU + tvl(s, l), U);
+    ld4(sU + tvl<A>(s, l), U);
     flux_conv_stored<A, D>(U, F, P, Pp, a.ph);
     tri_transform<T, A>(a, tile, s, l, F, sF, S);
   }
@@ -269,7 +290,7 @@ __global__ void __launch_bounds__(128) k_tri_euler(const __grid_constant__ Args<
     A out[V];
 #pragma unroll
     for (int v = 0; v < V; v++) out[v] = right ? -Fc[v] * dA : Fc[v] * dA;
-    st4(sFc + tvl(f, l), out);
+    st4(sFc + tvl<A>(f, l), out);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
@@ -295,9 +316,9 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
   constexpr int S = G::S, Fp = G::Fp, V = G::V, D = 2, NM = 5;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sops = reinterpret_cast<A *>(smem_raw);
-  A *sU = sops + G::OPS_PAD;    // [S][TW][4]
-  A *sUC = sU + S * V * TW;      // [Fp][TW][4]
-  A *sdU = sUC + Fp * V * TW;    // [D*S][TW][4]: physical gradient, then F~
+  A *sU = sops + G::OPS_PAD;    // [S] points
+  A *sUC = sU + S * V * TW;      // [Fp] points
+  A *sdU = sUC + Fp * V * TW;    // [D*S] points: physical gradient, then F~
   load_tri_ops<A, N>(sops, a.dops);
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
@@ -339,7 +360,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
       ghost_state<A, D>(-code - 1, Ua, n, URa, UBa, a.ph);
       to_stored<A, D>(UBa, UC, a.ph);
     }
-    st4(sUC + tvl(f, l), UC);
+    st4(sUC + tvl<A>(f, l), UC);
   }
   __syncthreads();
   // gradient: oppD U + oppD_fpts Ucomm, then physical
@@ -363,7 +384,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
       for (int t = 0; t < S; t++)
       {
         A x[4];
-        ld4(sU + tvl(t, l), x);
+        ld4(sU + tvl<A>(t, l), x);
 #pragma unroll
         for (int v = 0; v < V; v++) acc[v] += Dd[t] * x[v];
       }
@@ -371,7 +392,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
       for (int f = 0; f < Fp; f++)
       {
         A x[4];
-        ld4(sUC + tvl(f, l), x);
+        ld4(sUC + tvl<A>(f, l), x);
 #pragma unroll
         for (int v = 0; v < V; v++) cor[v] += Df[f] * x[v];
       }
@@ -391,7 +412,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
       A g[V];
 #pragma unroll
       for (int v = 0; v < V; v++) g[v] = (tdU[v][0] * adj[0][d1] + tdU[v][1] * adj[1][d1]) * inv_det;
-      st4(sdU + tvl(d1 * S + s, l), g);
+      st4(sdU + tvl<A>(d1 * S + s, l), g);
     }
   }
   __syncthreads();
@@ -402,7 +423,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
     for (int i = threadIdx.x; i < D * S * V * TW; i += blockDim.x)
     {
       const int l = i % TW, v = (i / TW) % V, p = i / (V * TW);
-      g[i] = (T)sdU[tvl(p, l) + v];
+      g[i] = (T)sdU[tix<A>(p, l, v)];
     }
   }
   // own viscous normal flux at flux points
@@ -447,12 +468,12 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
   {
     const int s = it / TW, l = it % TW;
     A U[V], dU[V][D], F[V][D], P, Pp, Ua[V];
-    ld4(sU + tvl(s, l), U);
+    ld4(sU + tvl<A>(s, l), U);
 #pragma unroll
     for (int d = 0; d < D; d++)
     {
       A x[V];
-      ld4(sdU + tvl(d * S + s, l), x);
+      ld4(sdU + tvl<A>(d * S + s, l), x);
 #pragma unroll
       for (int v = 0; v < V; v++) dU[v][d] = x[v];
     }
@@ -474,7 +495,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_grad(const __grid_constant__ Arg
     for (int k = 0; k < D * S; k++)
     {
       A x[V];
-      ld4(sdU + tvl(k, l), x);
+      ld4(sdU + tvl<A>(k, l), x);
 #pragma unroll
       for (int v = 0; v < V; v++) vol[v] += Dv[k] * x[v];
     }
@@ -494,7 +515,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_face(const __grid_constant__ Arg
   constexpr int S = G::S, Fp = G::Fp, V = G::V, D = 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *sops = reinterpret_cast<A *>(smem_raw);
-  A *sFc = sops + G::OPS_PAD;   // [Fp][TW][4]
+  A *sFc = sops + G::OPS_PAD;   // [Fp] points
   A *sUnew = sFc + Fp * V * TW;  // RK-updated state as store_rk writes it, [S][V][TW]
   load_tri_ops<A, N>(sops, a.dops);
   const int64_t tile = blockIdx.x;
@@ -578,7 +599,7 @@ __global__ void __launch_bounds__(128) k_tri_ns_face(const __grid_constant__ Arg
         acc += Fv[v] * dA;
       out[v] = acc;
     }
-    st4(sFc + tvl(f, l), out);
+    st4(sFc + tvl<A>(f, l), out);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
