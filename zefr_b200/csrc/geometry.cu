@@ -434,6 +434,8 @@ double *scratch(Ctx *c, size_t doubles)
   const size_t bytes = doubles * sizeof(double);
   if (bytes > c->geo_work_bytes)
   {
+    // earlier geometry work queued on the stream may still read the old buffer
+    CK(cudaStreamSynchronize(c->stream));
     if (c->geo_work) cudaFree(c->geo_work);
     c->geo_work = nullptr;
     c->geo_work_bytes = 0;
