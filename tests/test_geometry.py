@@ -25,7 +25,8 @@ class _PlanView:
         self.nspts, self.nvars, self.neles = self.info.nspts, self.info.nvars, int(self.info.n_eles)
 
 
-@pytest.mark.parametrize("name", ["cyl_p3_ns_char_adi", "quad_p2_ns_jitter", "hex_p2_euler_jitter"])
+@pytest.mark.parametrize("name", ["cyl_p3_ns_char_adi", "quad_p2_ns_jitter", "hex_p2_euler_jitter",
+                                  "tri_p3_euler_char", "tri_p4_ns_jitter"])
 def test_geometry_map_reproduces_plan_metrics(name):
     g = gc.load(name)
     v = _PlanView(g)
@@ -53,3 +54,24 @@ def test_torch_wall_force_matches_oracle(name):
     cfp = v.plan.get("coord_fpts").reshape(Fp, 2, E)
     Fo, _ = dfr_numpy.wall_force(st, g.U0, np.array([w1[f % N] for f in range(Fp)]), cfp, g.params, g.viscous)
     assert np.abs(F - Fo[:2]).max() <= 1e-12 * np.abs(Fo).max()
+
+
+@pytest.mark.parametrize("name", ["cyl_p3_ns_char_adi", "hex_p2_euler_jitter", "tri_p3_euler_char"])
+def test_plan_nodes_and_shape_tables_give_the_coordinates(name):
+    """The element nodes and solution-point shape functions the plan exports
+    (inputs of the device geometry kernels) reproduce its solution-point
+    coordinates bit for bit when summed in node order, as the set-up does."""
+    g = gc.load(name)
+    v = _PlanView(g)
+    D, S, E = v.ndims, v.nspts, v.neles
+    nodes = v.plan.get("nodes").reshape(-1, D, E)
+    nn = nodes.shape[0]
+    sh = v.plan.get("shape_spts").reshape(S, nn)
+    X = np.zeros((S, D, E))
+    for n in range(nn):
+        X += sh[:, n][:, None, None] * nodes[n][None, :, :]
+    assert np.array_equal(X.reshape(-1), v.plan.get("coord_spts"))
+    # the element nodes are the mesh nodes each element names, in gmsh order
+    mesh_nodes = np.asarray(g.mesh.nodes)[:, :D]
+    e2n = np.asarray(g.mesh.elements)
+    assert np.array_equal(nodes, mesh_nodes[e2n].transpose(1, 2, 0))
