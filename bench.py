@@ -19,6 +19,7 @@ beside it, and the two forms' kinetic-energy histories are compared.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -607,12 +608,22 @@ def reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return None
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    if world > 1:
+        # torchrun sets OMP_NUM_THREADS=1 for every rank; only this rank works
+        # here, so the reference gets all host cores (the environment for an
+        # OpenMP runtime not loaded yet, the call for one already loaded)
+        threads = os.cpu_count() or 1
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        try:
+            ctypes.CDLL("libgomp.so.1").omp_set_num_threads(threads)
+        except (OSError, AttributeError):
+            pass
     from oracle import refcpu
     if not refcpu.available(fast=True):
         return {"impl": "reference", "unavailable": "oracle/_ref/libzefr_ref_fast.so not built (make -C oracle)"}
     from zefr_b200 import ics, meshgen
     n = args.ref_cells
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     with tempfile.TemporaryDirectory() as tmp:
         mesh = meshgen.box_hexes(n, n, n)
         meshgen.write_gmsh(mesh, os.path.join(tmp, "tgv.msh"))
