@@ -2,7 +2,7 @@
 benchmarks and tests start from, and the cylinder O-mesh whose node
 positions the drag gradient differentiates (it must be affine in the wall
 coefficients, since the gradient sums node adjoints against one displacement
-field per coefficient)."""
+field per coefficient), and the seeded parameters of the batched workload."""
 import math
 
 import numpy as np
@@ -94,3 +94,18 @@ def test_cylinder_mesh_generator_matches_its_description():
     names = sorted({f[2] for f in m.bnd_faces})
     assert names == ["FARFIELD", "WALL"]
     assert sum(1 for f in m.bnd_faces if f[2] == "WALL") == 8
+
+
+def test_batched_vortex_case_parameters():
+    from zefr_b200.batch import vortex_case_params
+    cases = vortex_case_params(512, 4)
+    assert cases == vortex_case_params(512, 4) and cases != vortex_case_params(512, 5)
+    n = np.array([c["n"] for c in cases])
+    P = np.array([c["P"] for c in cases])
+    assert n.min() >= 8 and n.max() <= 96 and set(P.tolist()) == {1, 2, 3, 4, 5}
+    for c in cases:
+        assert all(-2.0 <= x <= 2.0 for x in c["center"])
+        assert 1.0 <= c["beta"] <= 5.0 and 0.2 <= c["mach"] <= 0.8
+        h = 10.0 / c["n"]
+        want = 0.1 * h / ((c["mach"] + 1.0) * math.sqrt(1.4) * (c["P"] + 1) ** 2)
+        assert c["dt"] == want

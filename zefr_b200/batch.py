@@ -20,13 +20,16 @@ from ._lib import check, lib
 from .solver import FRSolver, make_params
 
 
-def vortex_cases(ncases: int, seed: int, n_range=(8, 96), orders=(1, 5), precision: str = "mixed",
-                 dt_cfl: float = 0.1) -> List[FRSolver]:
-    """Seeded batched-vortex workload; dt = dt_cfl * h / ((Ma + 1) c (P + 1)^2)
-    per case (a fixed fraction of the explicit stability limit)."""
+def vortex_case_params(ncases: int, seed: int, n_range=(8, 96), orders=(1, 5), dt_cfl: float = 0.1,
+                       gamma: float = 1.4) -> List[dict]:
+    """Parameters of the seeded batched-vortex workload, one dict per case:
+    mesh size n (n x n quads on [-5,5]^2) and order P uniform in their
+    ranges, vortex centre uniform in [-2,2]^2, strength beta uniform in
+    [1,5], stream Mach uniform in [0.2,0.8], and dt = dt_cfl * h /
+    ((Ma + 1) c (P + 1)^2) (a fixed fraction of the explicit stability
+    limit)."""
     rng = np.random.default_rng(seed)
     out = []
-    gamma = 1.4
     for _ in range(ncases):
         n = int(rng.integers(n_range[0], n_range[1] + 1))
         P = int(rng.integers(orders[0], orders[1] + 1))
@@ -36,11 +39,25 @@ def vortex_cases(ncases: int, seed: int, n_range=(8, 96), orders=(1, 5), precisi
         c = math.sqrt(gamma)
         h = 10.0 / n
         dt = dt_cfl * h / ((mach + 1.0) * c * (P + 1) ** 2)
-        p = make_params(P, False, gamma=gamma, precision=precision, dt=dt)
+        out.append({"n": n, "P": P, "center": center.tolist(), "beta": beta, "mach": mach, "dt": dt})
+    return out
+
+
+def vortex_cases(ncases: int, seed: int, n_range=(8, 96), orders=(1, 5), precision: str = "mixed",
+                 dt_cfl: float = 0.1) -> List[FRSolver]:
+    """Seeded batched-vortex workload (vortex_case_params): one solver per
+    case with the vortex state set; the parameters are kept as ``s.case``."""
+    gamma = 1.4
+    c = math.sqrt(gamma)
+    out = []
+    for case in vortex_case_params(ncases, seed, n_range, orders, dt_cfl, gamma):
+        n, P = case["n"], case["P"]
+        p = make_params(P, False, gamma=gamma, precision=precision, dt=case["dt"])
         s = FRSolver(meshgen.box_quads(n, n), p, {"PERIODIC": "periodic"})
         X = s.plan.get("coord_spts").reshape(s.nspts, 2, s.neles)
-        s.set_state(ics.isentropic_vortex(X, beta=beta, center=tuple(center), u_inf=(mach * c, 0.0), gamma=gamma))
-        s.case = {"n": n, "P": P, "center": center.tolist(), "beta": beta, "mach": mach, "dt": dt}
+        s.set_state(ics.isentropic_vortex(X, beta=case["beta"], center=tuple(case["center"]),
+                                          u_inf=(case["mach"] * c, 0.0), gamma=gamma))
+        s.case = case
         out.append(s)
     return out
 
