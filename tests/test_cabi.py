@@ -103,3 +103,19 @@ def test_params_from_deck_matches_reference_nondim():
     c = np.sqrt(1.4)
     assert abs(p.V_fs[0] - 0.1 * c) < 1e-15
     assert abs(p.mu - 0.1 * c / 1600) < 1e-17
+
+
+def test_adjoint_and_geometry_entry_points_reject_a_null_context():
+    """The step adjoint and geometry entry points check their context before
+    touching the GPU: a null one is ZB_ERR_ARG with a message, no crash."""
+    L = _lib.lib()
+    calls = {
+        "zb_rk_step_vjp": lambda: L.zb_rk_step_vjp(None, None, None, None, 1, 1, 1, _lib.ZB_HOST, None, 0),
+        "zb_geometry_eval": lambda: L.zb_geometry_eval(None, None, None, None, None, None, _lib.ZB_HOST),
+        "zb_geometry_eval_vjp": lambda: L.zb_geometry_eval_vjp(None, None, None, None, None, None, None,
+                                                               _lib.ZB_HOST),
+        "zb_set_nodes": lambda: L.zb_set_nodes(None, None, _lib.ZB_HOST),
+    }
+    for name, call in calls.items():
+        assert call() == -1, name
+        assert b"null" in L.zb_last_error(), name
