@@ -181,29 +181,38 @@ zb_status zb_plan_info(const zb_plan *plan, zb_info *out);
  * reference normals), dshape_spts [dim][spt][node], dshape_fpts
  * [dim][fpt][node], shape_fpts [fpt][node], shape_spts [spt][node] (shape
  * functions, gmsh node order; for geometry derivatives), nodes
- * [node][dim][ele] (element node coordinates, Elements::nodes).  With out == NULL, *n receives the element count. */
+ * [node][dim][ele] (element node coordinates, Elements::nodes).  With
+ * out == NULL, *n receives the array's length. */
 zb_status zb_plan_get(const zb_plan *plan, const char *name, double *out, int64_t *n);
 
-/* Create a device context from a plan on the current device. */
+/* Create a device context from a plan on the current device: the device side
+ * of FRSolver::setup (src/solver.cpp:55-437, include/solver.hpp:150), which
+ * allocates and fills the solver's arrays; zb_destroy releases them. */
 zb_status zb_create(const zb_plan *plan, zb_ctx **out);
 /* Convenience: mesh + params -> plan -> context. */
 zb_status zb_create_from_mesh(const zb_mesh *mesh, const zb_params *params, zb_ctx **out);
 void zb_destroy(zb_ctx *ctx);
 zb_status zb_info_get(const zb_ctx *ctx, zb_info *out);
 
-/* Use a caller-provided CUDA stream (cudaStream_t) for all later work. */
+/* Use a caller-provided CUDA stream (cudaStream_t) for all later work.  No
+ * reference counterpart (the reference launches on its own streams). */
 zb_status zb_set_stream(zb_ctx *ctx, void *stream);
+/* The fixed time step: the deck's dt (src/input.cpp:74, InputStruct::dt). */
 zb_status zb_set_dt(zb_ctx *ctx, double dt);
 
-/* State access with get_q_spts strides (in doubles).  where: ZB_HOST/ZB_DEVICE.
- * zb_set_state copies and converts into the context's layout and precision. */
+/* State access with the strides of zefr::get_q_spts / get_q_spts_d
+ * (include/zefr_interface.hpp:126-129, src/zefr.cpp:607-645), in doubles.
+ * where: ZB_HOST/ZB_DEVICE.  zb_set_state copies and converts into the
+ * context's layout and precision. */
 zb_status zb_set_state(zb_ctx *ctx, const double *U, int64_t spt_stride, int64_t var_stride,
                        int64_t ele_stride, int where);
 zb_status zb_get_state(zb_ctx *ctx, double *U, int64_t spt_stride, int64_t var_stride,
                        int64_t ele_stride, int where);
 
-/* FRSolver::compute_residual(stage): divF_spts(stage) = |J| * div F in
- * reference form (physical residual is -divF/|J|). */
+/* FRSolver::compute_residual(stage) (include/solver.hpp:152,
+ * src/solver.cpp:1494-1645): divF_spts(stage) = |J| * div F in reference
+ * form (physical residual is -divF/|J|); zb_get_residual reads that register
+ * (Elements::divF_spts, include/elements.hpp:91) with caller strides. */
 zb_status zb_compute_residual(zb_ctx *ctx, unsigned stage);
 zb_status zb_get_residual(zb_ctx *ctx, unsigned stage, double *out, int64_t spt_stride,
                           int64_t var_stride, int64_t ele_stride, int where);
@@ -391,10 +400,12 @@ int64_t zb_batch_launch_count(const zb_batch *batch);
 zb_status zb_vjp(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride, int64_t var_stride,
                  int64_t ele_stride, int where, double *param_bar);
 
-/* Wait for all work queued on the context's stream. */
+/* Wait for all work queued on the context's stream.  No reference
+ * counterpart (its calls synchronise internally). */
 zb_status zb_synchronize(zb_ctx *ctx);
 
-/* Number of kernels this library launched on the context since creation. */
+/* Number of kernels this library launched on the context since creation.
+ * No reference counterpart. */
 int64_t zb_launch_count(const zb_ctx *ctx);
 
 /* Per-kernel device timing with CUDA events recorded on the context's stream
