@@ -94,9 +94,18 @@ class Clocks:
         time.sleep(0.25)
         self.proc.terminate()
         self.proc.wait(timeout=10)
+        with open(self.path) as f:
+            out = self.summary(f)
+        os.unlink(self.path)
+        return out
+
+    @staticmethod
+    def summary(lines):
+        """Median SM clock, maximum clock, sample count and the throttle
+        reasons seen Active, from nvidia-smi CSV lines in FIELDS order."""
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -108,7 +117,6 @@ class Clocks:
             for nm, val in zip(names, parts[5:9]):
                 if val.lower() == "active":
                     reasons.add(nm)
-        os.unlink(self.path)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
                 "reasons": sorted(reasons)}
 
