@@ -430,8 +430,12 @@ const char *zb_kernel_name(int id);
  * into that array, packs it, and runs the same kernels as
  * zb_compute_residual on `stream` (a cudaStream_t, or NULL for the default
  * stream), returning without synchronising.
+ * Every call copies the plan's geometry (adjugate, |J|, normals, dA,
+ * connectivity) from the plan's pageable host arrays: a few bytes per
+ * solution and flux point over PCIe, on top of the residual's own work.
  * The first call on each device looks up the array's device address, with
- * that device current; make that first call before any stream capture.
+ * that device current.  Do not record calls into a CUDA graph: the host
+ * copies read the plan's host memory at the time of the call.
  * All calls share the array: calls whose work overlaps on the GPU (other
  * streams, other host threads, other plans) race on it. */
 zb_status zb_compute_residual_noalloc(const zb_plan *plan, const double *U, double *divF, void *stream);

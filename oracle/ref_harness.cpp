@@ -6,14 +6,20 @@
  * read_input_file -> FRSolver::setup), overwrite the state, call
  * FRSolver::compute_residual (src/solver.cpp:1494-1645) or FRSolver::update
  * (src/solver.cpp:2598-2644), and read back the residual, state, operators,
- * metrics and face connectivity for comparison.
+ * metrics and face connectivity for comparison.  The diagnostics are the
+ * reference's own: report_residuals (src/solver.cpp:6990-7137),
+ * report_turbulent_stats (7813-7917) and compute_moments (7600-7811), run on
+ * the arrays the last compute_residual left.
  *
  * Layouts returned are the reference's own row-major mdvector layouts
  * (include/mdvector.hpp:189-260) with nElesPad == nEles on the CPU build
  * (src/elements.cpp:71-75).
  */
 #include <algorithm>
+#include <array>
+#include <chrono>
 #include <cmath>
+#include <fstream>
 #include <cstdio>
 #include <cstring>
 #include <exception>
@@ -215,6 +221,97 @@ int zr_update(void *p, int nsteps)
     {
       h->solver->update();
       h->input.iter++;
+    }
+    return 0;
+  }
+  catch (std::exception &e)
+  {
+    return fail(e);
+  }
+}
+
+/* report_residuals (src/solver.cpp:6990-7137) on divF_spts(0) as the last
+ * compute_residual left it: out[n] = the value the reference prints for
+ * variable n (max, sum of |.| or sqrt of the sum of squares of divF/|J| over
+ * solution points, per res_type 0/1/2, divided by nSpts * nEles), read from
+ * FRSolver::res_max with res_field = n.  Terminal and history output are
+ * dropped. */
+int zr_report_residuals(void *p, int res_type, double *out)
+{
+  try
+  {
+    auto *h = static_cast<RefHandle *>(p);
+    auto &in = h->input;
+    const unsigned old_type = in.res_type, old_field = in.res_field;
+    std::ofstream hist;  // never opened: the history lines go nowhere
+    std::streambuf *old = std::cout.rdbuf();
+    std::ostringstream sink;
+    std::cout.rdbuf(sink.rdbuf());
+    in.res_type = (unsigned)res_type;
+    for (unsigned n = 0; n < h->solver->eles->nVars; n++)
+    {
+      in.res_field = n;
+      h->solver->report_residuals(hist, std::chrono::high_resolution_clock::now());
+      out[n] = h->solver->res_max;
+    }
+    std::cout.rdbuf(old);
+    in.res_type = old_type;
+    in.res_field = old_field;
+    return 0;
+  }
+  catch (std::exception &e)
+  {
+    return fail(e);
+  }
+}
+
+/* report_turbulent_stats (src/solver.cpp:7813-7917) on U_spts and the
+ * physical gradient dU_spts the last compute_residual left: the reference
+ * writes "iter flow_time ke enstrophy" (17 significant digits) to the history
+ * file at `path`; out[0] = ke, out[1] = enstrophy as written there, both
+ * already divided by vol * rho_fs * |V_fs|^2; out[2] = that divisor. */
+int zr_turbulent_stats(void *p, const char *path, double *out)
+{
+  try
+  {
+    auto *h = static_cast<RefHandle *>(p);
+    std::streambuf *old = std::cout.rdbuf();
+    std::ostringstream sink;
+    std::cout.rdbuf(sink.rdbuf());
+    {
+      std::ofstream f(path);
+      h->solver->report_turbulent_stats(f);
+    }
+    std::cout.rdbuf(old);
+    std::ifstream g(path);
+    double iter = 0, t = 0;
+    if (!(g >> iter >> t >> out[0] >> out[1])) throw std::runtime_error("turbulent stats not written");
+    double vol = 0;
+    for (auto e : h->solver->elesObjs)
+      for (unsigned k = 0; k < e->nEles; k++) vol += e->vol(k);
+    out[2] = vol * h->input.rho_fs * h->input.v_mag_fs * h->input.v_mag_fs;
+    return 0;
+  }
+  catch (std::exception &e)
+  {
+    return fail(e);
+  }
+}
+
+/* compute_moments (src/solver.cpp:7600-7811) on the face arrays (P, U, dU)
+ * the last compute_residual left: out[0..2] total force, out[3..5] moment
+ * about geo.x_cg. */
+int zr_compute_moments(void *p, double *out)
+{
+  try
+  {
+    auto *h = static_cast<RefHandle *>(p);
+    std::array<double, 3> force, moment;
+    h->solver->compute_moments(force, moment, nullptr);
+    for (int d = 0; d < 3; d++)
+    {
+      out[d] = force[d];
+      out[3 + d] = moment[d];
     }
     return 0;
   }

@@ -47,6 +47,9 @@ def _lib(fast: bool) -> ctypes.CDLL:
         lib.zr_compute_residual.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.zr_get_residual.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         lib.zr_update.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.zr_report_residuals.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        lib.zr_turbulent_stats.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+        lib.zr_compute_moments.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         lib.zr_get_array.restype = ctypes.c_long
         lib.zr_get_array.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.c_long]
         _libs[path] = lib
@@ -122,6 +125,35 @@ class RefSolver:
     def update(self, nsteps: int = 1) -> None:
         if self.lib.zr_update(self.h, nsteps) != 0:
             raise RuntimeError(self.lib.zr_last_error().decode())
+
+    def report_residuals(self, res_type: int) -> np.ndarray:
+        """The per-variable residual the reference's report_residuals prints
+        for ``res_type`` (0 max, 1 L1, 2 L2 of divF/|J|, divided by the number
+        of solution points) after the last compute_residual."""
+        out = np.zeros(self.nvars)
+        if self.lib.zr_report_residuals(self.h, res_type, _dp(out)) != 0:
+            raise RuntimeError(self.lib.zr_last_error().decode())
+        return out
+
+    def turbulent_stats(self) -> Dict[str, float]:
+        """Kinetic energy and enstrophy as the reference's
+        report_turbulent_stats writes them (normalised by vol rho_fs |V_fs|^2),
+        with that normaliser, after the last compute_residual."""
+        import tempfile
+        out = np.zeros(3)
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, "turb_stats.dat")
+            if self.lib.zr_turbulent_stats(self.h, path.encode(), _dp(out)) != 0:
+                raise RuntimeError(self.lib.zr_last_error().decode())
+        return {"ke": float(out[0]), "enstrophy": float(out[1]), "norm": float(out[2])}
+
+    def compute_moments(self) -> Dict[str, np.ndarray]:
+        """Wall force and moment of the reference's compute_moments after the
+        last compute_residual."""
+        out = np.zeros(6)
+        if self.lib.zr_compute_moments(self.h, _dp(out)) != 0:
+            raise RuntimeError(self.lib.zr_last_error().decode())
+        return {"force": out[:3].copy(), "moment": out[3:].copy()}
 
     def array(self, name: str) -> np.ndarray:
         n = self.lib.zr_get_array(self.h, name.encode(), None, 0)

@@ -9,7 +9,11 @@ synthetic meshes of every workload shape, with seeded states, and stores:
   U0, R0        input state and divF_spts(0) = reference compute_residual(0)
   Un            state after ``nsteps`` reference RK44 steps (FRSolver::update)
 
-and, under tests/golden/time/, time-integration cases (RK54 with and without
+under tests/golden/diag/, the reference's own diagnostics at U0 after
+compute_residual(0) (report_residuals for res_type 0/1/2, report_turbulent_stats
+for 3D Navier-Stokes, compute_moments for cases with walls), under
+tests/golden/traj/ long RK44 trajectories (the state after every block of
+steps), and, under tests/golden/time/, time-integration cases (RK54 with and without
 the adaptive controller, RK44 with CFL time steps) holding the mesh, deck,
 U0, the reference's dt(0) after every step, its per-element dt array after
 the last step and the final state.
@@ -263,9 +267,106 @@ def make_time_case(name, spec, tmp):
     return out
 
 
+DIAG_DIR = os.path.join(HERE, "diag")
+WALL_NAMES = ("wall_slip", "wall_ns_iso", "wall_ns_adi")
+
+
+def make_diag_case(name, spec, tmp):
+    """The reference's diagnostics on the committed golden state U0 of case
+    ``name`` (its residual at U0 must equal the committed R0 bit for bit)."""
+    build, ndims, order, viscous, bounds, deck, _state_fn, _nsteps = spec
+    gold = np.load(os.path.join(HERE, name + ".npz"))
+    mesh = build()
+    meshgen.write_gmsh(mesh, os.path.join(tmp, name + ".msh"))
+    deck_path = refcpu.write_deck(os.path.join(tmp, name + ".deck"), name + ".msh", ndims, order, viscous,
+                                  bounds, deck)
+    r = refcpu.RefSolver(deck_path)
+    R0 = r.residual(gold["U0"], 0)
+    if not np.array_equal(R0, gold["R0"]):
+        raise RuntimeError(f"{name}: reference residual differs from the committed golden")
+    out = {"U0_crc": np.array(zlib.crc32(gold["U0"].tobytes()))}
+    for t, key in ((0, "res_max"), (1, "res_l1"), (2, "res_l2")):
+        out[key] = r.report_residuals(t)
+    if ndims == 3 and viscous:
+        ts = r.turbulent_stats()
+        out["turb"] = np.array([ts["ke"], ts["enstrophy"], ts["norm"]])
+    if any(b in WALL_NAMES for b in bounds.values()):
+        m = r.compute_moments()
+        out["force"], out["moment"] = m["force"], m["moment"]
+    r.close()
+    os.makedirs(DIAG_DIR, exist_ok=True)
+    path = os.path.join(DIAG_DIR, name + ".npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
+TRAJ_DIR = os.path.join(HERE, "traj")
+
+
+def _traj_cases():
+    """name -> (mesh builder, ndims, order, viscous, bounds, deck, state builder, checkpoint steps)."""
+    def vortex(X, g):
+        return ics.isentropic_vortex(X, beta=5.0, gamma=g)
+
+    def supersonic_vortex(X, g):
+        # a weak vortex on a Mach 2 stream (p = rho = 1 far away: c = sqrt(gamma))
+        return ics.isentropic_vortex(X, beta=0.5, u_inf=(2.0 * math.sqrt(g), 0.0), gamma=g)
+
+    eul = {"mach_fs": 0.3, "rho_fs": 1.0, "P_fs": 1.0}
+    return {
+        # the vortex workload as specified: 32 x 32 quads on periodic [-5,5]^2,
+        # P3, Rusanov, gamma 1.4, beta 5 vortex on a unit stream, RK44 with
+        # dt 1e-3 for 1000 steps; the state is kept after 1, 10, 100 and 1000
+        "quad_p3_vortex_32x32_rk44_1000": (lambda: meshgen.box_quads(32, 32), 2, 3, False,
+                                           {"PERIODIC": "periodic"}, dict(eul, dt=1e-3), vortex, (1, 10, 100, 1000)),
+        # supersonic inflow on the left, supersonic outflow on the right, slip
+        # walls top and bottom; the vortex leaves through the outflow
+        "quad_p2_supin_supout_slip": (lambda: meshgen.box_quads(8, 6, -1.0, 1.0, -0.75, 0.75,
+                                                                bnd=("INFLOW", "OUTFLOW", "WALL", "WALL")),
+                                      2, 2, False, {"INFLOW": "inlet_sup", "OUTFLOW": "outlet_sup", "WALL": "wall_slip"},
+                                      {"mach_fs": 2.0, "rho_fs": 1.0, "P_fs": 1.0, "dt": 2e-3}, supersonic_vortex,
+                                      (1, 10, 100, 200)),
+    }
+
+
+def make_traj_case(name, spec, tmp):
+    """Reference RK44 trajectory: U0 and the state after each checkpoint step count."""
+    build, ndims, order, viscous, bounds, deck, state_fn, checkpoints = spec
+    mesh = build()
+    meshgen.write_gmsh(mesh, os.path.join(tmp, name + ".msh"))
+    deck_path = refcpu.write_deck(os.path.join(tmp, name + ".deck"), name + ".msh", ndims, order, viscous,
+                                  bounds, deck)
+    r = refcpu.RefSolver(deck_path)
+    S, V, E = r.state_shape
+    X = r.array("coord_spts").reshape(S, ndims, E)
+    U0 = state_fn(X, r.params["gamma"])
+    r.set_state(U0)
+    states, done = [], 0
+    for k in checkpoints:
+        r.update(k - done)
+        done = k
+        states.append(r.get_state())
+    faces_t = np.array([f[0] for f in mesh.bnd_faces], dtype=np.int64)
+    npf = max((len(f[1]) for f in mesh.bnd_faces), default=1)
+    faces_n = np.full((len(mesh.bnd_faces), npf), -1, dtype=np.int64)
+    for i, f in enumerate(mesh.bnd_faces):
+        faces_n[i, :len(f[1])] = f[1]
+    faces_name = np.array([f[2] for f in mesh.bnd_faces])
+    meta = {"name": name, "ndims": ndims, "order": order, "viscous": bool(viscous), "bounds": bounds,
+            "deck": deck, "params": r.params, "checkpoints": list(checkpoints), "dt": r.params["dt"],
+            "shape": [S, V, E], "gmsh_type": mesh.gmsh_type}
+    os.makedirs(TRAJ_DIR, exist_ok=True)
+    out = os.path.join(TRAJ_DIR, name + ".npz")
+    np.savez_compressed(out, meta=json.dumps(meta), nodes=mesh.nodes, elements=mesh.elements, faces_type=faces_t,
+                        faces_nodes=faces_n, faces_name=faces_name, U0=U0, states=np.array(states))
+    r.close()
+    return out
+
+
 def main(names=None):
     with tempfile.TemporaryDirectory() as tmp:
-        for table, fn in ((_cases(), make_case), (_time_cases(), make_time_case)):
+        for table, fn in ((_cases(), make_case), (_time_cases(), make_time_case), (_cases(), make_diag_case),
+                          (_traj_cases(), make_traj_case)):
             for name, spec in table.items():
                 if names and name not in names:
                     continue

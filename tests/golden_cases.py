@@ -108,3 +108,70 @@ def load_time(name: str) -> TimeGolden:
                 bnd_faces=faces)
     return TimeGolden(name=name, meta=meta, mesh=mesh, bounds=meta["bounds"], params=meta["params"], U0=z["U0"],
                       Un=z["Un"], dt0=z["dt0"], dt_ele=z["dt_ele"])
+
+
+DIAG_DIR = os.path.join(GOLDEN_DIR, "diag")
+
+
+def diag_names() -> List[str]:
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(DIAG_DIR, "*.npz")))
+
+
+def load_diag(name: str) -> Dict[str, np.ndarray]:
+    """The reference's own diagnostics at the golden case's U0 after
+    compute_residual(0): res_max / res_l1 / res_l2 (report_residuals, per
+    variable, divided by the solution point count), turb = (ke, enstrophy,
+    normaliser) of report_turbulent_stats (3D Navier-Stokes cases), force and
+    moment of compute_moments (cases with walls)."""
+    z = np.load(os.path.join(DIAG_DIR, name + ".npz"), allow_pickle=False)
+    return {k: z[k] for k in z.files}
+
+
+TRAJ_DIR = os.path.join(GOLDEN_DIR, "traj")
+
+
+@dataclass
+class TrajGolden:
+    """Long RK44 trajectory of the reference: U0 and the state after each
+    step count in meta["checkpoints"] (states[i])."""
+    name: str
+    meta: Dict
+    mesh: Mesh
+    bounds: Dict[str, str]
+    params: Dict[str, float]
+    U0: np.ndarray
+    states: np.ndarray
+
+    @property
+    def viscous(self) -> bool:
+        return bool(self.meta["viscous"])
+
+    @property
+    def order(self) -> int:
+        return int(self.meta["order"])
+
+
+def traj_names() -> List[str]:
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(TRAJ_DIR, "*.npz")))
+
+
+def load_traj(name: str) -> TrajGolden:
+    z = np.load(os.path.join(TRAJ_DIR, name + ".npz"), allow_pickle=False)
+    meta = json.loads(str(z["meta"]))
+    faces = []
+    for t, nodes, nm in zip(z["faces_type"], z["faces_nodes"], z["faces_name"]):
+        faces.append((int(t), tuple(int(n) for n in nodes if n >= 0), str(nm)))
+    mesh = Mesh(ndims=meta["ndims"], nodes=z["nodes"], gmsh_type=meta["gmsh_type"], elements=z["elements"],
+                bnd_faces=faces)
+    return TrajGolden(name=name, meta=meta, mesh=mesh, bounds=meta["bounds"], params=meta["params"], U0=z["U0"],
+                      states=z["states"])
+
+
+def comp_err(a: np.ndarray, b: np.ndarray, floor: float = 1e-6) -> float:
+    """Largest relative difference per component, |a-b| / |b|, over the
+    components whose magnitude is at least ``floor`` times the largest |b| of
+    the same variable (below that, a component is a cancellation residue
+    whose relative difference measures nothing)."""
+    scale = np.abs(b).max(axis=(0, 2), keepdims=True)
+    mask = np.abs(b) >= floor * scale
+    return float((np.abs(a - b)[mask] / np.abs(b)[mask]).max())

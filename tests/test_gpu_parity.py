@@ -313,3 +313,57 @@ def test_wall_force_matches_oracle(name):
     assert scale > 0
     assert np.abs(out["force"] - F).max() <= 1e-12 * scale
     assert np.abs(out["moment"] - M).max() <= 1e-12 * max(np.abs(M).max(), scale)
+
+
+@pytest.mark.parametrize("name", gc.diag_names())
+def test_residual_norms_match_reference(name):
+    """zb_residual_norms against the values the reference's own
+    report_residuals (src/solver.cpp:6990-7137) prints for res_type 0, 1, 2."""
+    g, d = gc.load(name), gc.load_diag(name)
+    s = solver_for(g)
+    s.set_state(g.U0)
+    s.compute_residual(0)
+    n = s.residual_norms()
+    for mine, ref in (("linf", "res_max"), ("l1", "res_l1"), ("l2", "res_l2")):
+        assert np.abs(n[mine] - d[ref]).max() <= 1e-12 * np.abs(d[ref]).max(), mine
+
+
+@pytest.mark.parametrize("name", [n for n in gc.diag_names() if "turb" in gc.load_diag(n)])
+def test_functionals_match_reference(name):
+    """zb_functionals (kinetic energy, enstrophy, volume), normalised as the
+    reference's report_turbulent_stats (src/solver.cpp:7813-7917) prints them,
+    against its own output on the same state."""
+    g, d = gc.load(name), gc.load_diag(name)
+    s = solver_for(g)
+    s.set_state(g.U0)
+    f = s.functionals()
+    ke, en, norm = d["turb"]
+    vfs2 = sum(g.params[f"V_fs{i}"] ** 2 for i in range(3))
+    assert abs(f["volume"] * g.params["rho_fs"] * vfs2 - norm) <= 1e-13 * norm
+    assert abs(f["ke"] / norm - ke) <= 1e-12 * abs(ke)
+    assert abs(f["enstrophy"] / norm - en) <= 1e-12 * abs(en)
+
+
+@pytest.mark.parametrize("name", [n for n in gc.diag_names() if "force" in gc.load_diag(n)])
+def test_wall_force_matches_reference(name):
+    """zb_wall_force against the reference's own compute_moments
+    (src/solver.cpp:7600-7811, 2D branch) on the same state."""
+    g, d = gc.load(name), gc.load_diag(name)
+    s = solver_for(g)
+    s.set_state(g.U0)
+    out = s.wall_force()
+    scale = np.abs(d["force"]).max()
+    assert scale > 0
+    assert np.abs(out["force"] - d["force"]).max() <= 1e-12 * scale
+    assert np.abs(out["moment"] - d["moment"]).max() <= 1e-12 * max(np.abs(d["moment"]).max(), scale)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_residual_fp64_per_component(name):
+    """1e-12 relative per component: every residual component at least 1e-6 of
+    its variable's largest magnitude matches the reference to 1e-12 of
+    itself (smaller components are cancellation residues)."""
+    g = gc.load(name)
+    s = solver_for(g)
+    R = s.residual(g.U0, 0)
+    assert gc.comp_err(R, g.R0) < 1e-12

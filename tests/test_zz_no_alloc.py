@@ -29,7 +29,8 @@ def _noalloc(plan, U_dev, out_dev, stream=None):
                                                   ctypes.cast(out_dev.data_ptr(), _DP), stream)
 
 
-@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "hex_p3_ns_tgv", "cyl_p3_ns_char_adi"])
+@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "hex_p3_ns_tgv", "hex_p1_ns", "hex_p2_euler_jitter",
+                                  "hex_p4_euler", "cyl_p3_ns_char_adi"])
 def test_noalloc_matches_allocating_path(name):
     import torch
     g = gc.load(name)

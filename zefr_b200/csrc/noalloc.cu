@@ -10,12 +10,14 @@
 // file-scope device array below, which exists on every GPU that loads this
 // library until the process exits.
 //
-// It computes the FP64 residual with the same kernels as zb_compute_residual.
+// It computes the FP64 residual with the same kernels as zb_compute_residual:
+// the column-mapped k_hex_* kernels for hexahedra (with the one-sided common
+// flux under beta = +-1/2), the point-mapped kernels for quadrilaterals.
 #include <cstring>
 #include <mutex>
 
-#include "context.hpp"
-#include "dfr_kernels.cuh"
+#include "ctx_impl.cuh"
+#include "hex_kernels.cuh"
 
 namespace zb {
 namespace {
@@ -145,9 +147,16 @@ int blocks_for(int64_t work)
   return (int)(b < 1 ? 1 : b);
 }
 
+// hexahedral Navier-Stokes with beta = +-1/2: the gradient kernel forms the
+// common flux at the flux points whose side supplies the LDG normal flux
+bool one_sided_common_flux(const Plan &p)
+{
+  return p.ndims == 3 && p.params.viscous && (p.params.ldg_b == 0.5 || p.params.ldg_b == -0.5);
+}
+
 struct Regions
 {
-  size_t inv, det, fnorm, fdA, partner, slot, mets, fgeo, nbr, U, Ufp, divF, divF_vol, Fvn, total;
+  size_t inv, det, fnorm, fdA, partner, slot, mets, fgeo, nbr, U, Ufp, divF, divF_vol, Fvn, Fcom, total;
 };
 
 Regions layout(const Plan &p)
@@ -175,6 +184,7 @@ Regions layout(const Plan &p)
   r.divF = take(nt * S * V * TW * 8);
   r.divF_vol = p.params.viscous ? take(nt * S * V * TW * 8) : 0;
   r.Fvn = p.params.viscous ? take(nt * Fp * V * TW * 8) : 0;
+  r.Fcom = one_sided_common_flux(p) ? take(nt * Fp * V * TW * 8) : 0;
   r.total = off;
   return r;
 }
@@ -210,27 +220,41 @@ void run_kernels(const Plan &p, unsigned char *base, const Regions &r, cudaStrea
   a.divF = reinterpret_cast<double *>(base + r.divF);
   a.divF_vol = p.params.viscous ? reinterpret_cast<double *>(base + r.divF_vol) : nullptr;
   a.Fvn = p.params.viscous ? reinterpret_cast<double *>(base + r.Fvn) : nullptr;
+  a.Fcom = one_sided_common_flux(p) ? reinterpret_cast<double *>(base + r.Fcom) : nullptr;
   a.ntiles = p.ntiles;
-  const zb_params &q = p.params;
-  a.ph.gamma = q.gamma;
-  a.ph.prandtl = q.prandtl;
-  a.ph.mu = q.mu;
-  a.ph.rt = q.rt;
-  a.ph.c_sth = q.c_sth;
-  a.ph.rus_k = q.rus_k;
-  a.ph.ldg_b = q.ldg_b;
-  a.ph.ldg_tau = q.ldg_tau;
-  a.ph.rho_fs = q.rho_fs;
-  a.ph.P_fs = q.P_fs;
-  a.ph.T_wall = q.T_wall;
-  a.ph.R_ref = q.R_ref;
-  for (int d = 0; d < 3; d++)
+  const double zero_ref[5] = {0, 0, 0, 0, 0};
+  a.ph = phys_of<double>(p.params, zero_ref, p.ndims, false);
+  if constexpr (D == 3)
   {
-    a.ph.V_fs[d] = q.V_fs[d];
-    a.ph.V_wall[d] = q.V_wall[d];
+    // hexahedra: column-mapped kernels, TW x N^2 threads per tile (ZS per column)
+    constexpr int HT = TW * N * N;
+    dev::k_hex_extrap<double, double, N><<<(unsigned)p.ntiles, HT, 0, st>>>(
+        a.U, reinterpret_cast<double *>(base + r.Ufp), p.ntiles, ops);
+    NA_CK(cudaGetLastError());
+    if (!p.params.viscous)
+    {
+      const size_t smem = (size_t)(S * V + 3 * S * V + Fp * V) * TW * sizeof(double);
+      NA_CK(cudaFuncSetAttribute(dev::k_hex_euler<double, double, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+      dev::k_hex_euler<double, double, N><<<(unsigned)p.ntiles, HT, smem, st>>>(a, ops);
+      NA_CK(cudaGetLastError());
+    }
+    else
+    {
+      constexpr int ZG = dev::HexNsShape<double, N>::grad_zs, ZF = dev::HexNsShape<double, N>::face_zs;
+      const size_t smem1 = (size_t)((S * V + Fp * V + 3 * S * V) * TW + 3 * N * TW) * sizeof(double);
+      NA_CK(cudaFuncSetAttribute(dev::k_hex_ns_grad<double, double, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem1));
+      dev::k_hex_ns_grad<double, double, N><<<(unsigned)p.ntiles, HT * ZG, smem1, st>>>(a, ops);
+      NA_CK(cudaGetLastError());
+      const size_t smem2 = (size_t)(Fp * V + S * V) * TW * sizeof(double);
+      NA_CK(cudaFuncSetAttribute(dev::k_hex_ns_face<double, double, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem2));
+      dev::k_hex_ns_face<double, double, N><<<(unsigned)p.ntiles, HT * ZF, smem2, st>>>(a, ops);
+      NA_CK(cudaGetLastError());
+    }
+    return;
   }
-  a.ph.fix_vis = q.fix_vis;
-  a.ph.fconv = q.fconv;
   dev::k_extrap<double, double, D, N><<<blocks_for(p.ntiles * Fp * TW), 256, 0, st>>>(
       a.U, reinterpret_cast<double *>(base + r.Ufp), p.ntiles, ops);
   NA_CK(cudaGetLastError());
@@ -299,6 +323,8 @@ void noalloc_residual(const Plan &p, const double *U, double *divF, cudaStream_t
   // flux points skipped under beta = +-0.5 are never written; start them at zero
   if (p.params.viscous)
     NA_CK(cudaMemsetAsync(base + r.Fvn, 0, (size_t)p.ntiles * Fp * p.nvars * TW * 8, st));
+  if (one_sided_common_flux(p))
+    NA_CK(cudaMemsetAsync(base + r.Fcom, 0, (size_t)p.ntiles * Fp * p.nvars * TW * 8, st));
   k_na_to_tiles<<<blocks_for(p.ntiles * S * p.nvars * TW), 256, 0, st>>>(
       U, reinterpret_cast<double *>(base + r.U), p.neles, p.ntiles, (int)S, p.nvars);
   NA_CK(cudaGetLastError());

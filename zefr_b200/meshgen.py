@@ -133,11 +133,13 @@ def read_gmsh(path: str) -> Mesh:
 
 
 def box_quads(nx: int, ny: int, x0: float = -5.0, x1: float = 5.0, y0: float = -5.0, y1: float = 5.0,
-              bnd: str = "PERIODIC") -> Mesh:
-    """Structured nx-by-ny 4-node quads on [x0,x1]x[y0,y1], all sides tagged ``bnd``.
+              bnd="PERIODIC") -> Mesh:
+    """Structured nx-by-ny 4-node quads on [x0,x1]x[y0,y1], all sides tagged
+    ``bnd``, or, for a 4-tuple, the sides x0, x1, y0, y1 tagged in that order.
 
     Elements are ordered x fastest; each quad is counter-clockwise.
     """
+    b_x0, b_x1, b_y0, b_y1 = (bnd,) * 4 if isinstance(bnd, str) else tuple(bnd)
     xs = np.linspace(x0, x1, nx + 1)
     ys = np.linspace(y0, y1, ny + 1)
     X, Y = np.meshgrid(xs, ys)  # (ny+1, nx+1)
@@ -150,11 +152,11 @@ def box_quads(nx: int, ny: int, x0: float = -5.0, x1: float = 5.0, y0: float = -
                      for j in range(ny) for i in range(nx)], dtype=np.int64)
     faces: List[Tuple[int, Tuple[int, ...], str]] = []
     for i in range(nx):
-        faces.append((GMSH_LINE2, (nid(i, 0), nid(i + 1, 0)), bnd))
-        faces.append((GMSH_LINE2, (nid(i + 1, ny), nid(i, ny)), bnd))
+        faces.append((GMSH_LINE2, (nid(i, 0), nid(i + 1, 0)), b_y0))
+        faces.append((GMSH_LINE2, (nid(i + 1, ny), nid(i, ny)), b_y1))
     for j in range(ny):
-        faces.append((GMSH_LINE2, (nid(nx, j), nid(nx, j + 1)), bnd))
-        faces.append((GMSH_LINE2, (nid(0, j + 1), nid(0, j)), bnd))
+        faces.append((GMSH_LINE2, (nid(nx, j), nid(nx, j + 1)), b_x1))
+        faces.append((GMSH_LINE2, (nid(0, j + 1), nid(0, j)), b_x0))
     return Mesh(2, nodes, GMSH_QUAD4, eles, faces)
 
 
