@@ -221,6 +221,25 @@ zb_status zb_get_residual(zb_ctx *ctx, unsigned stage, double *out, int64_t spt_
  * stage s, then U = U_ini - a_s dt/|J| divF_s, or on the last stage
  * U = U_ini - sum_s b_s dt/|J| divF_s.  Stage 0 first saves U_ini. */
 zb_status zb_rk_stage(zb_ctx *ctx, unsigned stage);
+/* The residual and the RK44 stage in three parts, for callers that interleave
+ * their own work (the reference's exchange and overset steps) between them:
+ * FRSolver::compute_residual_start / _mid / _finish (include/solver.hpp:
+ * 153-155, src/solver.cpp:1647-1829) and step_RK_stage_start / _mid /
+ * _finish (src/solver.cpp:3696-3760; Zefr::do_rk_stage_start/mid/finish,
+ * src/zefr.cpp:372-430).  start extrapolates the state to the flux points;
+ * mid (Navier-Stokes) forms the common solution, corrected gradient, fluxes
+ * and volume divergence; finish forms the common fluxes and surface
+ * correction and, for a stage, applies the RK update.  Called in that order
+ * for one stage they equal zb_compute_residual / zb_rk_stage; any other order
+ * returns ZB_ERR_ARG and resets the sequence, and zb_set_state,
+ * zb_compute_residual and zb_rk_stage reset it too. */
+zb_status zb_compute_residual_start(zb_ctx *ctx, unsigned stage);
+zb_status zb_compute_residual_mid(zb_ctx *ctx, unsigned stage);
+zb_status zb_compute_residual_finish(zb_ctx *ctx, unsigned stage);
+zb_status zb_rk_stage_start(zb_ctx *ctx, unsigned stage);
+zb_status zb_rk_stage_mid(zb_ctx *ctx, unsigned stage);
+zb_status zb_rk_stage_finish(zb_ctx *ctx, unsigned stage);
+
 /* n time steps of FRSolver::update (src/solver.cpp:2600-2660): RK44
  * (step_RK) by default, or the scheme set with zb_set_time_scheme. */
 zb_status zb_step(zb_ctx *ctx, int n);
@@ -268,7 +287,10 @@ zb_status zb_time_state(zb_ctx *ctx, double *dt, double *prev_err, int64_t *reje
 zb_status zb_get_element_dt(zb_ctx *ctx, double *out);
 
 /* Residual norms of report_residuals (src/solver.cpp:6990-7137), FP64 device
- * reduction of divF(stage 0)/|J| per variable: out[3*nvars] = L1, L2, Linf. */
+ * reduction of divF(stage 0)/|J| per variable, each divided by nspts * n_eles
+ * as the reference prints them: out[0..nvars) = max |.| (res_type 0),
+ * out[nvars..2 nvars) = sum |.| (res_type 1), out[2 nvars..3 nvars) =
+ * sqrt(sum of squares) (res_type 2). */
 zb_status zb_residual_norms(zb_ctx *ctx, double *out);
 
 /* Volume integrals of FRSolver::report_turbulent_stats (src/solver.cpp:
@@ -416,6 +438,19 @@ int64_t zb_launch_count(const zb_ctx *ctx);
 zb_status zb_profile_enable(zb_ctx *ctx, int on);
 zb_status zb_profile_read(zb_ctx *ctx, double *ms, int64_t *count);
 const char *zb_kernel_name(int id);
+
+/* Operator product on the tensor pipe: C = alpha A B + beta C with A [m][k]
+ * (row stride lda) a small constant operator and B [k][n] (row stride ldb),
+ * C [m][n] (row stride ldc), all FP32 device arrays; n is the element count
+ * times the variables, as in the reference's products (B = U_spts viewed as
+ * [nSpts][nVars * nEles]).  Replaces gimmik_mm_gpu (include/gimmik.h:5-22,
+ * src/gimmik_gpu.cu:31183-31577), same argument order, in FP32 instead of
+ * FP64.  tcgen05 MMAs with the operands split into TF32 parts
+ * (A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 accumulation in tensor memory),
+ * about FP32 accuracy.  m <= 256 and the operator (m x k) must fit in shared
+ * memory; runs on `stream` (NULL: the default stream) and synchronises it. */
+zb_status zb_operator_mm_tf32x3(int m, int n, int k, float alpha, const float *a, int lda, const float *b, int ldb,
+                                float beta, float *c, int ldc, void *stream);
 
 /* FP64 residual divF_spts = |J| div F for callers that cannot allocate device
  * memory.  No counterpart in the reference (its residual lives in FRSolver's

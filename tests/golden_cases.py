@@ -167,7 +167,7 @@ def load_traj(name: str) -> TrajGolden:
                       states=z["states"])
 
 
-def comp_err(a: np.ndarray, b: np.ndarray, floor: float = 1e-6) -> float:
+def comp_err(a: np.ndarray, b: np.ndarray, floor: float = 1e-2) -> float:
     """Largest relative difference per component, |a-b| / |b|, over the
     components whose magnitude is at least ``floor`` times the largest |b| of
     the same variable (below that, a component is a cancellation residue

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "zb.h")).read()
-    return sorted(set(re.findall(r"\b(zb_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(zb_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_header_symbols_exported():

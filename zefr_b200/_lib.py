@@ -39,6 +39,8 @@ EXPORTED = [
     "zb_batch_stage", "zb_batch_synchronize", "zb_batch_launch_count",
     "zb_time_scheme_defaults", "zb_set_time_scheme", "zb_time_state", "zb_get_element_dt", "zb_rk_step_vjp",
     "zb_geometry_eval", "zb_geometry_eval_vjp", "zb_set_nodes",
+    "zb_compute_residual_start", "zb_compute_residual_mid", "zb_compute_residual_finish",
+    "zb_rk_stage_start", "zb_rk_stage_mid", "zb_rk_stage_finish", "zb_operator_mm_tf32x3",
 ]
 ZB_RK44, ZB_RK54 = 0, 1
 ZB_NKERNELS = 11
@@ -137,6 +139,12 @@ def lib() -> ctypes.CDLL:
         L.zb_compute_residual.argtypes = [vp, ctypes.c_uint]
         L.zb_get_residual.argtypes = [vp, ctypes.c_uint, dp, i64, i64, i64, ctypes.c_int]
         L.zb_rk_stage.argtypes = [vp, ctypes.c_uint]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.zb_operator_mm_tf32x3.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, fp,
+                                            ctypes.c_int, fp, ctypes.c_int, ctypes.c_float, fp, ctypes.c_int, vp]
+        for fn in ("zb_compute_residual_start", "zb_compute_residual_mid", "zb_compute_residual_finish",
+                   "zb_rk_stage_start", "zb_rk_stage_mid", "zb_rk_stage_finish"):
+            getattr(L, fn).argtypes = [vp, ctypes.c_uint]
         L.zb_step.argtypes = [vp, ctypes.c_int]
         L.zb_residual_norms.argtypes = [vp, dp]
         L.zb_synchronize.argtypes = [vp]

@@ -3,7 +3,9 @@
 // thread-local message, the C-ABI analogue of the reference's ThrowException
 // (include/macros.hpp:52-54).
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <vector>
 #include <string>
 
@@ -41,6 +43,24 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 
 #define ZB_REQUIRE(cond, msg) \
   if (!(cond)) ZB_THROW(ZB_ERR_ARG, msg)
+
+// one device int per GPU for the tensor-core product's timeout flag
+static int *opmm_flag_for_current_device()
+{
+  static std::mutex mu;
+  static std::map<int, int *> flags;
+  int d = 0;
+  cudaError_t e = cudaGetDevice(&d);
+  if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = flags.find(d);
+  if (it != flags.end()) return it->second;
+  int *p = nullptr;
+  e = cudaMalloc(&p, sizeof(int));
+  if (e != cudaSuccess) ZB_THROW(ZB_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  flags[d] = p;
+  return p;
+}
 
 extern "C" {
 
@@ -305,6 +325,22 @@ zb_status zb_rk_stage(zb_ctx *ctx, unsigned stage)
   })
 }
 
+#define ZB_SPLIT_ENTRY(fn, part, rk)          \
+  zb_status fn(zb_ctx *ctx, unsigned stage)     \
+  {                                             \
+    ZB_GUARD({                                  \
+      ZB_REQUIRE(ctx, "null context");          \
+      zb::ctx_residual_split(ctx->impl, stage, part, rk); \
+    })                                          \
+  }
+ZB_SPLIT_ENTRY(zb_compute_residual_start, 0, 0)
+ZB_SPLIT_ENTRY(zb_compute_residual_mid, 1, 0)
+ZB_SPLIT_ENTRY(zb_compute_residual_finish, 2, 0)
+ZB_SPLIT_ENTRY(zb_rk_stage_start, 0, 1)
+ZB_SPLIT_ENTRY(zb_rk_stage_mid, 1, 1)
+ZB_SPLIT_ENTRY(zb_rk_stage_finish, 2, 1)
+#undef ZB_SPLIT_ENTRY
+
 zb_status zb_step(zb_ctx *ctx, int n)
 {
   ZB_GUARD({
@@ -566,4 +602,15 @@ const char *zb_kernel_name(int id)
   return (id >= 0 && id < ZB_NKERNELS) ? names[id] : "unknown";
 }
 
+zb_status zb_operator_mm_tf32x3(int m, int n, int k, float alpha, const float *a, int lda, const float *b, int ldb,
+                                float beta, float *c, int ldc, void *stream)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(a && c && (b || n == 0), "null operand");
+    zb::opmm_tc(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, static_cast<cudaStream_t>(stream),
+                opmm_flag_for_current_device());
+  })
+}
+
 }  // extern "C"
+

@@ -353,6 +353,7 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
       constexpr int ZG = dev::HexNsShape<A, N>::grad_zs, ZF = dev::HexNsShape<A, N>::face_zs;
       const size_t smem1 = (size_t)((S * V + Fp * V + 3 * S * V) * TW + 3 * N * TW) * sizeof(A);  // + sX padding
       set_smem(dev::k_hex_ns_grad<T, A, N>, smem1);
+      if (!sc.face_only)
       {
         ProfScope ps(c, ZB_K_NS_GRAD);
         dev::k_hex_ns_grad<T, A, N><<<(unsigned)c.ntiles, HT * ZG, smem1, c.stream>>>(a, ops);
@@ -383,6 +384,7 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
   {
     const size_t smem1 = (size_t)(S * V + Fp * V + D * S * V) * TW * sizeof(A) + ops_bytes;
     set_smem(dev::k_ns_grad<T, A, D, N>, smem1);
+    if (!sc.face_only)
     {
       ProfScope ps(c, ZB_K_NS_GRAD);
       dev::k_ns_grad<T, A, D, N><<<(unsigned)c.ntiles, NT, smem1, c.stream>>>(a, ops);
@@ -433,6 +435,7 @@ static void launch_stage_tri(Ctx &c, const StageCfg &sc)
   {
     const size_t smem1 = (ops + (size_t)(S * V + Fp * V + D * S * V) * TW) * sizeof(A);
     set_smem(dev::k_tri_ns_grad<T, A, N>, smem1);
+    if (!sc.face_only)
     {
       ProfScope ps(c, ZB_K_NS_GRAD);
       dev::k_tri_ns_grad<T, A, N><<<(unsigned)c.ntiles, 128, smem1, c.stream>>>(a);
@@ -723,6 +726,7 @@ static size_t extent(const Ctx *c, int64_t ss, int64_t vs, int64_t es, int npts)
 
 void ctx_set_state(Ctx *c, const double *U, int64_t ss, int64_t vs, int64_t es, int where)
 {
+  c->split_phase = 0;
   if (!U) ZB_THROW(ZB_ERR_ARG, "null state");
   const size_t ext = extent(c, ss, vs, es, c->S);
   const double *src = stage_in(c, U, ext, where);
@@ -819,6 +823,7 @@ static void ensure_ufp(Ctx *c)
 void ctx_compute_residual(Ctx *c, unsigned stage)
 {
   if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  c->split_phase = 0;
   // extrapolate_U is step 1 of the reference residual (src/solver.cpp:1516-1518)
   c->ufp_valid = false;
   ensure_ufp(c);
@@ -833,16 +838,72 @@ void ctx_get_residual(Ctx *c, unsigned stage, double *out, int64_t ss, int64_t v
   from_tiles(c, c->divF[stage], nullptr, nullptr, out, ss, vs, es, where);
 }
 
-void ctx_rk_stage(Ctx *c, unsigned stage)
+static StageCfg rk_stage_cfg(const Ctx *c, unsigned stage)
 {
-  if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
-  if (c->ts.scheme != ZB_RK44) ZB_THROW(ZB_ERR_UNSUPPORTED, "stage-wise stepping is built for RK44");
-  ensure_ufp(c);
   StageCfg sc;
   sc.stage = stage;
   sc.rk_mode = (stage + 1 < (unsigned)c->nstages) ? 1 : 2;
   sc.save_ini = (stage == 0);
   sc.extrap_next = 1;
+  return sc;
+}
+
+void ctx_rk_stage(Ctx *c, unsigned stage)
+{
+  if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  if (c->ts.scheme != ZB_RK44) ZB_THROW(ZB_ERR_UNSUPPORTED, "stage-wise stepping is built for RK44");
+  c->split_phase = 0;
+  ensure_ufp(c);
+  c->launch_stage(*c, rk_stage_cfg(c, stage));
+}
+
+// Split residual and RK stage (compute_residual_start/mid/finish,
+// src/solver.cpp:1647-1829; step_RK_stage_start/mid/finish, 3696-3760).
+// start: the state's flux-point traces (extrapolate_U); mid: for
+// Navier-Stokes the gradient kernel (common solution, corrected gradient,
+// fluxes, volume divergence); finish: the common fluxes and surface
+// correction (the whole Euler kernel), with the RK update for a stage.
+// The three calls in order equal zb_compute_residual / zb_rk_stage.
+static void split_expect(Ctx *c, unsigned stage, int phase, int rk, const char *call)
+{
+  if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  if (rk && c->ts.scheme != ZB_RK44) ZB_THROW(ZB_ERR_UNSUPPORTED, "stage-wise stepping is built for RK44");
+  if (c->split_phase != phase || (phase != 0 && (c->split_stage != stage || c->split_rk != rk)))
+  {
+    c->split_phase = 0;
+    ZB_THROW(ZB_ERR_ARG, std::string(call) + " out of order: call _start, _mid and _finish of one stage in turn");
+  }
+}
+
+void ctx_residual_split(Ctx *c, unsigned stage, int part, int rk)
+{
+  static const char *names[2][3] = {{"compute_residual_start", "compute_residual_mid", "compute_residual_finish"},
+                                    {"rk_stage_start", "rk_stage_mid", "rk_stage_finish"}};
+  if (part < 0 || part > 2) ZB_THROW(ZB_ERR_ARG, "split part out of range");
+  split_expect(c, stage, part, rk ? 1 : 0, names[rk ? 1 : 0][part]);
+  const bool visc = c->plan.params.viscous != 0;
+  if (part == 0)
+  {
+    if (!rk) c->ufp_valid = false;
+    ensure_ufp(c);
+    c->split_stage = stage;
+    c->split_rk = rk ? 1 : 0;
+    c->split_phase = 1;
+    return;
+  }
+  StageCfg sc = rk ? rk_stage_cfg(c, stage) : StageCfg{stage, 0, 0, 0};
+  if (part == 1)
+  {
+    if (visc)
+    {
+      sc.grad_only = 1;
+      c->launch_stage(*c, sc);
+    }
+    c->split_phase = 2;
+    return;
+  }
+  sc.face_only = visc ? 1 : 0;
+  c->split_phase = 0;
   c->launch_stage(*c, sc);
 }
 

@@ -31,6 +31,7 @@ struct StageCfg
   int extrap_next;
   int want_dU = 0;     // write the physical gradient (NS)
   int grad_only = 0;   // NS: stop after the gradient kernel
+  int face_only = 0;   // NS: the face kernel alone (the gradient kernel ran before)
 };
 
 // RK44 tables (src/solver.cpp:722-735)
@@ -60,6 +61,11 @@ struct Ctx
   double *dred = nullptr;
   int cur = 0;
   bool ufp_valid = false;
+  // split residual (zb_compute_residual_start/mid/finish, zb_rk_stage_*):
+  // phase 0 idle, 1 after start, 2 after mid; the stage and kind being split
+  int split_phase = 0;
+  unsigned split_stage = 0;
+  int split_rk = 0;
   double dt = 0.0;
   // mixed form: reference state (FP32-representable values) the stored state
   // deviates from; zero for the FP64 form

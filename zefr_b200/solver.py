@@ -238,6 +238,19 @@ class FRSolver:
     def compute_residual(self, stage: int = 0) -> None:
         check(lib().zb_compute_residual(self.h, stage))
 
+    # FRSolver::compute_residual_start / _mid / _finish: the three together
+    # equal compute_residual (start: flux-point traces; mid: gradient, fluxes
+    # and volume divergence for Navier-Stokes; finish: common fluxes and the
+    # surface correction)
+    def compute_residual_start(self, stage: int = 0) -> None:
+        check(lib().zb_compute_residual_start(self.h, stage))
+
+    def compute_residual_mid(self, stage: int = 0) -> None:
+        check(lib().zb_compute_residual_mid(self.h, stage))
+
+    def compute_residual_finish(self, stage: int = 0) -> None:
+        check(lib().zb_compute_residual_finish(self.h, stage))
+
     def get_residual(self, stage: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
         if out is None:
             out = np.zeros(self.state_shape)
@@ -261,6 +274,16 @@ class FRSolver:
     # -- time stepping --
     def step_RK_stage(self, stage: int) -> None:
         check(lib().zb_rk_stage(self.h, stage))
+
+    # FRSolver::step_RK_stage_start / _mid / _finish (the RK update in finish)
+    def step_RK_stage_start(self, stage: int) -> None:
+        check(lib().zb_rk_stage_start(self.h, stage))
+
+    def step_RK_stage_mid(self, stage: int) -> None:
+        check(lib().zb_rk_stage_mid(self.h, stage))
+
+    def step_RK_stage_finish(self, stage: int) -> None:
+        check(lib().zb_rk_stage_finish(self.h, stage))
 
     def update(self) -> None:
         check(lib().zb_step(self.h, 1))
