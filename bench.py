@@ -55,8 +55,8 @@ TGV_DECK = dict(ndims=3, order=ORDER, viscous=1, disable_nondim=1, fix_vis=1, ma
 # above L2): 304 + 1232 + 588 MB over 110,592 elements.
 MIXED_DRAM_BYTES_PER_ELEMENT = 19210.0
 # the same for the FP64 form (k_hex_extrap + k_hex_ns_grad + k_hex_ns_face,
-# FP64, 48^3 hexes, state 283 MB)
-FP64_DRAM_BYTES_PER_ELEMENT = 38420.0
+# FP64, 48^3 hexes, state 283 MB): 748 + 2432 + 979 MB over 110,592 elements
+FP64_DRAM_BYTES_PER_ELEMENT = 37607.0
 
 
 def b_alg(E: int, S: int, V: int, D: int, G: int, Fp: int, w: int) -> float:
@@ -278,7 +278,8 @@ def triangle_solver(form: str, mesh=None):
         mesh = meshgen.box_tris(128, seed=2024, jitter=0.15)
     p = params_from_deck(ndims=2, order=4, viscous=1, disable_nondim=1, fix_vis=1, mach_fs=0.2, Re_fs=1000.0,
                          prandtl=0.71, P_fs=1.0, rho_fs=1.0, L_fs=1.0, ldg_b=0.5, ldg_tau=0.1, fconv=2,
-                         precision={"mixed": 1, "fp64": 0}[form], gamma=1.4, dt=1e-4)
+                         precision={"mixed": 1, "mixed_tc": 1, "fp64": 0}[form], gamma=1.4, dt=1e-4)
+    p.tensor_ops = int(form == "mixed_tc")
     s = FRSolver(mesh, p, {"PERIODIC": "periodic"})
     s.set_stream(torch.cuda.current_stream().cuda_stream)
     X = s.plan.get("coord_spts").reshape(s.nspts, 2, s.neles)
@@ -287,14 +288,16 @@ def triangle_solver(form: str, mesh=None):
 
 
 def triangle_side(K: int, W: int):
-    """The triangle workload (triangle_solver): GDOF/s per residual of both
-    forms and the mixed form's relative L2 error."""
+    """The triangle workload (triangle_solver): GDOF/s per residual of the
+    FP64 form and of the mixed form with its gradient kernel's operator
+    products on CUDA cores (mixed) and on the tensor pipe (mixed_tc), and the
+    mixed forms' relative L2 errors."""
     import torch
     from zefr_b200 import meshgen
     mesh = meshgen.box_tris(128, seed=2024, jitter=0.15)
     out = {"workload": "triangles_128x128x2_P4_navier_stokes_roe_ldg", "elements": int(mesh.n_elements)}
     R = {}
-    for form in ("mixed", "fp64"):
+    for form in ("mixed", "mixed_tc", "fp64"):
         s = triangle_solver(form, mesh)
         for i in range(W):
             s.compute_residual(i % 4)
@@ -309,10 +312,15 @@ def triangle_side(K: int, W: int):
         dof = s.nspts * s.nvars * s.neles
         s.compute_residual(0)
         R[form] = s.get_residual(0)
-        out[form] = {"gdof_s": dof / (ms * 1e-3) / 1e9, "ms_per_residual": ms, "dof": dof}
+        prof = kernel_profile(s, K)
+        out[form] = {"gdof_s": dof / (ms * 1e-3) / 1e9, "ms_per_residual": ms, "dof": dof,
+                     "kernels_ms": {k: v["ms_avg"] for k, v in prof.items() if v["launches"]}}
         s.close()
-    out["mixed_rel_l2_err_vs_fp64"] = float(np.linalg.norm(R["mixed"] - R["fp64"]) / np.linalg.norm(R["fp64"]))
+    nrm = np.linalg.norm(R["fp64"])
+    out["mixed_rel_l2_err_vs_fp64"] = float(np.linalg.norm(R["mixed"] - R["fp64"]) / nrm)
+    out["mixed_tc_rel_l2_err_vs_fp64"] = float(np.linalg.norm(R["mixed_tc"] - R["fp64"]) / nrm)
     out["mixed_over_fp64"] = out["fp64"]["ms_per_residual"] / out["mixed"]["ms_per_residual"]
+    out["mixed_tc_over_mixed"] = out["mixed"]["ms_per_residual"] / out["mixed_tc"]["ms_per_residual"]
     return out
 
 
@@ -741,7 +749,8 @@ def main():
     ap.add_argument("--ref-cells", type=int, default=REF_CELLS, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-side", action="store_true", help="skip the triangle and batched side workloads")
-    ap.add_argument("--profile-form", choices=["mixed", "fp64", "adjoint", "tri-mixed", "tri-fp64"], default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--profile-form", choices=["mixed", "fp64", "adjoint", "tri-mixed", "tri-mixed_tc", "tri-fp64"],
+                    default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

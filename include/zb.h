@@ -126,6 +126,11 @@ typedef struct zb_params {
   int tri_volume_div; /* triangles: 0 = the reference's operators, whose oppDiv
                          lacks the volume-divergence term (src/elements.cpp:
                          609-623 builds it for quads/hexes only); 1 = include it */
+  int tensor_ops;     /* mixed form, triangles, Navier-Stokes: 1 = the gradient
+                         kernel's dense operator products on the tensor pipe
+                         (tcgen05, TF32x3 split products, FP32 accumulation);
+                         0 = on CUDA cores (FP32 FMA).  No reference
+                         counterpart (its products are GiMMiK or cuBLAS). */
 } zb_params;
 
 /* Deck-style inputs for zb_params_from_deck (reference keys, src/input.cpp). */
@@ -448,7 +453,9 @@ const char *zb_kernel_name(int id);
  * FP64.  tcgen05 MMAs with the operands split into TF32 parts
  * (A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 accumulation in tensor memory),
  * about FP32 accuracy.  m <= 256 and the operator (m x k) must fit in shared
- * memory; runs on `stream` (NULL: the default stream) and synchronises it. */
+ * memory.  Queued on `stream` (NULL: the default stream) without waiting; a
+ * product whose tensor-core completion wait timed out (it sets a flag and
+ * leaves C unfinished) is reported as ZB_ERR_CUDA by the next call. */
 zb_status zb_operator_mm_tf32x3(int m, int n, int k, float alpha, const float *a, int lda, const float *b, int ldb,
                                 float beta, float *c, int ldc, void *stream);
 

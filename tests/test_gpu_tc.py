@@ -25,6 +25,8 @@ def _mm(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
                                           ctypes.cast(B.data_ptr(), _FP), ldb, beta,
                                           ctypes.cast(C.data_ptr(), _FP), ldc, None)
     assert st == 0, _lib.lib().zb_last_error().decode()
+    import torch
+    torch.cuda.synchronize()
 
 
 @pytest.mark.parametrize("m,k,n", [(15, 15, 4 * 1000 + 3),     # triangle P4 oppE

@@ -64,7 +64,7 @@ class ZbParams(ctypes.Structure):
         ("ldg_b", ctypes.c_double), ("ldg_tau", ctypes.c_double), ("rho_fs", ctypes.c_double),
         ("V_fs", ctypes.c_double * 3), ("P_fs", ctypes.c_double), ("T_wall", ctypes.c_double),
         ("R_ref", ctypes.c_double), ("V_wall", ctypes.c_double * 3), ("dt", ctypes.c_double),
-        ("tri_volume_div", ctypes.c_int),
+        ("tri_volume_div", ctypes.c_int), ("tensor_ops", ctypes.c_int),
     ]
 
 

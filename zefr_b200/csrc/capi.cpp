@@ -44,22 +44,34 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 #define ZB_REQUIRE(cond, msg) \
   if (!(cond)) ZB_THROW(ZB_ERR_ARG, msg)
 
-// one device int per GPU for the tensor-core product's timeout flag
-static int *opmm_flag_for_current_device()
+// one int of mapped pinned host memory per GPU for the tensor-core product's
+// timeout flag (host and device addresses)
+struct OpmmFlag
+{
+  volatile int *host = nullptr;
+  int *dev = nullptr;
+};
+
+static OpmmFlag opmm_flag_for_current_device()
 {
   static std::mutex mu;
-  static std::map<int, int *> flags;
+  static std::map<int, OpmmFlag> flags;
   int d = 0;
   cudaError_t e = cudaGetDevice(&d);
   if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   std::lock_guard<std::mutex> lk(mu);
   auto it = flags.find(d);
   if (it != flags.end()) return it->second;
-  int *p = nullptr;
-  e = cudaMalloc(&p, sizeof(int));
-  if (e != cudaSuccess) ZB_THROW(ZB_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-  flags[d] = p;
-  return p;
+  void *h = nullptr;
+  e = cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped);
+  if (e != cudaSuccess) ZB_THROW(ZB_ERR_NOMEM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+  *static_cast<volatile int *>(h) = 0;
+  void *dp = nullptr;
+  e = cudaHostGetDevicePointer(&dp, h, 0);
+  if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("cudaHostGetDevicePointer: ") + cudaGetErrorString(e));
+  OpmmFlag f{static_cast<volatile int *>(h), static_cast<int *>(dp)};
+  flags[d] = f;
+  return f;
 }
 
 extern "C" {
@@ -607,8 +619,8 @@ zb_status zb_operator_mm_tf32x3(int m, int n, int k, float alpha, const float *a
 {
   ZB_GUARD({
     ZB_REQUIRE(a && c && (b || n == 0), "null operand");
-    zb::opmm_tc(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, static_cast<cudaStream_t>(stream),
-                opmm_flag_for_current_device());
+    const OpmmFlag f = opmm_flag_for_current_device();
+    zb::opmm_tc(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, static_cast<cudaStream_t>(stream), f.host, f.dev);
   })
 }
 

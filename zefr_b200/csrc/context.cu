@@ -3,6 +3,7 @@
 #include "ctx_impl.cuh"
 #include "hex_kernels.cuh"
 #include "tri_kernels.cuh"
+#include "tri_tc_kernels.cuh"
 #include "time_kernels.cuh"
 
 namespace zb {
@@ -421,6 +422,11 @@ static void launch_stage_tri(Ctx &c, const StageCfg &sc)
   using G = dev::TriShape<N>;
   constexpr int S = G::S, Fp = G::Fp, V = G::V, D = 2;
   const Args<T, A> a = make_args<T, A>(c, sc);
+  if (c.tc_err_host && *c.tc_err_host)
+  {
+    *c.tc_err_host = 0;
+    ZB_THROW(ZB_ERR_CUDA, "a tensor-core completion wait of an earlier launch timed out");
+  }
   const size_t ops = (size_t)G::OPS_PAD;
   if (!c.plan.params.viscous)
   {
@@ -434,11 +440,26 @@ static void launch_stage_tri(Ctx &c, const StageCfg &sc)
   else
   {
     const size_t smem1 = (ops + (size_t)(S * V + Fp * V + D * S * V) * TW) * sizeof(A);
-    set_smem(dev::k_tri_ns_grad<T, A, N>, smem1);
     if (!sc.face_only)
     {
       ProfScope ps(c, ZB_K_NS_GRAD);
-      dev::k_tri_ns_grad<T, A, N><<<(unsigned)c.ntiles, 128, smem1, c.stream>>>(a);
+      bool launched = false;
+      if constexpr (std::is_same<A, float>::value)
+      {
+        if (c.plan.params.tensor_ops)
+        {
+          using C = dev::TriTc<N>;
+          set_smem(dev::k_tri_ns_grad_tc<N>, C::SMEM);
+          const int64_t groups = (c.ntiles + C::TILES - 1) / C::TILES;
+          dev::k_tri_ns_grad_tc<N><<<(unsigned)groups, C::NT, C::SMEM, c.stream>>>(a);
+          launched = true;
+        }
+      }
+      if (!launched)
+      {
+        set_smem(dev::k_tri_ns_grad<T, A, N>, smem1);
+        dev::k_tri_ns_grad<T, A, N><<<(unsigned)c.ntiles, 128, smem1, c.stream>>>(a);
+      }
       c.launches++;
       CK(cudaGetLastError());
     }
@@ -511,6 +532,7 @@ static void free_all(Ctx *c)
                   c->dfw, c->U_til, c->rk_err, c->rkv, c->rkfvn, c->geo_tab, c->geo_pair, c->geo_work};
   for (void *b : bufs)
     if (b) cudaFree(b);
+  if (c->tc_err_host) cudaFreeHost(const_cast<int *>(c->tc_err_host));
   for (auto &r : c->recs)
   {
     cudaEventDestroy(r.a);
@@ -595,6 +617,9 @@ Ctx *ctx_create(const Plan &plan)
   c->ntiles = plan.ntiles;
   c->dt = plan.params.dt;
   if (plan.tile != TW) ZB_THROW(ZB_ERR_INTERNAL, "plan tile width does not match kernels");
+  if (plan.params.tensor_ops && !(c->prec == ZB_MIXED && plan.etype == ET_TRI && plan.params.viscous))
+    ZB_THROW(ZB_ERR_UNSUPPORTED, "tensor-core operator products are built for the mixed form on triangles "
+                                 "(Navier-Stokes)");
   if (c->prec == ZB_FP64)
   {
     bind_t<double, double>(*c);
@@ -623,6 +648,15 @@ Ctx *ctx_create(const Plan &plan)
     c->nbr = (int *)dalloc((size_t)c->ntiles * c->Fp * TW * sizeof(int));
     c->dred = (double *)dalloc(3 * 8 * sizeof(double));
     c->dref = (double *)dalloc(8 * sizeof(double));
+    if (plan.params.tensor_ops)
+    {
+      void *h = nullptr, *dp = nullptr;
+      CK(cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped));
+      c->tc_err_host = static_cast<volatile int *>(h);
+      *c->tc_err_host = 0;
+      CK(cudaHostGetDevicePointer(&dp, h, 0));
+      c->tc_err_dev = static_cast<int *>(dp);
+    }
     CK(cudaMemsetAsync(c->dref, 0, 8 * sizeof(double), c->stream));
     if (c->prec == ZB_FP64)
       upload_static<double>(*c);

@@ -27,9 +27,9 @@ void ctx_get_state(Ctx *c, double *U, int64_t ss, int64_t vs, int64_t es, int wh
 void ctx_compute_residual(Ctx *c, unsigned stage);
 void ctx_get_residual(Ctx *c, unsigned stage, double *out, int64_t ss, int64_t vs, int64_t es, int where);
 void ctx_rk_stage(Ctx *c, unsigned stage);
-// C = alpha A B + beta C on the tensor pipe (TF32x3, tc_opmm.cu); synchronises st
+// C = alpha A B + beta C on the tensor pipe (TF32x3, tc_opmm.cu), queued on st
 void opmm_tc(int m, int n, int k, float alpha, const float *a, int lda, const float *b, int ldb, float beta, float *c,
-             int ldc, cudaStream_t st, int *err_dev, int max_ctas = 0);
+             int ldc, cudaStream_t st, volatile int *err_host, int *err_dev, int max_ctas = 0);
 size_t opmm_tc_smem_bytes(int m, int k);
 // part 0 start, 1 mid, 2 finish; rk: the RK44 stage rather than the residual alone
 void ctx_residual_split(Ctx *c, unsigned stage, int part, int rk);

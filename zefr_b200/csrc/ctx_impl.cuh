@@ -107,6 +107,10 @@ struct Ctx
   double *dfw = nullptr;      // face-point quadrature weights [Fp / faces]
   void *U_til = nullptr, *rk_err = nullptr;
   bool use_dt_dev = false, use_dt_ele = false;  // stage kernels read the step from d_dt / dt_ele
+  // tensor-core kernels' timeout flag: mapped pinned host memory (host and
+  // device addresses), checked before each stage launch
+  volatile int *tc_err_host = nullptr;
+  int *tc_err_dev = nullptr;
   void (*launch_extrap)(Ctx &) = nullptr;
   void (*launch_stage)(Ctx &, const StageCfg &) = nullptr;
   void (*launch_vjp)(Ctx &, bool, bool) = nullptr;
@@ -249,6 +253,7 @@ static Args<T, A> make_args(Ctx &c, const StageCfg &sc)
   a.ntiles = c.ntiles;
   a.dU_out = sc.want_dU ? (T *)c.dU : nullptr;
   a.dops = (const A *)c.dops;
+  a.err = c.tc_err_dev;
   a.ph = phys_of<A>(c.plan.params, c.uref, c.D, sizeof(T) < sizeof(double));
   if (sc.rk_mode == 1)
     a.rk_coef[0] = (A)kRkAlpha[sc.stage];

@@ -76,6 +76,7 @@ struct Args
   A dt;
   int64_t ntiles;
   const A *dops;     // triangles: dense operators (TriOps layout), nullptr otherwise
+  int *err;          // tensor-core kernels: set when a completion wait gave up
   Phys<A> ph;
 };
 

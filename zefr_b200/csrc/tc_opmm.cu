@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kCols) k_opmm_tf32x3(int m, int n, int k, floa
   }
   if (!ok)
   {
-    if (tid == 0) atomicExch(err, 1);
+    if (tid == 0) *reinterpret_cast<volatile int *>(err) = 1;
     // the MMAs of the unfinished step may still be running: wait once more
     // (bounded) before the tensor memory is released
     tc::mbar_wait(mbar, phase ^ 1, kPolls);
@@ -172,11 +172,18 @@ size_t opmm_tc_smem_bytes(int m, int k)
   return (size_t)2 * NP * KP * 4 + (size_t)2 * kCols * kKB * 4 + 16;
 }
 
-// Launches the product on `st` and synchronises it (the timeout flag of the
-// kernel's waits is read back).  err_dev: one device int, zeroed here.
+// Launches the product on `st` without waiting for it.  err_host / err_dev:
+// one int of mapped pinned host memory (host and device addresses) that a
+// kernel whose tensor-core wait timed out sets; it is checked, and cleared,
+// when the next product is launched.
 void opmm_tc(int m, int n, int k, float alpha, const float *a, int lda, const float *b, int ldb, float beta, float *c,
-             int ldc, cudaStream_t st, int *err_dev, int max_ctas)
+             int ldc, cudaStream_t st, volatile int *err_host, int *err_dev, int max_ctas)
 {
+  if (*err_host)
+  {
+    *err_host = 0;
+    ZB_THROW(ZB_ERR_CUDA, "operator product: a tensor-core completion wait of an earlier product timed out");
+  }
   if (m < 1 || n < 0 || k < 1) ZB_THROW(ZB_ERR_ARG, "operator product: m and k must be positive, n non-negative");
   if (m > 256) ZB_THROW(ZB_ERR_UNSUPPORTED, "operator product on the tensor pipe: m <= 256");
   if (lda < k || ldb < n || ldc < n) ZB_THROW(ZB_ERR_ARG, "operator product: leading dimension too small");
@@ -186,7 +193,6 @@ void opmm_tc(int m, int n, int k, float alpha, const float *a, int lda, const fl
                                      std::to_string(k) + " does not fit in shared memory");
   if (n == 0) return;
   cudaError_t e = cudaFuncSetAttribute(k_opmm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess) e = cudaMemsetAsync(err_dev, 0, sizeof(int), st);
   if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("operator product set-up: ") + cudaGetErrorString(e));
   const int64_t chunks = ((int64_t)n + kCols - 1) / kCols;
   // resident CTAs: shared memory and tensor-memory columns (512 per SM)
@@ -200,11 +206,6 @@ void opmm_tc(int m, int n, int k, float alpha, const float *a, int lda, const fl
   k_opmm_tf32x3<<<(unsigned)grid, kCols, smem, st>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, err_dev);
   e = cudaGetLastError();
   if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("operator product launch: ") + cudaGetErrorString(e));
-  int herr = 0;
-  e = cudaMemcpyAsync(&herr, err_dev, sizeof(int), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) ZB_THROW(ZB_ERR_CUDA, std::string("operator product: ") + cudaGetErrorString(e));
-  if (herr) ZB_THROW(ZB_ERR_CUDA, "operator product: a tensor-core completion wait timed out");
 }
 
 }  // namespace zb

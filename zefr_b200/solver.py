@@ -25,8 +25,11 @@ def make_params(order: int, viscous: bool = False, *, gamma: float = 1.4, prandt
                 rt: float = 0.0, c_sth: float = 0.0, fix_vis: bool = True, rus_k: float = 0.0,
                 ldg_b: float = 0.5, ldg_tau: float = 1.0, rho_fs: float = 1.0, V_fs=(0.0, 0.0, 0.0),
                 P_fs: float = 1.0, T_wall: float = 0.0, R_ref: float = 0.0, V_wall=(0.0, 0.0, 0.0),
-                dt: float = 1e-3, fconv: str = "rusanov", precision: str = "fp64") -> ZbParams:
-    """Solver parameters with the meaning of the reference InputStruct fields."""
+                dt: float = 1e-3, fconv: str = "rusanov", precision: str = "fp64",
+                tensor_ops: bool = False) -> ZbParams:
+    """Solver parameters with the meaning of the reference InputStruct fields.
+    ``tensor_ops``: mixed form on triangles (Navier-Stokes), the gradient
+    kernel's operator products on the tensor pipe (TF32x3)."""
     p = ZbParams()
     p.order = order
     p.viscous = int(bool(viscous))
@@ -39,6 +42,7 @@ def make_params(order: int, viscous: bool = False, *, gamma: float = 1.4, prandt
     for d in range(3):
         p.V_fs[d] = float(V_fs[d]) if d < len(V_fs) else 0.0
         p.V_wall[d] = float(V_wall[d]) if d < len(V_wall) else 0.0
+    p.tensor_ops = int(bool(tensor_ops))
     return p
 
 
