@@ -222,6 +222,20 @@ zb_status zb_compute_residual(zb_ctx *ctx, unsigned stage);
 zb_status zb_get_residual(zb_ctx *ctx, unsigned stage, double *out, int64_t spt_stride,
                           int64_t var_stride, int64_t ele_stride, int where);
 
+/* divF_spts(stage) for n states held in host memory: for each i,
+ * zb_set_state(U[i]) + zb_compute_residual(stage) + zb_get_residual(stage,
+ * divF[i]), with U[i] and divF[i] dense in the reference layout
+ * [nspts][nvars][n_eles] (the layout of zefr::get_q_spts with its default
+ * strides, include/zefr_interface.hpp:126-129, around FRSolver::
+ * compute_residual, include/solver.hpp:152).  The copies of state i+1 to the
+ * device and of residual i-1 to the host overlap the computation of residual
+ * i (one copy engine each way, two staging buffers each way, allocated on the
+ * first call and kept by the context); with pinned host buffers the
+ * copies run asynchronously, with pageable ones they still complete but
+ * overlap less.  Returns once every residual is in host memory; the context
+ * then holds state U[n-1] and its residual. */
+zb_status zb_compute_residuals_host(zb_ctx *ctx, unsigned stage, int n, const double *const *U, double *const *divF);
+
 /* One RK44 stage of FRSolver::step_RK (src/solver.cpp:2864-3097): residual of
  * stage s, then U = U_ini - a_s dt/|J| divF_s, or on the last stage
  * U = U_ini - sum_s b_s dt/|J| divF_s.  Stage 0 first saves U_ini. */

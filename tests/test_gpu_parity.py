@@ -416,3 +416,28 @@ def test_split_residual_out_of_order_rejected():
     s.compute_residual_mid(1)
     s.compute_residual_finish(1)
     assert gc.rel_err(s.get_residual(1), g.R0) < TOL_FP64
+
+
+@pytest.mark.parametrize("name", ["hex_p3_ns_tgv", "quad_p3_euler_vortex", "tri_p4_ns_jitter"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_residuals_host_equal_one_by_one(name, precision):
+    """zb_compute_residuals_host over several host states (pinned and
+    pageable) equals set_state + compute_residual + get_residual per state bit
+    for bit, and leaves the context at the last state."""
+    import torch
+    g = gc.load(name)
+    s = solver_for(g, precision=precision)
+    rng = np.random.default_rng(5)
+    states = [g.U0 * (1.0 + 1e-3 * rng.standard_normal(g.U0.shape)) for _ in range(5)]
+    want = [s.residual(u, 2).copy() for u in states]
+    pinned = [torch.from_numpy(u.copy()).pin_memory().numpy() for u in states[:3]]
+    ins = pinned + [u.copy() for u in states[3:]]
+    outs = [torch.empty(g.U0.shape, dtype=torch.float64).pin_memory().numpy() for _ in range(3)] + \
+        [np.full(g.U0.shape, np.nan) for _ in range(2)]
+    s.residuals_host(ins, outs, 2)
+    for got, ref in zip(outs, want):
+        assert np.array_equal(got, ref)
+    assert np.array_equal(s.get_residual(2), want[-1])
+    s.residuals_host([], [], 0)  # nothing to do
+    s.residuals_host(ins[:1], outs[:1], 2)
+    assert np.array_equal(outs[0], want[0])

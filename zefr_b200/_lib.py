@@ -41,6 +41,7 @@ EXPORTED = [
     "zb_geometry_eval", "zb_geometry_eval_vjp", "zb_set_nodes",
     "zb_compute_residual_start", "zb_compute_residual_mid", "zb_compute_residual_finish",
     "zb_rk_stage_start", "zb_rk_stage_mid", "zb_rk_stage_finish", "zb_operator_mm_tf32x3",
+    "zb_compute_residuals_host",
 ]
 ZB_RK44, ZB_RK54 = 0, 1
 ZB_NKERNELS = 11
@@ -139,6 +140,8 @@ def lib() -> ctypes.CDLL:
         L.zb_compute_residual.argtypes = [vp, ctypes.c_uint]
         L.zb_get_residual.argtypes = [vp, ctypes.c_uint, dp, i64, i64, i64, ctypes.c_int]
         L.zb_rk_stage.argtypes = [vp, ctypes.c_uint]
+        L.zb_compute_residuals_host.argtypes = [vp, ctypes.c_uint, ctypes.c_int, ctypes.POINTER(dp),
+                                                ctypes.POINTER(dp)]
         fp = ctypes.POINTER(ctypes.c_float)
         L.zb_operator_mm_tf32x3.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, fp,
                                             ctypes.c_int, fp, ctypes.c_int, ctypes.c_float, fp, ctypes.c_int, vp]

@@ -329,6 +329,14 @@ zb_status zb_get_residual(zb_ctx *ctx, unsigned stage, double *out, int64_t ss, 
   })
 }
 
+zb_status zb_compute_residuals_host(zb_ctx *ctx, unsigned stage, int n, const double *const *U, double *const *divF)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(ctx, "null context");
+    zb::ctx_residuals_host(ctx->impl, stage, n, U, divF);
+  })
+}
+
 zb_status zb_rk_stage(zb_ctx *ctx, unsigned stage)
 {
   ZB_GUARD({

@@ -533,6 +533,15 @@ static void free_all(Ctx *c)
   for (void *b : bufs)
     if (b) cudaFree(b);
   if (c->tc_err_host) cudaFreeHost(const_cast<int *>(c->tc_err_host));
+  for (int b = 0; b < 2; b++)
+  {
+    if (c->pipe_in[b]) cudaFree(c->pipe_in[b]);
+    if (c->pipe_out[b]) cudaFree(c->pipe_out[b]);
+  }
+  if (c->pipe_h2d) cudaStreamDestroy(c->pipe_h2d);
+  if (c->pipe_d2h) cudaStreamDestroy(c->pipe_d2h);
+  for (auto e : c->pipe_ev)
+    if (e) cudaEventDestroy(e);
   for (auto &r : c->recs)
   {
     cudaEventDestroy(r.a);
@@ -870,6 +879,63 @@ void ctx_get_residual(Ctx *c, unsigned stage, double *out, int64_t ss, int64_t v
   if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
   if (!out) ZB_THROW(ZB_ERR_ARG, "null output");
   from_tiles(c, c->divF[stage], nullptr, nullptr, out, ss, vs, es, where);
+}
+
+// divF_spts(stage) of n states held in host memory, dense in the reference
+// layout [nspts][nvars][n_eles].  A software pipeline over two input and two
+// output staging buffers: the host-to-device copy of state i+1 (its own
+// stream and copy engine) and the device-to-host copy of residual i-1 (the
+// other copy engine) run while residual i is computed on the context's
+// stream; events hand each buffer from one stream to the next.
+void ctx_residuals_host(Ctx *c, unsigned stage, int n, const double *const *U, double *const *R)
+{
+  if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
+  if (n < 0) ZB_THROW(ZB_ERR_ARG, "negative state count");
+  if (n == 0) return;
+  if (!U || !R) ZB_THROW(ZB_ERR_ARG, "null state or residual list");
+  for (int i = 0; i < n; i++)
+    if (!U[i] || !R[i]) ZB_THROW(ZB_ERR_ARG, "null state or residual pointer at index " + std::to_string(i));
+  const int64_t E = c->plan.neles;
+  const size_t ext = (size_t)c->S * c->V * E, bytes = ext * sizeof(double);
+  if (!c->pipe_h2d)
+  {
+    for (int b = 0; b < 2; b++)
+    {
+      c->pipe_in[b] = (double *)dalloc(bytes);
+      c->pipe_out[b] = (double *)dalloc(bytes);
+    }
+    CK(cudaStreamCreateWithFlags(&c->pipe_h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->pipe_d2h, cudaStreamNonBlocking));
+    for (auto &e : c->pipe_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  // events per buffer b: in_ready, in_free, out_ready, out_free
+  cudaEvent_t *in_ready = c->pipe_ev, *in_free = c->pipe_ev + 2, *out_ready = c->pipe_ev + 4,
+              *out_free = c->pipe_ev + 6;
+  const int64_t ss = (int64_t)c->V * E, vs = E, es = 1;
+  // nothing queued earlier on the context's stream may still use the buffers
+  CK(cudaEventRecord(in_free[0], c->stream));
+  CK(cudaEventRecord(in_free[1], c->stream));
+  CK(cudaEventRecord(out_free[0], c->stream));
+  CK(cudaEventRecord(out_free[1], c->stream));
+  for (int i = 0; i < n; i++)
+  {
+    const int b = i & 1;
+    CK(cudaStreamWaitEvent(c->pipe_h2d, in_free[b], 0));
+    CK(cudaMemcpyAsync(c->pipe_in[b], U[i], bytes, cudaMemcpyHostToDevice, c->pipe_h2d));
+    CK(cudaEventRecord(in_ready[b], c->pipe_h2d));
+    CK(cudaStreamWaitEvent(c->stream, in_ready[b], 0));
+    ctx_set_state(c, c->pipe_in[b], ss, vs, es, ZB_DEVICE);
+    CK(cudaEventRecord(in_free[b], c->stream));
+    ctx_compute_residual(c, stage);
+    CK(cudaStreamWaitEvent(c->stream, out_free[b], 0));
+    from_tiles(c, c->divF[stage], nullptr, nullptr, c->pipe_out[b], ss, vs, es, ZB_DEVICE);
+    CK(cudaEventRecord(out_ready[b], c->stream));
+    CK(cudaStreamWaitEvent(c->pipe_d2h, out_ready[b], 0));
+    CK(cudaMemcpyAsync(R[i], c->pipe_out[b], bytes, cudaMemcpyDeviceToHost, c->pipe_d2h));
+    CK(cudaEventRecord(out_free[b], c->pipe_d2h));
+  }
+  CK(cudaStreamSynchronize(c->pipe_d2h));
+  CK(cudaStreamSynchronize(c->pipe_h2d));
 }
 
 static StageCfg rk_stage_cfg(const Ctx *c, unsigned stage)

@@ -26,6 +26,7 @@ void ctx_set_state(Ctx *c, const double *U, int64_t ss, int64_t vs, int64_t es, 
 void ctx_get_state(Ctx *c, double *U, int64_t ss, int64_t vs, int64_t es, int where);
 void ctx_compute_residual(Ctx *c, unsigned stage);
 void ctx_get_residual(Ctx *c, unsigned stage, double *out, int64_t ss, int64_t vs, int64_t es, int where);
+void ctx_residuals_host(Ctx *c, unsigned stage, int n, const double *const *U, double *const *R);
 void ctx_rk_stage(Ctx *c, unsigned stage);
 // C = alpha A B + beta C on the tensor pipe (TF32x3, tc_opmm.cu), queued on st
 void opmm_tc(int m, int n, int k, float alpha, const float *a, int lda, const float *b, int ldb, float beta, float *c,

@@ -107,6 +107,12 @@ struct Ctx
   double *dfw = nullptr;      // face-point quadrature weights [Fp / faces]
   void *U_til = nullptr, *rk_err = nullptr;
   bool use_dt_dev = false, use_dt_ele = false;  // stage kernels read the step from d_dt / dt_ele
+  // residuals of host-resident states with overlapped copies
+  // (ctx_residuals_host): two input and two output staging buffers, a copy
+  // stream per direction, and the events that hand the buffers over
+  double *pipe_in[2] = {nullptr, nullptr}, *pipe_out[2] = {nullptr, nullptr};
+  cudaStream_t pipe_h2d = nullptr, pipe_d2h = nullptr;
+  cudaEvent_t pipe_ev[8] = {};
   // tensor-core kernels' timeout flag: mapped pinned host memory (host and
   // device addresses), checked before each stage launch
   volatile int *tc_err_host = nullptr;

@@ -263,6 +263,21 @@ class FRSolver:
         check(lib().zb_get_residual(self.h, stage, out.ctypes.data_as(_DP), *self._strides(), _lib.ZB_HOST))
         return out
 
+    def residuals_host(self, states, outs, stage: int = 0) -> None:
+        """divF(stage) of each host state into the matching host array
+        (zb_compute_residuals_host): C-contiguous float64 arrays of
+        state_shape; pinned memory (e.g. numpy views of pinned torch tensors)
+        lets the copies overlap the computation."""
+        if len(states) != len(outs):
+            raise ValueError("states and outputs differ in number")
+        for a in list(states) + list(outs):
+            if a.shape != self.state_shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("arrays must be C-contiguous float64 of state_shape")
+        n = len(states)
+        U = (_DP * n)(*[a.ctypes.data_as(_DP) for a in states])
+        R = (_DP * n)(*[a.ctypes.data_as(_DP) for a in outs])
+        check(lib().zb_compute_residuals_host(self.h, stage, n, U, R))
+
     def get_residual_device(self, out, stage: int = 0) -> None:
         """Copy a residual register into a contiguous float64 CUDA tensor
         (complete on return)."""
