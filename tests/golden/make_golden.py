@@ -105,6 +105,16 @@ def _cases():
                               angled_state, 2),
         "tri_p1_ns_adi": (lambda: meshgen.box_tris(4, 0.0, 1.0, seed=4, bnd="WALL"), 2, 1, True,
                           {"WALL": "wall_ns_adi"}, cyl_deck, shear_unit, 2),
+        # higher orders (Williams-Shunn points P5-P8)
+        "tri_p5_ns_jitter": (lambda: meshgen.box_tris(3, seed=5), 2, 5, True, per,
+                             dict(cyl_deck, Re_fs=1000, prandtl=0.71), shear_unit, 2),
+        "tri_p6_euler_vortex": (lambda: meshgen.box_tris(3, -5.0, 5.0, seed=6), 2, 6, False, per, eul, vortex, 2),
+        "tri_p7_ns_adi": (lambda: meshgen.box_tris(3, 0.0, 1.0, seed=7, bnd="WALL"), 2, 7, True,
+                          {"WALL": "wall_ns_adi"}, cyl_deck, shear_unit, 1),
+        "tri_p8_euler_char": (lambda: meshgen.box_tris(2, -2.0, 2.0, seed=8, bnd="FARFIELD"), 2, 8, False,
+                              {"FARFIELD": "char"},
+                              dict(eul, mach_fs=0.2, nx_fs=math.cos(math.pi / 6), ny_fs=math.sin(math.pi / 6)),
+                              angled_state, 1),
     }
 
 

@@ -444,7 +444,7 @@ static void launch_stage_tri(Ctx &c, const StageCfg &sc)
     {
       ProfScope ps(c, ZB_K_NS_GRAD);
       bool launched = false;
-      if constexpr (std::is_same<A, float>::value)
+      if constexpr (std::is_same<A, float>::value && N <= 5)
       {
         if (c.plan.params.tensor_ops)
         {
@@ -495,7 +495,8 @@ static void bind_t(Ctx &c)
     c.launch_stage = &launch_stage_tri<T, A, NN>;         \
     return;                                               \
   }
-    ZB_BIND_TRI(2) ZB_BIND_TRI(3) ZB_BIND_TRI(4) ZB_BIND_TRI(5)
+    ZB_BIND_TRI(2) ZB_BIND_TRI(3) ZB_BIND_TRI(4) ZB_BIND_TRI(5) ZB_BIND_TRI(6) ZB_BIND_TRI(7) ZB_BIND_TRI(8)
+    ZB_BIND_TRI(9)
 #undef ZB_BIND_TRI
     ZB_THROW(ZB_ERR_UNSUPPORTED, "no triangle kernels for P=" + std::to_string(N - 1));
   }
@@ -626,9 +627,9 @@ Ctx *ctx_create(const Plan &plan)
   c->ntiles = plan.ntiles;
   c->dt = plan.params.dt;
   if (plan.tile != TW) ZB_THROW(ZB_ERR_INTERNAL, "plan tile width does not match kernels");
-  if (plan.params.tensor_ops && !(c->prec == ZB_MIXED && plan.etype == ET_TRI && plan.params.viscous))
+  if (plan.params.tensor_ops && !(c->prec == ZB_MIXED && plan.etype == ET_TRI && plan.params.viscous && plan.order <= 4))
     ZB_THROW(ZB_ERR_UNSUPPORTED, "tensor-core operator products are built for the mixed form on triangles "
-                                 "(Navier-Stokes)");
+                                 "(Navier-Stokes, P <= 4)");
   if (c->prec == ZB_FP64)
   {
     bind_t<double, double>(*c);

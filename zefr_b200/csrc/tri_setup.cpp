@@ -50,8 +50,42 @@ static std::vector<WsOrbit> ws_orbits(int P)
               {3, {-0.5165412084640660, 0.0330824169281320, 0}, 0.2554243917625300},
               {3, {-0.0513824244458420, -0.8972351511083160, 0}, 0.1524121247710700},
               {6, {0.5023672622129680, -0.5969922362364000, -0.9053750259765680}, 0.1114996200542300}};
+    case 5:
+      return {{3, {-0.9437740956346720, 0.8875481912693440, 0}, 0.0207187493930760},
+              {3, {-0.6457218030613660, 0.2914436061227320, 0}, 0.1507897686534760},
+              {3, {-0.1889828082651340, -0.6220343834697321, 0}, 0.1950956047464840},
+              {6, {0.6358019600569980, -0.7028683754582260, -0.9329335845987720}, 0.0579385387449460},
+              {6, {0.2099578235502660, -0.2856074027686380, -0.9243504207816280}, 0.0920927331918700}};
+    case 6:
+      return {{1, {-0.3333333333333330, 0, 0}, 0.1672164244312740},
+              {3, {-0.9600456257556140, 0.9200912515112279, 0}, 0.0105443405609900},
+              {3, {-0.7365564649400040, 0.4731129298800080, 0}, 0.0891058733590080},
+              {3, {-0.0297293064130780, -0.9405413871738439, 0}, 0.0676314256083960},
+              {6, {0.7358224202359001, -0.7840960363079780, -0.9517263839279220}, 0.0314209226803660},
+              {6, {0.4017451407614460, -0.4583184541568660, -0.9434266866045800}, 0.0564102725612320},
+              {6, {0.0733093684122760, -0.3669008023107660, -0.7064085661015100}, 0.1339919142556600}};
+    case 7:
+      return {{3, {-0.9576571544410700, 0.9153143088821400, 0}, 0.0112782475738200},
+              {3, {-0.7988312052082240, 0.5976624104164480, 0}, 0.0542979363845560},
+              {3, {-0.4579233845761360, -0.0841532308477280, 0}, 0.1262018250667180},
+              {3, {-0.1196174831923360, -0.7607650336153280, 0}, 0.1035055913597980},
+              {6, {0.7599592828544620, -0.9634866418505040, -0.7964726410039580}, 0.0197335071492920},
+              {6, {0.1651240457273440, -0.2119334566600260, -0.9531905890673180}, 0.0440164096002940},
+              {6, {0.5030612290855641, -0.5475089381815420, -0.9555522909040221}, 0.0332891401534720},
+              {6, {0.2714743665262100, -0.5018415447573360, -0.7696328217688740}, 0.0886524762378280}};
+    case 8:
+      return {{3, {-0.8958458673313620, 0.7916917346627240, 0}, 0.0264519521410120},
+              {3, {-0.7725869427780080, 0.5451738855560160, 0}, 0.0347516292773620},
+              {3, {-0.5656623084521640, 0.1313246169043280, 0}, 0.0945461565676520},
+              {3, {-0.2278544512773540, -0.5442910974452920, 0}, 0.1060044409420360},
+              {3, {-0.0201481341734600, -0.9597037316530800, 0}, 0.0378851639278180},
+              {6, {0.6693761812315560, -0.7035037567771640, -0.9658724244543920}, 0.0238755661869220},
+              {6, {0.4144959853084960, -0.5795767423228601, -0.8349192429856360}, 0.0493958430852700},
+              {6, {0.9258038332858580, -0.9258815152162200, -0.9999223180696380}, 0.0043857672678220},
+              {6, {0.3480122228257960, -0.3820797590136400, -0.9659324638121560}, 0.0308750382999060},
+              {6, {0.0838979176456600, -0.2793516463213580, -0.8045462713243020}, 0.0749814470654740}};
     default:
-      ZB_THROW(ZB_ERR_UNSUPPORTED, "triangle solution points built for P = 1..4, not P = " + std::to_string(P));
+      ZB_THROW(ZB_ERR_UNSUPPORTED, "triangle solution points built for P = 1..8, not P = " + std::to_string(P));
   }
 }
 
