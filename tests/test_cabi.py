@@ -81,8 +81,8 @@ def test_gmsh_reader_errors(tmp_path):
 
 def test_unsupported_element_and_order():
     m = meshgen.box_tris(2, seed=0, jitter=0.0)
-    Plan(m, make_params(4), {"PERIODIC": "periodic"})  # triangles P1-P4 are built
-    e = _err(lambda: Plan(m, make_params(5), {"PERIODIC": "periodic"}))
+    Plan(m, make_params(8), {"PERIODIC": "periodic"})  # triangles P1-P8 are built
+    e = _err(lambda: Plan(m, make_params(9), {"PERIODIC": "periodic"}))
     assert e.status == -4
     e = _err(lambda: Plan(meshgen.box_quads(2, 2), make_params(12), {"PERIODIC": "periodic"}))
     assert e.status == -4
