@@ -668,9 +668,27 @@ def gpu_arm(args):
 
 def profile_run(args):
     """Short run of one form for an external profiler: W + K residuals (or
-    adjoint applications at the FP64 form), no timing."""
+    adjoint applications at the FP64 form, or, for "opmm", tensor-core
+    products of the hexahedral P3 extrapolation operator's shape, 96 x 64, on
+    5 n^3 columns), no timing."""
     import torch
     torch.cuda.set_device(0)
+    if args.profile_form == "opmm":
+        from zefr_b200 import _lib
+        fp = ctypes.POINTER(ctypes.c_float)
+        m, k, n = 96, 64, 5 * args.cells ** 3
+        g = torch.Generator(device="cuda").manual_seed(1)
+        A = torch.randn(m, k, device="cuda", generator=g)
+        B = torch.randn(k, n, device="cuda", generator=g)
+        C = torch.empty(m, n, device="cuda")
+        for _ in range(args.warmup + args.steps):
+            st = _lib.lib().zb_operator_mm_tf32x3(m, n, k, 1.0, ctypes.cast(A.data_ptr(), fp), k,
+                                                  ctypes.cast(B.data_ptr(), fp), n, 0.0,
+                                                  ctypes.cast(C.data_ptr(), fp), n, None)
+            if st != 0:
+                raise RuntimeError(_lib.lib().zb_last_error().decode())
+        torch.cuda.synchronize()
+        return
     adj = args.profile_form == "adjoint"
     if args.profile_form.startswith("tri-"):
         s = triangle_solver(args.profile_form[4:])
@@ -754,7 +772,8 @@ def main():
     ap.add_argument("--ref-cells", type=int, default=REF_CELLS, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-side", action="store_true", help="skip the triangle and batched side workloads")
-    ap.add_argument("--profile-form", choices=["mixed", "fp64", "adjoint", "tri-mixed", "tri-mixed_tc", "tri-fp64"],
+    ap.add_argument("--profile-form", choices=["mixed", "fp64", "adjoint", "tri-mixed", "tri-mixed_tc", "tri-fp64",
+                                               "opmm"],
                     default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.warmup < 3:
