@@ -294,49 +294,78 @@ __device__ __forceinline__ A step_dt(const Args<T, A> &a, int64_t tile, int l)
 template <typename T, typename A, int S, int V, int NM>
 __device__ __forceinline__ void store_rk(const Args<T, A> &a, int64_t tile, int s, int l, const A res[V], A *sUnew)
 {
-  constexpr int D = NM == 5 ? 2 : 3;
+  constexpr int D = NM == 5 ? 2 : 3, MAXPREV = 3;
   const int64_t base = (tile * S + s) * (int64_t)V * TW;
+  if (a.rk_mode == 0)
+  {
 #pragma unroll
-  for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
-  if (a.rk_mode == 0) return;
+    for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
+    return;
+  }
+  // every load of the point before the first store: a load cannot move above
+  // a store that may alias it, so interleaving them serialises the accesses
   const A detJ = a.mets[((tile * S + s) * NM + D * D) * TW + l];
   const A dtv = step_dt(a, tile, l);
+  const bool fast = a.rk_mode == 1 || a.nprev <= MAXPREV;
+  A u_ini[V], prev[MAXPREV][V], comp[V];
 #pragma unroll
   for (int v = 0; v < V; v++)
   {
     const int64_t idx = base + v * TW + l;
-    A u_ini;
-    if (a.save_ini)
-    {
-      u_ini = a.U[idx];
-      a.U_ini[idx] = u_ini;
-    }
-    else
-      u_ini = a.U_ini[idx];
+    u_ini[v] = a.save_ini ? (A)a.U[idx] : (A)a.U_ini[idx];
+    comp[v] = (a.rk_mode == 2 && a.Ucomp) ? (A)a.Ucomp[idx] : A(0);
+  }
+  if (a.rk_mode == 2 && fast)
+  {
+#pragma unroll
+    for (int st = 0; st < MAXPREV; st++)
+      if (st < a.nprev)
+      {
+#pragma unroll
+        for (int v = 0; v < V; v++) prev[st][v] = (A)a.divF_prev[st][base + v * TW + l];
+      }
+  }
+#pragma unroll
+  for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
+#pragma unroll
+  for (int v = 0; v < V; v++)
+  {
+    const int64_t idx = base + v * TW + l;
+    if (a.save_ini) a.U_ini[idx] = u_ini[v];
     A unew;
     if (a.rk_mode == 1)
-      unew = u_ini - a.rk_coef[0] * dtv / detJ * res[v];
-    else
+      unew = u_ini[v] - a.rk_coef[0] * dtv / detJ * res[v];
+    else if (a.Ucomp)
     {
-      if (a.Ucomp)
+      // Kahan-compensated accumulation of the step increment; the
+      // remainder includes the rounding of the stored state
+      A delta = A(0);
+      if (fast)
       {
-        // Kahan-compensated accumulation of the step increment; the
-        // remainder includes the rounding of the stored state
-        A delta = A(0);
-        for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * dtv / detJ * (A)a.divF_prev[st][idx];
-        delta -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
-        const A c = a.Ucomp[idx];
-        const A y = delta - c;
-        unew = (A)(T)(u_ini + y);
-        a.Ucomp[idx] = (T)((unew - u_ini) - y);
+#pragma unroll
+        for (int st = 0; st < MAXPREV; st++)
+          if (st < a.nprev) delta -= a.rk_coef[st] * dtv / detJ * prev[st][v];
       }
       else
+        for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * dtv / detJ * (A)a.divF_prev[st][idx];
+      delta -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
+      const A y = delta - comp[v];
+      unew = (A)(T)(u_ini[v] + y);
+      a.Ucomp[idx] = (T)((unew - u_ini[v]) - y);
+    }
+    else
+    {
+      // reference order: U = U_ini; U -= b_s dt/|J| divF_s for s = 0..
+      unew = u_ini[v];
+      if (fast)
       {
-        // reference order: U = U_ini; U -= b_s dt/|J| divF_s for s = 0..
-        unew = u_ini;
-        for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * dtv / detJ * a.divF_prev[st][idx];
-        unew -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
+#pragma unroll
+        for (int st = 0; st < MAXPREV; st++)
+          if (st < a.nprev) unew -= a.rk_coef[st] * dtv / detJ * prev[st][v];
       }
+      else
+        for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * dtv / detJ * a.divF_prev[st][idx];
+      unew -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
     }
     a.Uout[idx] = unew;
     if (sUnew) sUnew[(s * V + v) * TW + l] = (A)(T)unew;  // the state as stored

@@ -285,49 +285,82 @@ __device__ __forceinline__ A hex_surface(const LineOpsT<A, N> &ops, const RowOps
 }
 
 // RK update of one spt and optional staging of the new state for extrapolation
-// (src/solver.cpp:2916-2937, 3040-3094)
+// (src/solver.cpp:2916-2937, 3040-3094).  Every load of the point (RK start
+// state, earlier residual registers, compensation remainder) is issued before
+// the first store: the compiler cannot move a load above a store that may
+// alias it, so interleaving them would serialise the point's memory accesses.
 template <typename T, typename A, int N>
 __device__ __forceinline__ void hex_finish(const Args<T, A> &a, int64_t tile, int s, int l, const A res[5], A *sUnew)
 {
   using H = HexIdx<N>;
-  constexpr int V = 5, NM = 10;
+  constexpr int V = 5, NM = 10, MAXPREV = 3;
   const int64_t base = (tile * H::S + s) * (int64_t)V * TW;
+  if (a.rk_mode == 0)
+  {
 #pragma unroll
-  for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
-  if (a.rk_mode == 0) return;
+    for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
+    return;
+  }
   const A detJ = a.mets[((tile * H::S + s) * NM + 9) * TW + l];
   const A dtv = step_dt(a, tile, l);
+  const bool fast = a.rk_mode == 1 || a.nprev <= MAXPREV;
+  A u_ini[V], prev[MAXPREV][V], comp[V];
 #pragma unroll
   for (int v = 0; v < V; v++)
   {
     const int64_t idx = base + v * TW + l;
-    A u_ini;
-    if (a.save_ini)
-    {
-      u_ini = a.U[idx];
-      a.U_ini[idx] = u_ini;
-    }
-    else
-      u_ini = a.U_ini[idx];
+    u_ini[v] = a.save_ini ? (A)a.U[idx] : (A)a.U_ini[idx];
+    comp[v] = (a.rk_mode == 2 && a.Ucomp) ? (A)a.Ucomp[idx] : A(0);
+  }
+  if (a.rk_mode == 2 && fast)
+  {
+#pragma unroll
+    for (int st = 0; st < MAXPREV; st++)
+      if (st < a.nprev)
+      {
+#pragma unroll
+        for (int v = 0; v < V; v++) prev[st][v] = (A)a.divF_prev[st][base + v * TW + l];
+      }
+  }
+#pragma unroll
+  for (int v = 0; v < V; v++) a.divF[base + v * TW + l] = res[v];
+#pragma unroll
+  for (int v = 0; v < V; v++)
+  {
+    const int64_t idx = base + v * TW + l;
+    if (a.save_ini) a.U_ini[idx] = u_ini[v];
     A unew;
     if (a.rk_mode == 1)
-      unew = u_ini - a.rk_coef[0] * dtv / detJ * res[v];
+      unew = u_ini[v] - a.rk_coef[0] * dtv / detJ * res[v];
     else if (a.Ucomp)
     {
       // Kahan-compensated step increment; the remainder includes the
       // rounding of the stored state
       A delta = A(0);
-      for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * dtv / detJ * (A)a.divF_prev[st][idx];
+      if (fast)
+      {
+#pragma unroll
+        for (int st = 0; st < MAXPREV; st++)
+          if (st < a.nprev) delta -= a.rk_coef[st] * dtv / detJ * prev[st][v];
+      }
+      else
+        for (int st = 0; st < a.nprev; st++) delta -= a.rk_coef[st] * dtv / detJ * (A)a.divF_prev[st][idx];
       delta -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
-      const A c = a.Ucomp[idx];
-      const A y = delta - c;
-      unew = (A)(T)(u_ini + y);
-      a.Ucomp[idx] = (T)((unew - u_ini) - y);
+      const A y = delta - comp[v];
+      unew = (A)(T)(u_ini[v] + y);
+      a.Ucomp[idx] = (T)((unew - u_ini[v]) - y);
     }
     else
     {
-      unew = u_ini;
-      for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * dtv / detJ * a.divF_prev[st][idx];
+      unew = u_ini[v];
+      if (fast)
+      {
+#pragma unroll
+        for (int st = 0; st < MAXPREV; st++)
+          if (st < a.nprev) unew -= a.rk_coef[st] * dtv / detJ * prev[st][v];
+      }
+      else
+        for (int st = 0; st < a.nprev; st++) unew -= a.rk_coef[st] * dtv / detJ * a.divF_prev[st][idx];
       unew -= a.rk_coef[a.nprev] * dtv / detJ * res[v];
     }
     a.Uout[idx] = unew;
