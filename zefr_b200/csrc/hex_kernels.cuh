@@ -780,14 +780,25 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::face_zs, HexNsS
   else
     hex_common_flux<T, A, N, true, ZS>(a, tile, l, ix, iy, sFc, zs);
   __syncthreads();
-#pragma unroll 1
-  for (int iz = zs * NZ; iz < (zs + 1) * NZ; iz++)
+  // the volume residual of all of this thread's levels before any store
+  // (a load cannot move above a store that may alias it)
+  A dvol[NZ][V];
+#pragma unroll
+  for (int k = 0; k < NZ; k++)
   {
-    const int s = ix + N * iy + H::N2 * iz;
+    const int s = ix + N * iy + H::N2 * (zs * NZ + k);
     const A *dv = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
+#pragma unroll
+    for (int v = 0; v < V; v++) dvol[k][v] = dv[v * TW];
+  }
+#pragma unroll
+  for (int k = 0; k < NZ; k++)
+  {
+    const int iz = zs * NZ + k;
+    const int s = ix + N * iy + H::N2 * iz;
     A res[V];
 #pragma unroll
-    for (int v = 0; v < V; v++) res[v] = dv[v * TW] + hex_surface<A, N>(ops, o, sFc, ix, iy, iz, v, l);
+    for (int v = 0; v < V; v++) res[v] = dvol[k][v] + hex_surface<A, N>(ops, o, sFc, ix, iy, iz, v, l);
     hex_finish<T, A, N>(a, tile, s, l, res, a.extrap_next ? sUnew : nullptr);
   }
   if (a.extrap_next)
