@@ -19,10 +19,12 @@ pytestmark = pytest.mark.gpu
 TOL_FD = 1e-6
 H = 1e-7
 
-# every boundary kind, Euler and Navier-Stokes, quads and hexes, beta 0.5 and 0.3
+# every boundary kind, Euler and Navier-Stokes, quads, hexes and triangles
+# (P1-P8), beta 0.5 and 0.3
 CASES = ["quad_p1_euler", "quad_p3_euler_vortex", "quad_p5_euler", "quad_p2_ns_jitter", "hex_p1_ns",
          "hex_p2_euler_jitter", "hex_p3_ns_tgv", "cyl_p3_ns_char_adi", "cyl_p2_ns_iso_farfield_b03",
-         "cyl_p3_euler_slip_char", "cyl_p2_euler_supin_sym"]
+         "cyl_p3_euler_slip_char", "cyl_p2_euler_supin_sym", "tri_p1_ns_adi", "tri_p2_euler_vortex",
+         "tri_p3_euler_char", "tri_p4_ns_jitter", "tri_p5_ns_jitter", "tri_p7_ns_adi", "tri_p8_euler_char"]
 
 
 def solver_for(g, **kw):
@@ -51,8 +53,31 @@ def test_vjp_matches_central_differences(name):
     assert abs(lhs - rhs) <= TOL_FD * max(abs(rhs), 1e-300), (lhs, rhs)
 
 
+@pytest.mark.parametrize("name", ["tri_p4_ns_jitter", "tri_p3_euler_char"])
+def test_vjp_roe_matches_central_differences(name):
+    """The Roe flux's reverse mode on triangles (the golden cases run the
+    reference's Rusanov)."""
+    g = gc.load(name)
+    s = solver_for(g, fconv="roe")
+    lam, v = _directions(g, 13)
+    s.set_state(g.U0)
+    lhs = float(np.sum(s.vjp(lam) * v))
+    rhs = float(np.sum(lam * (s.residual(g.U0 + H * v) - s.residual(g.U0 - H * v))) / (2 * H))
+    assert abs(lhs - rhs) <= TOL_FD * max(abs(rhs), 1e-300), (lhs, rhs)
+
+
+def test_vjp_geometry_rejected_on_triangles():
+    from zefr_b200._lib import ZbError
+    g = gc.load("tri_p2_euler_vortex")
+    s = solver_for(g)
+    s.set_state(g.U0)
+    with pytest.raises(ZbError) as ei:
+        s.vjp_geometry(np.ones(g.U0.shape))
+    assert ei.value.status == -4
+
+
 @pytest.mark.parametrize("name", ["cyl_p3_ns_char_adi", "cyl_p2_ns_iso_farfield_b03", "cyl_p3_euler_slip_char",
-                                  "cyl_p2_euler_supin_sym"])
+                                  "cyl_p2_euler_supin_sym", "tri_p3_euler_char", "tri_p8_euler_char"])
 def test_vjp_freestream_matches_central_differences(name):
     g = gc.load(name)
     s = solver_for(g)

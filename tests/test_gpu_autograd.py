@@ -32,7 +32,7 @@ def test_residual_backward_is_the_library_adjoint():
     assert np.array_equal(U.grad.cpu().numpy(), ref)
 
 
-@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "cyl_p3_ns_char_adi"])
+@pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "cyl_p3_ns_char_adi", "tri_p4_ns_jitter"])
 def test_rk_step_vjp_equals_composed_stage_adjoints(name):
     """zb_rk_step_vjp against the RK44 transpose written out here from the
     residual adjoint (zb_vjp) and the stage tables of src/solver.cpp:722-735:

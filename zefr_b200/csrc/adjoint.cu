@@ -2,6 +2,7 @@
 // translation unit so they build in parallel with the forward kernels.
 #include "ctx_impl.cuh"
 #include "adjoint.cuh"
+#include "tri_adjoint.cuh"
 
 namespace zb {
 
@@ -87,10 +88,76 @@ static void launch_vjp_impl(Ctx &c, bool params, bool geo)
     launch_adj_kernels<D, N, false>(c, a, ops);
 }
 
+// Triangles: lift, then the Euler pass or the two Navier-Stokes passes
+// (tri_adjoint.cuh); the state and free-stream adjoints, no geometry adjoint.
+template <int N>
+static void launch_vjp_tri(Ctx &c, bool params, bool geo)
+{
+  if (geo) ZB_THROW(ZB_ERR_UNSUPPORTED, "the geometry adjoint is built for quadrilaterals and hexahedra");
+  using G = dev::TriShape<N>;
+  dev::AdjArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.U = (const double *)c.U;
+  a.Ufp = (const double *)c.Ufp[c.cur];
+  a.mets = (const double *)c.mets;
+  a.fgeo = (const double *)c.fgeo;
+  a.nbr = c.nbr;
+  a.lam = c.lam;
+  a.Lfp = c.Lfp;
+  a.Ubfp = c.Ubfp;
+  a.dUbfp = c.dUbfp;
+  a.Ubx = c.Ubx;
+  a.UCb = c.UCb;
+  a.Ubar = c.Ubar;
+  a.pbar = params ? c.pbar : nullptr;
+  a.Fvn = (const double *)c.Fvn;
+  a.dops = (const double *)c.dops;
+  a.ntiles = c.ntiles;
+  a.ph = phys_of<double>(c.plan.params, c.uref, 2, false);
+  {
+    ProfScope ps(c, ZB_K_ADJ_LIFT);
+    dev::k_tri_adj_lift<N><<<grid_for(c.ntiles * G::Fp * TW, 128), 128, 0, c.stream>>>(a);
+    c.launches++;
+    CK(cudaGetLastError());
+  }
+  if (!c.plan.params.viscous)
+  {
+    const size_t smem = dev::tri_adj_euler_smem<N>();
+    set_smem(dev::k_tri_adj_euler<N>, smem);
+    ProfScope ps(c, ZB_K_ADJ_VOL);
+    dev::k_tri_adj_euler<N><<<(unsigned)c.ntiles, 128, smem, c.stream>>>(a);
+    c.launches++;
+    CK(cudaGetLastError());
+    return;
+  }
+  {
+    const size_t smem1 = dev::tri_adj_ns1_smem<N>();
+    set_smem(dev::k_tri_adj_ns1<N>, smem1);
+    ProfScope ps(c, ZB_K_ADJ_VOL);
+    dev::k_tri_adj_ns1<N><<<(unsigned)c.ntiles, 128, smem1, c.stream>>>(a);
+    c.launches++;
+    CK(cudaGetLastError());
+  }
+  const size_t smem2 = dev::tri_adj_ns2_smem<N>();
+  set_smem(dev::k_tri_adj_ns2<N>, smem2);
+  ProfScope ps(c, ZB_K_ADJ_TRACE);
+  dev::k_tri_adj_ns2<N><<<(unsigned)c.ntiles, 128, smem2, c.stream>>>(a);
+  c.launches++;
+  CK(cudaGetLastError());
+}
+
 void bind_vjp(Ctx &c)
 {
   c.launch_vjp = nullptr;
-  if (c.plan.etype == ET_TRI) return;  // tensor-product elements only
+  if (c.plan.etype == ET_TRI)
+  {
+#define ZB_BIND_TRI(NN) \
+  if (c.N == NN) { c.launch_vjp = &launch_vjp_tri<NN>; return; }
+    ZB_BIND_TRI(2) ZB_BIND_TRI(3) ZB_BIND_TRI(4) ZB_BIND_TRI(5) ZB_BIND_TRI(6) ZB_BIND_TRI(7) ZB_BIND_TRI(8)
+    ZB_BIND_TRI(9)
+#undef ZB_BIND_TRI
+    return;
+  }
   // the adjoint's shared memory fits hexahedra up to P3
 #define ZB_BIND(DD, NN) \
   if (c.D == DD && c.N == NN) { c.launch_vjp = &launch_vjp_impl<DD, NN>; return; }

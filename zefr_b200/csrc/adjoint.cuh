@@ -799,6 +799,7 @@ struct AdjArgs
                        // left side or the boundary; zero at right sides) and of the own dA
   double *nbx;         // NS: [tile][Fp][D][TW] right side's part of its face's normal adjoint
   const double *Fvn;   // NS: forward viscous normal flux at own flux points
+  const double *dops;  // triangles: the dense operators (TriShape layout)
   int64_t ntiles;
   Phys<double> ph;
 };
