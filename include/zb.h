@@ -436,7 +436,9 @@ int64_t zb_batch_launch_count(const zb_batch *batch);
  * divF as zb_compute_residual computes it.  param_bar, when not NULL,
  * receives d (lam . divF) / d (rho_fs, V_fs[0..2], P_fs), the free-stream
  * state the far-field and characteristic boundaries prescribe (5 doubles).
- * Plain FP64 contexts only; quadrilaterals P1-P5 and hexahedra P1-P3.
+ * Plain FP64 contexts only; quadrilaterals P1-P5, hexahedra P1-P3 and
+ * triangles P1-P8 (the geometry adjoint of zb_vjp_geometry: quadrilaterals
+ * and hexahedra).
  * No reference counterpart: the reference has no adjoint. */
 zb_status zb_vjp(zb_ctx *ctx, const double *lam, double *Ubar, int64_t spt_stride, int64_t var_stride,
                  int64_t ele_stride, int where, double *param_bar);
