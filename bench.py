@@ -313,6 +313,11 @@ def triangle_side(K: int, W: int):
         prof = kernel_profile(s, K)
         out[form] = {"gdof_s": dof / (ms * 1e-3) / 1e9, "ms_per_residual": ms, "dof": dof,
                      "kernels_ms": {k: v["ms_avg"] for k, v in prof.items() if v["launches"]}}
+        if form == "fp64":
+            # the triangle adjoint: one (d divF/dU)^T lam against one FP64 residual
+            adj = time_adjoint(s, s.get_state(), K, W)
+            out["adjoint"] = {"ms_per_vjp": adj["ms_per_vjp"], "kernels": adj["kernels"],
+                              "adjoint_over_forward": adj["ms_per_vjp"] / sum(out[form]["kernels_ms"].values())}
         s.close()
     nrm = np.linalg.norm(R["fp64"])
     out["mixed_rel_l2_err_vs_fp64"] = float(np.linalg.norm(R["mixed"] - R["fp64"]) / nrm)
