@@ -349,6 +349,18 @@ def batched_side(steps: int = 5, ncases: int = 512, seed: int = 4):
     bt.synchronize()
     ms_batch = (time.perf_counter() - t0) * 1e3 / steps
     batch_launches = (bt.launch_count() - n0) // steps
+    # the other form with the same launch shape: one launch per stage for all
+    # orders, or one per order, whichever the autotuner did not pick
+    bt.set_config(threads=cfg["threads"], blocks_per_sm=cfg["blocks_per_sm"], order=cfg["order"],
+                  group=cfg["group"], chunk=cfg["chunk"], fused=not cfg["fused"])
+    bt.step(2)
+    bt.synchronize()
+    n1 = bt.launch_count()
+    t0 = time.perf_counter()
+    bt.step(steps)
+    bt.synchronize()
+    ms_other = (time.perf_counter() - t0) * 1e3 / steps
+    other_launches = (bt.launch_count() - n1) // steps
     # one launch per case and stage, every case on its own context stream
     for c in cases:
         c.step(1)
@@ -380,13 +392,17 @@ def batched_side(steps: int = 5, ncases: int = 512, seed: int = 4):
            "setup_s": setup_s, "autotuned": cfg,
            "batched": {"gdof_s": dof * res_per_step / (ms_batch * 1e-3) / 1e9, "ms_per_step": ms_batch,
                        "launches_per_step": batch_launches,
-                       "kernels": "one persistent kernel per order present and stage, concurrent streams"},
+                       "kernels": ("one persistent kernel per stage for all orders" if cfg["fused"] else
+                                   "one persistent kernel per order present and stage, concurrent streams")},
            "one_launch_per_case": {"gdof_s": dof * res_per_step / (ms_single * 1e-3) / 1e9,
                                    "ms_per_step": ms_single, "launches_per_step": 4 * ncases,
                                    "streams": "one per case (concurrent)"},
            "one_launch_per_case_one_stream": {"gdof_s": dof * res_per_step / (ms_serial * 1e-3) / 1e9,
                                               "ms_per_step": ms_serial, "launches_per_step": 4 * ncases},
            "timing": "host clock around synchronised steps (both paths), 4 residuals per RK44 step"}
+    out["other_form"] = {"form": "one launch per stage (all orders)" if not cfg["fused"] else
+                         "one launch per order and stage", "gdof_s": dof * res_per_step / (ms_other * 1e-3) / 1e9,
+                         "ms_per_step": ms_other, "launches_per_step": other_launches}
     out["batched_over_single"] = ms_single / ms_batch
     out["batched_over_single_one_stream"] = ms_serial / ms_batch
     bt.close()

@@ -415,6 +415,10 @@ typedef struct zb_batch_config {
                          runs threads/group tiles at once */
   int chunk;          /* consecutive work items a group takes at a time; 0: one
                          contiguous run per group */
+  int fused;          /* 1: one persistent kernel per stage for all orders (each
+                         item dispatches to its order's tile body; registers and
+                         shared memory of the largest order present); 0: one
+                         kernel per order present, run concurrently */
 } zb_batch_config;
 
 zb_status zb_batch_create(zb_ctx *const *ctxs, int n, zb_batch **out);

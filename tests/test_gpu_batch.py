@@ -82,6 +82,26 @@ def test_autotune_keeps_state_and_picks_a_shape():
         assert _same(s1.get_state(), s2.get_state(), "mixed")
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("shape", [(256, 64, 0), (128, 128, 1), (256, 256, 8)])
+def test_fused_single_launch_matches_cases_stepped_alone(precision, shape):
+    """One persistent launch per stage for every order present: the same
+    stages as the cases stepped alone, four launches per step."""
+    alone, batched = _pair(precision, seed=21, n=9)
+    orders = len({s.case["P"] for s in alone})
+    assert orders >= 3
+    for s in alone:
+        s.step(3)
+    bt = zbatch.Batch(batched)
+    bt.set_config(threads=shape[0], blocks_per_sm=2, order=0, group=shape[1], chunk=shape[2], fused=True)
+    n0 = bt.launch_count()
+    bt.step(3)
+    bt.synchronize()
+    assert bt.launch_count() - n0 == 3 * 4
+    for s1, s2 in zip(alone, batched):
+        assert _same(s1.get_state(), s2.get_state(), precision)
+
+
 def test_graph_is_one_replay_of_one_launch_per_order_and_stage():
     cases = zbatch.vortex_cases(4, 1, n_range=(3, 5), precision="mixed")
     orders = len({c.info.order for c in cases})

@@ -80,7 +80,8 @@ class ZbTimeScheme(ctypes.Structure):
 
 class ZbBatchConfig(ctypes.Structure):
     _fields_ = [("threads", ctypes.c_int), ("blocks_per_sm", ctypes.c_int), ("order", ctypes.c_int),
-                ("ms_per_step", ctypes.c_double), ("group", ctypes.c_int), ("chunk", ctypes.c_int)]
+                ("ms_per_step", ctypes.c_double), ("group", ctypes.c_int), ("chunk", ctypes.c_int),
+                ("fused", ctypes.c_int)]
 
 
 class ZbDeck(ctypes.Structure):

@@ -89,10 +89,11 @@ class Batch:
         c = _lib.ZbBatchConfig()
         check(lib().zb_batch_autotune(self.h, steps, ctypes.byref(c)))
         return {"threads": c.threads, "group": c.group, "chunk": c.chunk, "blocks_per_sm": c.blocks_per_sm,
-                "order": c.order, "ms_per_step": c.ms_per_step}
+                "order": c.order, "ms_per_step": c.ms_per_step, "fused": c.fused}
 
-    def set_config(self, threads: int, blocks_per_sm: int, order: int = 0, group: int = 64, chunk: int = 1) -> None:
-        c = _lib.ZbBatchConfig(threads, blocks_per_sm, order, 0.0, group, chunk)
+    def set_config(self, threads: int, blocks_per_sm: int, order: int = 0, group: int = 64, chunk: int = 1,
+                   fused: bool = False) -> None:
+        c = _lib.ZbBatchConfig(threads, blocks_per_sm, order, 0.0, group, chunk, int(bool(fused)))
         check(lib().zb_batch_set_config(self.h, ctypes.byref(c)))
 
     def launch_count(self) -> int:

@@ -1,7 +1,8 @@
-// Batched RK stepping of many independent Euler cases on quadrilaterals: one
-// persistent launch per RK stage covers every tile of every case, the four
-// stages of a step are captured once as a CUDA graph, and a small autotuner
-// picks the launch shape.
+// Batched RK stepping of many independent Euler cases on quadrilaterals:
+// per RK stage either one persistent launch per polynomial order present (run
+// concurrently) or one persistent launch for all of them, the four stages of
+// a step captured once as a CUDA graph, and a small autotuner that picks the
+// form and the launch shape.
 //
 // Each case is an ordinary context (its own mesh, order 1-5, state, time
 // step and reference state); the batch only builds per-stage descriptors of
@@ -83,6 +84,53 @@ __global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__re
   }
 }
 
+// The single-launch form: one persistent kernel per stage walks the items of
+// every order (costliest order first) and runs each with its order's tile
+// body; the group's shared memory fits the largest order present.
+template <typename T, typename A>
+__global__ void __launch_bounds__(256) k_batch_euler_fused(const BatchCase<T, A> *__restrict__ cases,
+                                                           const int2 *__restrict__ items, int begin, int end, int gsz,
+                                                           int gstride, int chunk)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ng = blockDim.x / gsz, g = threadIdx.x / gsz, tid = threadIdx.x % gsz;
+  const int bar = (ng == 1) ? 0 : g + 1;
+  unsigned char *gbase = smem_raw + (size_t)g * gstride;
+  BatchCase<T, A> *sbc = reinterpret_cast<BatchCase<T, A> *>(gbase);
+  unsigned char *tsm = gbase + batch_desc_bytes<T, A>();
+  constexpr int nwords = (int)(sizeof(BatchCase<T, A>) / sizeof(int));
+  const int gid = blockIdx.x * ng + g, ngroups = gridDim.x * ng;
+  int have = -1;
+  for (int c0 = begin + gid * chunk; c0 < end; c0 += ngroups * chunk)
+  {
+    const int c1 = min(c0 + chunk, end);
+    for (int it = c0; it < c1; it++)
+    {
+      const int2 w = items[it];
+      if (w.x != have)
+      {
+        dev::group_sync(bar, gsz);
+        const int *src = reinterpret_cast<const int *>(&cases[w.x]);
+        int *dst = reinterpret_cast<int *>(sbc);
+        for (int k = tid; k < nwords; k += gsz) dst[k] = src[k];
+        have = w.x;
+      }
+      dev::group_sync(bar, gsz);
+      switch (sbc->N)
+      {
+#define ZB_TILE(NN)                                                                                              \
+  case NN:                                                                                                       \
+    dev::euler_tile<T, A, 2, NN>(sbc->a, *reinterpret_cast<const LineOpsT<A, NN> *>(sbc->ops), w.y, tsm, tid, gsz, \
+                                 bar);                                                                           \
+    break;
+        ZB_TILE(2) ZB_TILE(3) ZB_TILE(4) ZB_TILE(5) ZB_TILE(6)
+#undef ZB_TILE
+        default: break;
+      }
+    }
+  }
+}
+
 static size_t euler_smem_bytes(int N, size_t asz)
 {
   switch (N)
@@ -111,7 +159,7 @@ struct Batch
   cudaStream_t ost[kBatchMaxN + 1] = {nullptr};  // one stream per order, forked from and joined to `stream`
   cudaEvent_t efork = nullptr, ejoin[kBatchMaxN + 1] = {nullptr};
   int sms = 148;
-  zb_batch_config cfg{256, 4, 0, 0.0, 64, 1};
+  zb_batch_config cfg{256, 4, 0, 0.0, 64, 1, 0};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int64_t launches = 0;
@@ -223,11 +271,35 @@ static void launch_order(Batch &b, unsigned st)
   CK(cudaStreamWaitEvent(b.stream, b.ejoin[NN], 0));
 }
 
+// the whole stage in one persistent launch (cfg.fused)
+template <typename T, typename A>
+static void launch_fused(Batch &b, unsigned st)
+{
+  size_t gstride = 0;
+  for (int N = 2; N <= kBatchMaxN; N++)
+    if (b.oend[N] > b.obeg[N]) gstride = std::max(gstride, b.gstride[N]);
+  const int n = b.nitems;
+  const int ng = b.cfg.threads / b.cfg.group;
+  int chunk = b.cfg.chunk, blocks;
+  if (chunk == 0)
+  {
+    blocks = std::max(1, std::min((n + ng - 1) / ng, b.cfg.blocks_per_sm * b.sms));
+    chunk = (n + blocks * ng - 1) / (blocks * ng);
+  }
+  else
+    blocks = std::max(1, std::min((n + ng * chunk - 1) / (ng * chunk), b.cfg.blocks_per_sm * b.sms));
+  k_batch_euler_fused<T, A><<<blocks, b.cfg.threads, ng * gstride, b.stream>>>(
+      (const BatchCase<T, A> *)b.cases[st], b.items, 0, n, b.cfg.group, (int)gstride, chunk);
+  b.launches++;
+  CK(cudaGetLastError());
+}
+
 // one stage: the per-order kernels run concurrently on their own streams,
 // forked from and joined back to the batch stream (also under graph capture)
 template <typename T, typename A>
 static void launch_stage_t(Batch &b, unsigned st)
 {
+  if (b.cfg.fused) return launch_fused<T, A>(b, st);
   CK(cudaEventRecord(b.efork, b.stream));
   launch_order<T, A, 6>(b, st);
   launch_order<T, A, 5>(b, st);
@@ -294,6 +366,9 @@ static void prepare(Batch &b, unsigned first)
 template <typename T, typename A>
 static void set_batch_smem(Batch &b)
 {
+  size_t gmax = 0;
+  for (int N = 2; N <= kBatchMaxN; N++) gmax = std::max(gmax, b.gstride[N]);
+  CK(cudaFuncSetAttribute(k_batch_euler_fused<T, A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * gmax)));
   CK(cudaFuncSetAttribute(k_batch_euler<T, A, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * b.gstride[2])));
   CK(cudaFuncSetAttribute(k_batch_euler<T, A, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * b.gstride[3])));
   CK(cudaFuncSetAttribute(k_batch_euler<T, A, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * b.gstride[4])));
@@ -380,7 +455,7 @@ void batch_step(Batch *b, int nsteps, int use_graph)
     if (use_graph)
     {
       CK(cudaGraphLaunch(b->exec, b->stream));
-      b->launches += 4 * b->norders;
+      b->launches += 4 * (b->cfg.fused ? 1 : b->norders);
     }
     else
       for (unsigned st = 0; st < 4; st++) launch_stage(*b, st);
@@ -418,7 +493,8 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
   const int bps[] = {2, 4, 8, 16};
   const int orders[] = {0, 1};
   const int chunks[] = {0, 1, 8, 32};  // 0: one contiguous run per group
-  zb_batch_config best{0, 0, 0, 1e300, 0, 1};
+  zb_batch_config best{0, 0, 0, 1e300, 0, 1, 0};
+  for (int fused : {0, 1})
   for (int order : orders)
   {
     build_items(*b, order);
@@ -431,6 +507,7 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
         b->cfg.blocks_per_sm = bp;
         b->cfg.order = order;
         b->cfg.chunk = ch;
+        b->cfg.fused = fused;
         build_graph(*b);
         CK(cudaGraphLaunch(b->exec, b->stream));  // warm-up
         CK(cudaEventRecord(e0, b->stream));
@@ -440,7 +517,7 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e0, e1));
         const double per = ms / steps;
-        if (per < best.ms_per_step) best = zb_batch_config{sh[0], bp, order, per, sh[1], ch};
+        if (per < best.ms_per_step) best = zb_batch_config{sh[0], bp, order, per, sh[1], ch, fused};
       }
   }
   cudaEventDestroy(e0);
@@ -475,6 +552,7 @@ void batch_config(Batch *b, const zb_batch_config *cfg)
   if (cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 64) ZB_THROW(ZB_ERR_ARG, "blocks_per_sm out of range");
   if (cfg->order != 0 && cfg->order != 1) ZB_THROW(ZB_ERR_ARG, "order must be 0 or 1");
   if (cfg->chunk < 0) ZB_THROW(ZB_ERR_ARG, "chunk must be 0 (contiguous runs) or positive");
+  if (cfg->fused != 0 && cfg->fused != 1) ZB_THROW(ZB_ERR_ARG, "fused must be 0 or 1");
   CK(cudaStreamSynchronize(b->stream));
   b->cfg = *cfg;
   build_items(*b, cfg->order);
