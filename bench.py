@@ -417,9 +417,10 @@ def cylinder_adjoint_side(nsteps: int = 500, every: int = 50):
     adiabatic no-slip wall; objective = drag averaged over 500 RK44 steps;
     gradient with respect to 16 wall Fourier coefficients and the free-stream
     angle through the hand-written adjoint, checkpoints every 50 steps, FP64.
-    Checked against central differences (step 1e-6) of the forward run for the
-    first, the third (the largest component) and the last wall coefficient
-    and the angle."""
+    Checked against central differences (step 1e-6, and Richardson's
+    extrapolation from steps 1e-6 and 2e-6, which removes the difference's own
+    h^2 error) of the forward run for the first, the third (the largest
+    component) and the last wall coefficient and the angle."""
     from zefr_b200.shape import CylinderDrag
     prob = CylinderDrag(nr=48, nt=96, order=3, dt=1e-4, checkpoint_every=every)
     coef = np.zeros(16)
@@ -434,19 +435,26 @@ def cylinder_adjoint_side(nsteps: int = 500, every: int = 50):
     g = prob.gradient(coef, alpha, nsteps)
     t_adj = time.perf_counter() - t0
     h = 1e-6
+    gmax = max(float(np.abs(g["dJ_dcoef"]).max()), abs(g["dJ_dalpha"]))
 
-    def fd_coef(k):
+    def fd(k, step):
+        """central difference in coefficient k (k = -1: the angle)"""
+        if k < 0:
+            return (prob.drag(coef, alpha + step, nsteps) - prob.drag(coef, alpha - step, nsteps)) / (2 * step)
         cp, cm = coef.copy(), coef.copy()
-        cp[k] += h
-        cm[k] -= h
-        return (prob.drag(cp, alpha, nsteps) - prob.drag(cm, alpha, nsteps)) / (2 * h)
+        cp[k] += step
+        cm[k] -= step
+        return (prob.drag(cp, alpha, nsteps) - prob.drag(cm, alpha, nsteps)) / (2 * step)
 
-    fd = {k: fd_coef(k) for k in (0, 2, 15)}
-    fda = (prob.drag(coef, alpha + h, nsteps) - prob.drag(coef, alpha - h, nsteps)) / (2 * h)
-    checks = {f"coef{k}": {"adjoint": float(g["dJ_dcoef"][k]), "central_difference": v,
-                           "rel_err": abs(g["dJ_dcoef"][k] - v) / abs(v)} for k, v in fd.items()}
-    checks["alpha"] = {"adjoint": g["dJ_dalpha"], "central_difference": fda,
-                       "rel_err": abs(g["dJ_dalpha"] - fda) / abs(fda)}
+    checks = {}
+    for k in (0, 2, 15, -1):
+        adj = float(g["dJ_dcoef"][k]) if k >= 0 else float(g["dJ_dalpha"])
+        d1, d2 = fd(k, h), fd(k, 2 * h)
+        rich = (4.0 * d1 - d2) / 3.0  # Richardson: removes the h^2 term of the central difference
+        checks["alpha" if k < 0 else f"coef{k}"] = {
+            "adjoint": adj, "central_difference": d1, "central_difference_richardson": rich,
+            "rel_err": abs(adj - d1) / abs(d1), "rel_err_richardson": abs(adj - rich) / abs(rich),
+            "err_over_largest_gradient_component": abs(adj - d1) / gmax}
     return {"workload": "cylinder_omesh_48x96_quad9_P3_ns_drag_adjoint", "steps": nsteps,
             "checkpoint_every": every, "J_mean_drag": J,
             "dJ_dcoef": [float(x) for x in g["dJ_dcoef"]], "dJ_dalpha": g["dJ_dalpha"],
