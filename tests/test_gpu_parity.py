@@ -288,10 +288,11 @@ def test_kernels_launched():
     g = gc.load("hex_p3_ns_tgv")
     s = solver_for(g)
     s.set_state(g.U0)
-    s.step(1)  # first step after set_state also extrapolates the new state
+    s.step(1)
     n0 = s.launch_count()
     s.step(1)
-    # viscous RK44 step: two kernels per stage, extrapolation fused into the second
+    # viscous RK44 step: two kernels per stage; with one-sided LDG the gradient
+    # kernel forms the flux-point traces from the state (no trace kernel)
     assert s.launch_count() - n0 == 8
 
 

@@ -369,7 +369,13 @@ static void launch_stage_impl(Ctx &c, const StageCfg &sc)
       c.launches++;
       CK(cudaGetLastError());
     }
-    if (sc.extrap_next) c.cur ^= 1;
+    if (sc.extrap_next)
+    {
+      if (a.Fcom)
+        c.ufp_valid = false;  // the state changed and no traces were stored
+      else
+        c.cur ^= 1;
+    }
     return;
   }
   if (!c.plan.params.viscous)
@@ -651,6 +657,7 @@ Ctx *ctx_create(const Plan &plan)
       c->divF_vol = dalloc(nU * c->asz);
       c->Fvn = dalloc(nF * c->tsz);
       if (c->D == 3) c->Fcom = dalloc(nF * c->tsz);  // hexahedra: one-sided common flux
+      c->fused_traces = c->Fcom && (plan.params.ldg_b == 0.5 || plan.params.ldg_b == -0.5);
     }
     if (c->prec != ZB_FP64) c->Ucomp = dalloc(nU * c->tsz);
     c->mets = dalloc((size_t)c->ntiles * c->S * (c->D * c->D + 1) * TW * c->tsz);
@@ -864,13 +871,20 @@ static void ensure_ufp(Ctx *c)
   }
 }
 
+// traces for a residual or RK stage: none when the gradient kernel forms them
+// from the state (hexahedral Navier-Stokes with one-sided LDG)
+static void ensure_stage_ufp(Ctx *c)
+{
+  if (!c->fused_traces) ensure_ufp(c);
+}
+
 void ctx_compute_residual(Ctx *c, unsigned stage)
 {
   if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
   c->split_phase = 0;
   // extrapolate_U is step 1 of the reference residual (src/solver.cpp:1516-1518)
   c->ufp_valid = false;
-  ensure_ufp(c);
+  ensure_stage_ufp(c);
   StageCfg sc{stage, 0, 0, 0};
   c->launch_stage(*c, sc);
 }
@@ -954,13 +968,15 @@ void ctx_rk_stage(Ctx *c, unsigned stage)
   if (stage >= (unsigned)c->nstages) ZB_THROW(ZB_ERR_ARG, "stage out of range");
   if (c->ts.scheme != ZB_RK44) ZB_THROW(ZB_ERR_UNSUPPORTED, "stage-wise stepping is built for RK44");
   c->split_phase = 0;
-  ensure_ufp(c);
+  ensure_stage_ufp(c);
   c->launch_stage(*c, rk_stage_cfg(c, stage));
 }
 
 // Split residual and RK stage (compute_residual_start/mid/finish,
 // src/solver.cpp:1647-1829; step_RK_stage_start/mid/finish, 3696-3760).
-// start: the state's flux-point traces (extrapolate_U); mid: for
+// start: the state's flux-point traces (extrapolate_U; nothing for
+// hexahedral Navier-Stokes with one-sided LDG, whose gradient kernel forms
+// the traces from the state); mid: for
 // Navier-Stokes the gradient kernel (common solution, corrected gradient,
 // fluxes, volume divergence); finish: the common fluxes and surface
 // correction (the whole Euler kernel), with the RK update for a stage.
@@ -986,7 +1002,7 @@ void ctx_residual_split(Ctx *c, unsigned stage, int part, int rk)
   if (part == 0)
   {
     if (!rk) c->ufp_valid = false;
-    ensure_ufp(c);
+    ensure_stage_ufp(c);
     c->split_stage = stage;
     c->split_rk = rk ? 1 : 0;
     c->split_phase = 1;
@@ -1188,7 +1204,9 @@ static void vjp_tiles(Ctx *c, bool params, double *param_bar, bool geo, bool acc
     if (c->plan.params.viscous && !fvn_ready)
     {
       StageCfg sc{0, 0, 0, 0};
+      c->need_fvn = true;
       c->launch_stage(*c, sc);
+      c->need_fvn = false;
     }
   }
   c->launch_vjp(*c, params || param_bar, geo);
@@ -1356,7 +1374,9 @@ void ctx_rk_step_vjp(Ctx *c, const double *U0, const double *Ubar1, double *Ubar
     c->ufp_valid = false;
     ensure_ufp(c);
     StageCfg sc{0, 0, 0, 0};
+    c->need_fvn = keep_fvn;
     c->launch_stage(*c, sc);
+    c->need_fvn = false;
     CK(cudaMemcpyAsync(Rs[s], c->divF[0], (size_t)nU * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     if (keep_fvn)
       CK(cudaMemcpyAsync(c->rkfvn + s * nF, c->Fvn, nF * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));

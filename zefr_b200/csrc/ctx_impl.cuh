@@ -61,6 +61,8 @@ struct Ctx
   double *dred = nullptr;
   int cur = 0;
   bool ufp_valid = false;
+  bool need_fvn = false;  // the next stage launch must store the viscous normal flux
+  bool fused_traces = false;  // hexahedral NS with one-sided LDG: residuals read no trace buffer
   // split residual (zb_compute_residual_start/mid/finish, zb_rk_stage_*):
   // phase 0 idle, 1 after start, 2 after mid; the stage and kind being split
   int split_phase = 0;
@@ -245,11 +247,15 @@ static Args<T, A> make_args(Ctx &c, const StageCfg &sc)
   a.nbr = c.nbr;
   a.divF = (T *)c.divF[sc.stage];
   a.divF_vol = (A *)c.divF_vol;
-  a.Fvn = (T *)c.Fvn;
   if (c.Fcom && (c.plan.params.ldg_b == 0.5 || c.plan.params.ldg_b == -0.5)) a.Fcom = (T *)c.Fcom;
+  // with the one-sided common flux the face kernel does not read the viscous
+  // normal flux; only the geometry adjoint does (need_fvn)
+  a.Fvn = (a.Fcom && !c.need_fvn) ? nullptr : (T *)c.Fvn;
   a.rk_mode = sc.rk_mode;
   a.save_ini = sc.save_ini;
-  a.extrap_next = sc.extrap_next;
+  // the one-sided form keeps no trace buffer: the gradient kernel forms the
+  // traces from the state, so the next stage's extrapolation is not stored
+  a.extrap_next = a.Fcom ? 0 : sc.extrap_next;
   a.Uout = (T *)c.U;
   a.U_ini = (T *)c.U_ini;
   a.Ucomp = nullptr;

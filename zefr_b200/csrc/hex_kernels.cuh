@@ -391,6 +391,61 @@ __device__ __forceinline__ void hex_extrap_next(const Args<T, A> &a, int64_t til
   }
 }
 
+// Trace of the state at the flux point with tile-layout index pidx
+// ((tile * Fp + f) * TW + lane, the partner index of a connectivity code),
+// formed from that element's state along the line normal to its face with
+// the extrapolation's arithmetic (k_hex_extrap), so the same values.
+template <typename T, typename A, int N>
+__device__ __forceinline__ void hex_partner_trace(const T *__restrict__ U, const LineOpsT<A, N> &ops, int pidx,
+                                                  A out[5])
+{
+  using H = HexIdx<N>;
+  constexpr int V = 5;
+  const int lane = pidx % TW, pt = pidx / TW;
+  const int64_t ptile = pt / H::Fp;
+  const int f = pt % H::Fp, q = f / H::N2, r = f % H::N2;
+  // invert H::fpt: the (ix, iy) of the column that owns flux point f on face q
+  int ix, iy;
+  switch (q)
+  {
+    case 0: ix = r % N; iy = r / N; break;
+    case 1: ix = N - 1 - r % N; iy = r / N; break;
+    case 2: ix = r / N; iy = r % N; break;
+    case 3: ix = r / N; iy = N - 1 - r % N; break;
+    case 4: ix = N - 1 - r % N; iy = r / N; break;
+    default: ix = r % N; iy = r / N; break;
+  }
+  const T *Up = U + ptile * (int64_t)H::S * V * TW + lane;
+  const bool minus = q_minus(q);
+#pragma unroll
+  for (int v = 0; v < V; v++)
+  {
+    A acc = (minus ? ops.Em[0] : ops.Ep[0]) * Up[(H::line_spt(q, ix, iy, 0) * V + v) * TW];
+#pragma unroll
+    for (int m = 1; m < N; m++) acc += (minus ? ops.Em[m] : ops.Ep[m]) * Up[(H::line_spt(q, ix, iy, m) * V + v) * TW];
+    out[v] = acc;
+  }
+}
+
+// Own trace at own flux point q of column (ix, iy) from the state tile in
+// shared memory ([S][V][TW]), with the extrapolation's arithmetic
+template <typename A, int N>
+__device__ __forceinline__ void hex_own_trace(const LineOpsT<A, N> &ops, const A *sU, int q, int ix, int iy, int l,
+                                              A out[5])
+{
+  using H = HexIdx<N>;
+  constexpr int V = 5;
+#pragma unroll
+  for (int v = 0; v < V; v++)
+  {
+    A acc = (q_minus(q) ? ops.Em[0] : ops.Ep[0]) * sU[(H::line_spt(q, ix, iy, 0) * V + v) * TW + l];
+#pragma unroll
+    for (int m = 1; m < N; m++)
+      acc += (q_minus(q) ? ops.Em[m] : ops.Ep[m]) * sU[(H::line_spt(q, ix, iy, m) * V + v) * TW + l];
+    out[v] = acc;
+  }
+}
+
 template <typename T, typename A>
 __device__ __forceinline__ void load_adj(const Args<T, A> &a, int64_t tile, int S, int s, int l, A adj[3][3], A &det)
 {
@@ -528,57 +583,118 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
         sU[(s * V + v) * TW + l] = Ut[(s * V + v) * TW + l];
       }
   }
-  // common solution at own flux points (LDG, flip_beta = 1); unrolled so the
-  // partner gathers of all points are in flight together
-#pragma unroll
-  for (int kq = 0; kq < 6 / ZS; kq++)
+  // common solution at own flux points (LDG, flip_beta = 1).  The points'
+  // connectivity codes stay in registers for the viscous pass.
+  int codes[6 / ZS];
+  if (a.Fcom)
   {
-    const int q = own_face<ZS>(zs, kq);
-    const int fq = H::fpt(q, ix, iy);
-    A n[3], dA;
-    int code;
-    load_face_geo<T, A, N>(a, tile, fq, l, n, dA, code);
-    A Uo[V], UC[V];
-    const T *uo = a.Ufp + (tile * Fp + fq) * (int64_t)V * TW + l;
+    // One-sided LDG (beta = +-1/2): no trace buffer.  The side that takes the
+    // partner's trace forms it from the partner's state line (all such
+    // gathers in flight together, before the barrier that completes the
+    // state tile); the other side and boundary points use the own trace,
+    // formed from the state tile afterwards.
+    const int supplier = beta == A(0.5) ? 0 : 1;
+    A Un[6 / ZS][V];
 #pragma unroll
-    for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
-    if (code >= 0)
+    for (int kq = 0; kq < 6 / ZS; kq++)
     {
-      const int slot = code & 1;
-      if ((beta == A(0.5) && slot) || (beta == A(-0.5) && !slot))
-      {
-        // beta = +1/2 (-1/2) takes the right (left) trace: this side's own,
-        // no partner gather
+      const int fq = H::fpt(own_face<ZS>(zs, kq), ix, iy);
+      const int code = a.nbr[(tile * Fp + fq) * (int64_t)TW + l];
+      codes[kq] = code;
+      if (code >= 0 && (code & 1) == supplier) hex_partner_trace<T, A, N>(a.U, ops, code >> 1, Un[kq]);
+    }
+    __syncthreads();
 #pragma unroll
-        for (int v = 0; v < V; v++) UC[v] = Uo[v];
+    for (int kq = 0; kq < 6 / ZS; kq++)
+    {
+      const int q = own_face<ZS>(zs, kq);
+      const int fq = H::fpt(q, ix, iy);
+      const int code = codes[kq];
+      A UC[V];
+      if (code >= 0 && (code & 1) == supplier)
+      {
+#pragma unroll
+        for (int v = 0; v < V; v++) UC[v] = Un[kq][v];
       }
       else
       {
-        A Un[V];
-        gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
-#pragma unroll
-        for (int v = 0; v < V; v++)
+        A Uo[V];
+        hex_own_trace<A, N>(ops, sU, q, ix, iy, l, Uo);
+        if (code >= 0)
         {
-          const A ul = slot ? Un[v] : Uo[v];
-          const A ur = slot ? Uo[v] : Un[v];
-          if (beta == A(0.5))
-            UC[v] = ur;
-          else if (beta == A(-0.5))
-            UC[v] = ul;
-          else
-            UC[v] = A(0.5) * (ul + ur) - beta * (ul - ur);
+#pragma unroll
+          for (int v = 0; v < V; v++) UC[v] = Uo[v];
+        }
+        else
+        {
+          A n[3], dA;
+          int c2;
+          load_face_geo<T, A, N>(a, tile, fq, l, n, dA, c2);
+          A Ua[V], URa[V], UBa[V];
+          to_abs<A, 3>(Uo, Ua, a.ph);
+          ghost_state<A, 3>(-code - 1, Ua, n, URa, UBa, a.ph);
+          to_stored<A, 3>(UBa, UC, a.ph);
         }
       }
-    }
-    else
-    {
-      A Ua[V], URa[V], UBa[V];
-      to_abs<A, 3>(Uo, Ua, a.ph);
-      ghost_state<A, 3>(-code - 1, Ua, n, URa, UBa, a.ph);
-      to_stored<A, 3>(UBa, UC, a.ph);
-    }
 #pragma unroll
-    for (int v = 0; v < V; v++) sUC[(fq * V + v) * TW + l] = UC[v];
+      for (int v = 0; v < V; v++) sUC[(fq * V + v) * TW + l] = UC[v];
+    }
+  }
+  else
+  {
+    // traces from the trace buffer; unrolled so the partner gathers of all
+    // points are in flight together
+#pragma unroll
+    for (int kq = 0; kq < 6 / ZS; kq++)
+    {
+      const int q = own_face<ZS>(zs, kq);
+      const int fq = H::fpt(q, ix, iy);
+      A n[3], dA;
+      int code;
+      load_face_geo<T, A, N>(a, tile, fq, l, n, dA, code);
+      codes[kq] = code;
+      A Uo[V], UC[V];
+      const T *uo = a.Ufp + (tile * Fp + fq) * (int64_t)V * TW + l;
+#pragma unroll
+      for (int v = 0; v < V; v++) Uo[v] = uo[v * TW];
+      if (code >= 0)
+      {
+        const int slot = code & 1;
+        if ((beta == A(0.5) && slot) || (beta == A(-0.5) && !slot))
+        {
+          // beta = +1/2 (-1/2) takes the right (left) trace: this side's own,
+          // no partner gather
+#pragma unroll
+          for (int v = 0; v < V; v++) UC[v] = Uo[v];
+        }
+        else
+        {
+          A Un[V];
+          gather_fpt<T, A, V>(a.Ufp, code >> 1, Un);
+#pragma unroll
+          for (int v = 0; v < V; v++)
+          {
+            const A ul = slot ? Un[v] : Uo[v];
+            const A ur = slot ? Uo[v] : Un[v];
+            if (beta == A(0.5))
+              UC[v] = ur;
+            else if (beta == A(-0.5))
+              UC[v] = ul;
+            else
+              UC[v] = A(0.5) * (ul + ur) - beta * (ul - ur);
+          }
+        }
+      }
+      else
+      {
+        A Ua[V], URa[V], UBa[V];
+        to_abs<A, 3>(Uo, Ua, a.ph);
+        ghost_state<A, 3>(-code - 1, Ua, n, URa, UBa, a.ph);
+        to_stored<A, 3>(UBa, UC, a.ph);
+      }
+#pragma unroll
+      for (int v = 0; v < V; v++) sUC[(fq * V + v) * TW + l] = UC[v];
+    }
   }
   __syncthreads();
   // corrected reference gradient -> physical gradient
@@ -631,22 +747,30 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
     }
   }
   __syncthreads();
-  // viscous normal flux at own flux points
+  // viscous normal flux at own flux points: the points where the partner
+  // supplies the LDG normal flux are skipped without a memory access; the own
+  // trace is formed from the state in shared memory
 #pragma unroll 1
   for (int kq = 0; kq < 6 / ZS; kq++)
   {
+    int code = codes[0];
+#pragma unroll
+    for (int j = 1; j < 6 / ZS; j++) code = kq == j ? codes[j] : code;  // register select
+    if (code >= 0 && ((beta == A(0.5) && (code & 1)) || (beta == A(-0.5) && !(code & 1)))) continue;
     const int q = own_face<ZS>(zs, kq);
     const int fq = H::fpt(q, ix, iy);
-    A n[3], dA;
-    int code;
-    load_face_geo<T, A, N>(a, tile, fq, l, n, dA, code);
-    if (code >= 0 && ((beta == A(0.5) && (code & 1)) || (beta == A(-0.5) && !(code & 1)))) continue;
+    A n[3];
+    {
+      const T *gq = a.fgeo + (tile * Fp + fq) * (int64_t)4 * TW + l;
+      n[0] = gq[0];
+      n[1] = gq[TW];
+      n[2] = gq[2 * TW];
+    }
     A Uf[V], dUf[V][3], Fn[V];
-    const T *uo = a.Ufp + (tile * Fp + fq) * (int64_t)V * TW + l;
+    hex_own_trace<A, N>(ops, sU, q, ix, iy, l, Uf);
 #pragma unroll
     for (int v = 0; v < V; v++)
     {
-      Uf[v] = uo[v * TW];
 #pragma unroll
       for (int d = 0; d < 3; d++)
       {
@@ -668,9 +792,12 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
       ghost_grad<A, 3>(-code - 1, Ua, dUf, n, dUB);
       visc_normal<A, 3>(UB, dUB, n, Fn, a.ph);
     }
-    T *out = a.Fvn + (tile * Fp + fq) * (int64_t)V * TW + l;
+    if (a.Fvn)
+    {
+      T *out = a.Fvn + (tile * Fp + fq) * (int64_t)V * TW + l;
 #pragma unroll
-    for (int v = 0; v < V; v++) out[v * TW] = Fn[v];
+      for (int v = 0; v < V; v++) out[v * TW] = Fn[v];
+    }
     if (a.Fcom)
     {
       // this side supplies the LDG normal flux, so it forms the whole common

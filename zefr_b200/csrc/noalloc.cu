@@ -228,9 +228,13 @@ void run_kernels(const Plan &p, unsigned char *base, const Regions &r, cudaStrea
   {
     // hexahedra: column-mapped kernels, TW x N^2 threads per tile (ZS per column)
     constexpr int HT = TW * N * N;
-    dev::k_hex_extrap<double, double, N><<<(unsigned)p.ntiles, HT, 0, st>>>(
-        a.U, reinterpret_cast<double *>(base + r.Ufp), p.ntiles, ops);
-    NA_CK(cudaGetLastError());
+    // with the one-sided common flux the gradient kernel forms the traces
+    if (!a.Fcom)
+    {
+      dev::k_hex_extrap<double, double, N><<<(unsigned)p.ntiles, HT, 0, st>>>(
+          a.U, reinterpret_cast<double *>(base + r.Ufp), p.ntiles, ops);
+      NA_CK(cudaGetLastError());
+    }
     if (!p.params.viscous)
     {
       const size_t smem = (size_t)(S * V + 3 * S * V + Fp * V) * TW * sizeof(double);
