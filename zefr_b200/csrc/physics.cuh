@@ -34,6 +34,9 @@ struct Phys
 // Arithmetic of the perturbation form: FP32 stores deviations from Ur.
 template <typename T> struct Pert { static constexpr bool on = false; };
 template <> struct Pert<float> { static constexpr bool on = true; };
+// plain FP64 arithmetic (not the perturbation form, not dual numbers)
+template <typename T> struct IsF64 { static constexpr bool on = false; };
+template <> struct IsF64<double> { static constexpr bool on = true; };
 
 template <typename T> ZB_HD T dsqrt(T x);
 template <> ZB_HD double dsqrt<double>(double x) { return sqrt(x); }
@@ -41,6 +44,17 @@ template <> ZB_HD float dsqrt<float>(float x) { return sqrtf(x); }
 template <typename T> ZB_HD T dpow(T x, T y);
 template <> ZB_HD double dpow<double>(double x, double y) { return pow(x, y); }
 template <> ZB_HD float dpow<float>(float x, float y) { return powf(x, y); }
+// reciprocal square root: CUDA's rsqrt on the device (max 1 ulp error), the
+// quotient on the host
+template <typename T> ZB_HD T drsqrt(T x);
+template <> ZB_HD double drsqrt<double>(double x)
+{
+#ifdef __CUDA_ARCH__
+  return rsqrt(x);
+#else
+  return 1.0 / sqrt(x);
+#endif
+}
 template <typename T> ZB_HD T dabs(T x) { return x < T(0) ? -x : x; }
 template <typename T> ZB_HD T dmax(T a, T b) { return a > b ? a : b; }
 
@@ -175,14 +189,14 @@ ZB_HD void flux_visc_add(const T U[D + 2], const T dU[D + 2][D], T F[D + 2][D],
   T div = dvel[0][0];
 #pragma unroll
   for (int d = 1; d < D; d++) div += dvel[d][d];
-  const T diag = div / T(3);
+  const T diag = div * (T(1) / T(3));
   T tau[D][D];
 #pragma unroll
   for (int i = 0; i < D; i++)
 #pragma unroll
     for (int j = 0; j < D; j++)
       tau[i][j] = (i == j) ? T(2) * mu * (dvel[i][i] - diag) : mu * (dvel[i][j] + dvel[j][i]);
-  const T kappa = (mu / ph.prandtl) * ph.gamma;
+  const T kappa = mu * (ph.gamma / ph.prandtl);  // gamma / Pr is loop-invariant
 #pragma unroll
   for (int j = 0; j < D; j++)
   {
@@ -261,9 +275,17 @@ ZB_HD void rusanov(const T UL[D + 2], const T UR[D + 2], const T n[D], T Fc[D + 
 // |l| below delta = 0.1 * (|u_n| + a) of the Roe state is replaced by
 // (l^2 + delta^2) / (2 delta).  No reference counterpart.
 template <typename T, int D>
+ZB_HD void roe_plain(const T SL[D + 2], const T SR[D + 2], const T n[D], T Fc[D + 2], const Phys<T> &ph);
+
+template <typename T, int D>
 ZB_HD void roe(const T SL[D + 2], const T SR[D + 2], const T n[D], T Fc[D + 2],
                                     const Phys<T> &ph)
 {
+  if constexpr (IsF64<T>::on)
+  {
+    roe_plain<T, D>(SL, SR, n, Fc, ph);
+    return;
+  }
   const T g = ph.gamma;
   T FL[D + 2][D], FR[D + 2][D], PL, PR, QL, QR;
   flux_conv_stored<T, D>(SL, FL, PL, QL, ph);
@@ -336,6 +358,80 @@ ZB_HD void roe(const T SL[D + 2], const T SR[D + 2], const T n[D], T Fc[D + 2],
     }
     Fc[v] = T(0.5) * (fl + fr) - T(0.5) * diss[v];
   }
+}
+
+// The same Roe flux in FP64 arithmetic on absolute states: the normal fluxes
+// F(U).n = [m.n, m u.n + p n, (E + p) u.n] directly, and 1/rho, sqrt(rho),
+// the sound speed and 1/a^2 from reciprocal square roots (three rsqrt and
+// two divisions per face in place of three square roots and seven
+// divisions); equal to the form above to a few ulp.
+template <typename T, int D>
+ZB_HD void roe_plain(const T SL[D + 2], const T SR[D + 2], const T n[D], T Fc[D + 2], const Phys<T> &ph)
+{
+  const T g = ph.gamma;
+  T UL[D + 2], UR[D + 2];
+  to_abs<T, D>(SL, UL, ph);
+  to_abs<T, D>(SR, UR, ph);
+  const T rL = UL[0], rR = UR[0];
+  const T rsL = drsqrt<T>(rL), rsR = drsqrt<T>(rR);
+  const T sL = rL * rsL, sR = rR * rsR;      // sqrt(rho)
+  const T irL = rsL * rsL, irR = rsR * rsR;  // 1 / rho
+  const T inv = T(1) / (sL + sR);
+  T u[D], uL[D], uR[D];
+  T unL = T(0), unR = T(0), kL = T(0), kR = T(0);
+#pragma unroll
+  for (int d = 0; d < D; d++)
+  {
+    uL[d] = UL[d + 1] * irL;
+    uR[d] = UR[d + 1] * irR;
+    u[d] = (sL * uL[d] + sR * uR[d]) * inv;
+    unL += uL[d] * n[d];
+    unR += uR[d] * n[d];
+    kL += UL[d + 1] * uL[d];  // |m|^2 / rho
+    kR += UR[d + 1] * uR[d];
+  }
+  const T PL = (g - T(1)) * (UL[D + 1] - T(0.5) * kL), PR = (g - T(1)) * (UR[D + 1] - T(0.5) * kR);
+  const T HL = (UL[D + 1] + PL) * irL, HR = (UR[D + 1] + PR) * irR;
+  const T H = (sL * HL + sR * HR) * inv;
+  T q2 = T(0), un = T(0);
+#pragma unroll
+  for (int d = 0; d < D; d++)
+  {
+    q2 += u[d] * u[d];
+    un += u[d] * n[d];
+  }
+  T a2 = (g - T(1)) * (H - T(0.5) * q2);
+  a2 = dmax<T>(a2, T(1e-30));
+  const T ra = drsqrt<T>(a2);
+  const T a = a2 * ra, ia2 = ra * ra;
+  const T rho = sL * sR;
+  const T dp = PR - PL, dr = UR[0] - UL[0], dun = unR - unL;
+  const T a1 = (dp - rho * a * dun) * (T(0.5) * ia2);
+  const T a3 = (dp + rho * a * dun) * (T(0.5) * ia2);
+  const T a2w = dr - dp * ia2;
+  T l1 = dabs<T>(un - a), l2 = dabs<T>(un), l3 = dabs<T>(un + a);
+  const T delta = T(0.1) * (dabs<T>(un) + a);
+  const T i2d = T(0.5) / delta;
+  if (l1 < delta) l1 = (l1 * l1 + delta * delta) * i2d;
+  if (l2 < delta) l2 = (l2 * l2 + delta * delta) * i2d;
+  if (l3 < delta) l3 = (l3 * l3 + delta * delta) * i2d;
+  T diss[D + 2];
+  diss[0] = l1 * a1 + l2 * a2w + l3 * a3;
+  T udvt = T(0);
+#pragma unroll
+  for (int d = 0; d < D; d++)
+  {
+    const T dvt = (uR[d] - uL[d]) - dun * n[d];
+    diss[d + 1] = l1 * a1 * (u[d] - a * n[d]) + l2 * (a2w * u[d] + rho * dvt) + l3 * a3 * (u[d] + a * n[d]);
+    udvt += u[d] * dvt;
+  }
+  diss[D + 1] = l1 * a1 * (H - a * un) + l2 * (a2w * T(0.5) * q2 + rho * udvt) + l3 * a3 * (H + a * un);
+  const T mnL = rL * unL, mnR = rR * unR;
+  Fc[0] = T(0.5) * (mnL + mnR) - T(0.5) * diss[0];
+#pragma unroll
+  for (int d = 0; d < D; d++)
+    Fc[d + 1] = T(0.5) * ((UL[d + 1] * unL + PL * n[d]) + (UR[d + 1] * unR + PR * n[d])) - T(0.5) * diss[d + 1];
+  Fc[D + 1] = T(0.5) * (mnL * HL + mnR * HR) - T(0.5) * diss[D + 1];
 }
 
 // Boundary ghost states (src/faces.cpp:123-506, explicit time stepping so
