@@ -50,13 +50,13 @@ TGV_DECK = dict(ndims=3, order=ORDER, viscous=1, disable_nondim=1, fix_vis=1, ma
                 prandtl=0.71, P_fs=1.0, rho_fs=1.0, L_fs=1.0, ldg_b=0.5, ldg_tau=0.1, dt=5e-4, gamma=1.4)
 
 
-# DRAM bytes per element of one mixed-form residual (extrapolation, gradient and
-# face kernels), read + write, from an ncu capture at 48^3 hexes (state 141 MB,
-# above L2): 304 + 1232 + 588 MB over 110,592 elements.
-MIXED_DRAM_BYTES_PER_ELEMENT = 19210.0
-# the same for the FP64 form (k_hex_extrap + k_hex_ns_grad + k_hex_ns_face,
-# FP64, 48^3 hexes, state 283 MB): 748 + 2432 + 979 MB over 110,592 elements
-FP64_DRAM_BYTES_PER_ELEMENT = 37607.0
+# DRAM bytes per element of one mixed-form residual (gradient and face
+# kernels), read + write, from an ncu capture at 48^3 hexes (state 141 MB,
+# above L2): 884.7 + 584.6 MB over 110,592 elements.
+MIXED_DRAM_BYTES_PER_ELEMENT = 13286.0
+# the same for the FP64 form (k_hex_ns_grad + k_hex_ns_face, FP64, 48^3
+# hexes, state 283 MB): 1733.5 + 978.8 MB over 110,592 elements
+FP64_DRAM_BYTES_PER_ELEMENT = 24525.0
 
 
 def b_alg(E: int, S: int, V: int, D: int, G: int, Fp: int, w: int) -> float:

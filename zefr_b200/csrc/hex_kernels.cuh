@@ -81,6 +81,13 @@ struct RowOps
   }
 };
 
+// Prefetch `bytes` (a multiple of 16, 16-byte aligned) from global memory
+// into L2 without waiting: one bulk request, no registers held
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes)
+{
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // own flux point q (0..5): side of the face
 __device__ __forceinline__ bool q_minus(int q) { return (q & 1) == 0; }
 
@@ -566,6 +573,20 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
   const int ix = c % N, iy = c / N, iz0 = zs * NZ;
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
+  // the tile's metrics (gradient and flux passes) and face geometry (viscous
+  // pass) on their way to L2 while the state and partner traces load; the
+  // state and codes of the tile one wave of resident CTAs ahead (2 per SM)
+  if (threadIdx.x == 0)
+  {
+    prefetch_l2(a.mets + tile * (int64_t)S * 10 * TW, S * 10 * TW * sizeof(T));
+    prefetch_l2(a.fgeo + tile * (int64_t)Fp * 4 * TW, Fp * 4 * TW * sizeof(T));
+    const int64_t ahead = tile + 2 * 148;
+    if (ahead < a.ntiles)
+    {
+      prefetch_l2(a.U + ahead * (int64_t)S * V * TW, S * V * TW * sizeof(T));
+      prefetch_l2(a.nbr + ahead * (int64_t)Fp * TW, Fp * TW * sizeof(int));
+    }
+  }
   RowOps<A, N> o;
   o.load(ops, ix, iy);
   int f[6];
