@@ -101,6 +101,32 @@ def test_residual_matches_oracle_larger(case):
     assert gc.rel_err(R, Ro) < TOL_FP64
 
 
+@pytest.mark.parametrize("fconv", ["rusanov", "roe"])
+@pytest.mark.parametrize("ldg_b", [0.5, -0.5, 0.25])
+@pytest.mark.parametrize("bc", ["wall_ns_adi", "wall_ns_iso", "char"])
+def test_hex_ns_boundaries_and_ldg_beta(bc, ldg_b, fconv):
+    """Hexahedral Navier-Stokes on a jittered box whose six sides are one
+    boundary, against the oracle.  beta = +-1/2 takes the one-sided path (the
+    gradient kernel forms the traces from the state, with the supplying side
+    on the left or the right); beta = 1/4 takes the path through the trace
+    buffer.  Both pass boundary flux points through the ghost states."""
+    mesh = meshgen.jitter_interior(meshgen.box_hexes(4, 3, 3, bnd="WALL"), 0.12, 11)
+    order, visc, bounds = 3, True, {"WALL": bc}
+    p = _ref_params(True, mu=2e-3, ldg_b=ldg_b, ldg_tau=0.3, V_fs=(0.2, 0.05, -0.03))
+    params = make_params(order, visc, mu=p["mu"], ldg_b=p["ldg_b"], ldg_tau=p["ldg_tau"], prandtl=p["prandtl"],
+                         V_fs=(p["V_fs0"], p["V_fs1"], p["V_fs2"]), rho_fs=1.0, P_fs=1.0, T_wall=1.0, R_ref=1.0,
+                         fconv=fconv)
+    s = FRSolver(mesh, params, bounds)
+    X = s.plan.get("coord_spts").reshape(s.nspts, mesh.ndims, s.neles)
+    U = ics.perturb(ics.taylor_green(X, mach=0.1), 1e-2, seed=3)
+    plan = Plan(mesh, make_params(order, visc), bounds)
+    st = dfr_numpy.Setup.from_arrays(mesh.ndims, s.nspts, plan.info.nfpts, s.neles, plan.get)
+    Ro = dfr_numpy.residual(st, U, p, visc, fconv=fconv)
+    for stage in (0, 2):
+        assert gc.rel_err(s.residual(U, stage), Ro) < TOL_FP64
+    s.close()
+
+
 @pytest.mark.parametrize("name", ["quad_p3_euler_vortex", "hex_p3_ns_tgv", "cyl_p3_ns_char_adi", "quad_p2_ns_jitter",
                                   "hex_p2_euler_jitter", "cyl_p2_ns_iso_farfield_b03", "tri_p4_ns_jitter",
                                   "tri_p3_euler_char"])
