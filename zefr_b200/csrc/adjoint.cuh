@@ -281,8 +281,10 @@ ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double 
   const double g = ph.gamma;
   // ---- forward recomputation ----
   const double rL = UL[0], rR = UR[0];
-  // reciprocals formed once: the FP64 division is a multi-instruction sequence
-  const double irL = 1.0 / rL, irR = 1.0 / rR;
+  // 1/rho and sqrt(rho) from one reciprocal square root per state (the FP64
+  // division and square root are multi-instruction sequences)
+  const double rsL = drsqrt<double>(rL), rsR = drsqrt<double>(rR);
+  const double irL = rsL * rsL, irR = rsR * rsR;
   double m2L = 0.0, m2R = 0.0;
   for (int d = 0; d < D; d++)
   {
@@ -291,7 +293,7 @@ ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double 
   }
   const double PL = (g - 1.0) * (UL[V - 1] - 0.5 * m2L * irL);
   const double PR = (g - 1.0) * (UR[V - 1] - 0.5 * m2R * irR);
-  const double sL = sqrt(rL), sR = sqrt(rR);
+  const double sL = rL * rsL, sR = rR * rsR;
   const double inv = 1.0 / (sL + sR);
   double uL[D], uR[D], u[D], unL = 0.0, unR = 0.0;
   for (int d = 0; d < D; d++)
@@ -313,8 +315,8 @@ ZB_HD void roe_vjp(const double UL[D + 2], const double UR[D + 2], const double 
   double c2 = (g - 1.0) * (H - 0.5 * q2);
   const bool clamped = !(c2 > 1e-30);
   if (clamped) c2 = 1e-30;
-  const double a = sqrt(c2);
-  const double ic2 = 1.0 / c2, ia = 1.0 / a;
+  const double ia = drsqrt<double>(c2);
+  const double a = c2 * ia, ic2 = ia * ia;
   const double rho = sL * sR;
   const double dp = PR - PL, dr = rR - rL, dun = unR - unL;
   const double t2 = 0.5 * ic2;
@@ -1184,15 +1186,35 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
   double *sFace = sdU + D * S * V * TW;
   const int64_t tile = blockIdx.x;
   if (tile >= a.ntiles) return;
+  // this tile's metrics (gradient, volume and gradient-adjoint passes) and
+  // the inputs of the tile one wave of resident CTAs (one per SM) ahead on
+  // their way to L2
+  if (threadIdx.x == 0)
+  {
+    prefetch_l2(a.mets + tile * (int64_t)S * NM * TW, S * NM * TW * sizeof(double));
+    const int64_t ahead = tile + 148;
+    if (ahead < a.ntiles)
+    {
+      prefetch_l2(a.Ufp + ahead * (int64_t)Fp * V * TW, Fp * V * TW * sizeof(double));
+      prefetch_l2(a.Lfp + ahead * (int64_t)Fp * V * TW, Fp * V * TW * sizeof(double));
+      prefetch_l2(a.fgeo + ahead * (int64_t)Fp * (D + 1) * TW, Fp * (D + 1) * TW * sizeof(double));
+      prefetch_l2(a.nbr + ahead * (int64_t)Fp * TW, Fp * TW * sizeof(int));
+      prefetch_l2(a.U + ahead * (int64_t)S * V * TW, S * V * TW * sizeof(double));
+    }
+  }
   const double beta = a.ph.ldg_b, tau = a.ph.ldg_tau;
   double pb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   {
     const double *src = a.U + tile * (int64_t)S * V * TW;
     for (int i = threadIdx.x; i < S * V * TW; i += blockDim.x) sU[i] = src[i];
   }
-  // common solution (as k_ns_grad)
-  for (int it = threadIdx.x; it < Fp * TW; it += blockDim.x)
+  // common solution (as k_ns_grad); unrolled over a thread's items so their
+  // gathers are in flight together
+#pragma unroll
+  for (int k = 0; k < (Fp * TW + G::NT - 1) / G::NT; k++)
   {
+    const int it = (int)threadIdx.x + k * G::NT;
+    if (it >= Fp * TW) break;
     const int f = it / TW, l = it % TW;
     const int code = a.nbr[(tile * Fp + f) * (int64_t)TW + l];
     double Uo[V], UC[V];
@@ -1249,8 +1271,11 @@ __global__ void __launch_bounds__(Shape<D, N>::NT) k_adj_ns1(const __grid_consta
   }
   __syncthreads();
   // physical gradient (as k_ns_grad)
-  for (int it = threadIdx.x; it < S * TW; it += blockDim.x)
+#pragma unroll
+  for (int k = 0; k < (S * TW + G::NT - 1) / G::NT; k++)
   {
+    const int it = (int)threadIdx.x + k * G::NT;
+    if (it >= S * TW) break;
     const int s = it / TW, l = it % TW;
     double tdU[V][D];
 #pragma unroll

@@ -35,6 +35,13 @@ struct Shape
   static constexpr int NT = (D == 2) ? ((S * TW <= 128) ? 128 : 256) : 256;
 };
 
+// Prefetch `bytes` (a multiple of 16, 16-byte aligned) from global memory
+// into L2 without waiting: one bulk request, no registers held
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes)
+{
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 template <typename T, int N>
 struct LineOpsT
 {

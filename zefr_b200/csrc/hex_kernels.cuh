@@ -81,13 +81,6 @@ struct RowOps
   }
 };
 
-// Prefetch `bytes` (a multiple of 16, 16-byte aligned) from global memory
-// into L2 without waiting: one bulk request, no registers held
-__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes)
-{
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
 // own flux point q (0..5): side of the face
 __device__ __forceinline__ bool q_minus(int q) { return (q & 1) == 0; }
 
