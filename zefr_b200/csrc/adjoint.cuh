@@ -20,9 +20,12 @@
 #include "dfr_kernels.cuh"
 #include "dual.cuh"
 
-// Boundary-face functions run on few flux points and hold many dual numbers:
-// out of line, so their registers do not weigh on the interior path.
+// Boundary-face functions run on few flux points and hold many dual numbers.
+// In 3D they are called out of line, so their registers do not weigh on the
+// interior path; in 2D they are inlined (their frames are small, and a call
+// from the register-bound 2D kernels costs more than the registers).
 #define ZB_HD_COLD __host__ __device__ __noinline__
+#define ZB_HD_INLINE __host__ __device__ __forceinline__
 
 namespace zb {
 namespace dev {
@@ -533,7 +536,7 @@ ZB_HD void visc_normal_vjp(const double U[D + 2], const double dU[D + 2][D], con
 //   convective common flux with the ghost state, plus for viscous runs
 //   F_visc(UB, ghost_grad(U, dU)) . n + tau (U - UB).
 template <int D, bool VISC>
-ZB_HD_COLD void bnd_face_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+ZB_HD_INLINE void bnd_face_vjp_body(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
                         const double w[D + 2], const Phys<Dual<double>> &pd, double Ub[D + 2], double dUb[D + 2][D])
 {
   constexpr int V = D + 2;
@@ -566,11 +569,26 @@ ZB_HD_COLD void bnd_face_vjp(int bc, const double U[D + 2], const double dU[D + 
       dUb[(k - V) / D][(k - V) % D] += acc;
   }
 }
+template <int D, bool VISC>
+ZB_HD_COLD void bnd_face_vjp_cold(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+                        const double w[D + 2], const Phys<Dual<double>> &pd, double Ub[D + 2], double dUb[D + 2][D])
+{
+  bnd_face_vjp_body<D, VISC>(bc, U, dU, n, w, pd, Ub, dUb);
+}
+template <int D, bool VISC>
+ZB_HD_INLINE void bnd_face_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+                        const double w[D + 2], const Phys<Dual<double>> &pd, double Ub[D + 2], double dUb[D + 2][D])
+{
+  if constexpr (D == 2)
+    bnd_face_vjp_body<D, VISC>(bc, U, dU, n, w, pd, Ub, dUb);
+  else
+    bnd_face_vjp_cold<D, VISC>(bc, U, dU, n, w, pd, Ub, dUb);
+}
 
 // Ub += (d UB / d U)^T w for the prescribed boundary state UB of the LDG
 // common solution.
 template <int D>
-ZB_HD_COLD void bnd_ucomm_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+ZB_HD_INLINE void bnd_ucomm_vjp_body(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
                          const Phys<Dual<double>> &pd, double Ub[D + 2])
 {
   constexpr int V = D + 2;
@@ -586,6 +604,21 @@ ZB_HD_COLD void bnd_ucomm_vjp(int bc, const double U[D + 2], const double n[D], 
     for (int v = 0; v < V; v++) acc += w[v] * UB[v].d;
     Ub[k] += acc;
   }
+}
+template <int D>
+ZB_HD_COLD void bnd_ucomm_vjp_cold(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+                         const Phys<Dual<double>> &pd, double Ub[D + 2])
+{
+  bnd_ucomm_vjp_body<D>(bc, U, n, w, pd, Ub);
+}
+template <int D>
+ZB_HD_INLINE void bnd_ucomm_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+                         const Phys<Dual<double>> &pd, double Ub[D + 2])
+{
+  if constexpr (D == 2)
+    bnd_ucomm_vjp_body<D>(bc, U, n, w, pd, Ub);
+  else
+    bnd_ucomm_vjp_cold<D>(bc, U, n, w, pd, Ub);
 }
 
 // Free-stream parameters a boundary state depends on: k = 0 rho_fs,
@@ -605,7 +638,7 @@ ZB_HD void seed_param(Phys<Dual<double>> &q, int k)
 // pb[k] += d (w . phi) / d param_k for the boundary face function of
 // bnd_face_vjp.
 template <int D, bool VISC>
-ZB_HD_COLD void bnd_face_param_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+ZB_HD_INLINE void bnd_face_param_vjp_body(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
                               const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
 {
   constexpr int V = D + 2;
@@ -638,10 +671,25 @@ ZB_HD_COLD void bnd_face_param_vjp(int bc, const double U[D + 2], const double d
     pb[k] += acc;
   }
 }
+template <int D, bool VISC>
+ZB_HD_COLD void bnd_face_param_vjp_cold(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+                              const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
+{
+  bnd_face_param_vjp_body<D, VISC>(bc, U, dU, n, w, pd, pb);
+}
+template <int D, bool VISC>
+ZB_HD_INLINE void bnd_face_param_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+                              const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
+{
+  if constexpr (D == 2)
+    bnd_face_param_vjp_body<D, VISC>(bc, U, dU, n, w, pd, pb);
+  else
+    bnd_face_param_vjp_cold<D, VISC>(bc, U, dU, n, w, pd, pb);
+}
 
 // pb[k] += d (w . UB) / d param_k for the LDG boundary common solution.
 template <int D>
-ZB_HD_COLD void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+ZB_HD_INLINE void bnd_ucomm_param_vjp_body(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
                                const Phys<Dual<double>> &pd, double pb[5])
 {
   constexpr int V = D + 2;
@@ -662,6 +710,21 @@ ZB_HD_COLD void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const double 
     pb[k] += acc;
   }
 }
+template <int D>
+ZB_HD_COLD void bnd_ucomm_param_vjp_cold(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+                               const Phys<Dual<double>> &pd, double pb[5])
+{
+  bnd_ucomm_param_vjp_body<D>(bc, U, n, w, pd, pb);
+}
+template <int D>
+ZB_HD_INLINE void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+                               const Phys<Dual<double>> &pd, double pb[5])
+{
+  if constexpr (D == 2)
+    bnd_ucomm_param_vjp_body<D>(bc, U, n, w, pd, pb);
+  else
+    bnd_ucomm_param_vjp_cold<D>(bc, U, n, w, pd, pb);
+}
 
 // ---------------------------------------------------------------------------
 // Kernels
@@ -671,7 +734,7 @@ ZB_HD_COLD void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const double 
 
 // nb += d (w . Fc(UL, UR, n)) / d n for an interior face (dual-number seeds on n)
 template <int D>
-ZB_HD_COLD void conv_face_n_vjp(const double UL[D + 2], const double UR[D + 2], const double n[D],
+ZB_HD_INLINE void conv_face_n_vjp_body(const double UL[D + 2], const double UR[D + 2], const double n[D],
                                 const double w[D + 2], const Phys<double> &ph, double nb[D])
 {
   constexpr int V = D + 2;
@@ -693,10 +756,25 @@ ZB_HD_COLD void conv_face_n_vjp(const double UL[D + 2], const double UR[D + 2], 
     nb[k] += acc;
   }
 }
+template <int D>
+ZB_HD_COLD void conv_face_n_vjp_cold(const double UL[D + 2], const double UR[D + 2], const double n[D],
+                                const double w[D + 2], const Phys<double> &ph, double nb[D])
+{
+  conv_face_n_vjp_body<D>(UL, UR, n, w, ph, nb);
+}
+template <int D>
+ZB_HD_INLINE void conv_face_n_vjp(const double UL[D + 2], const double UR[D + 2], const double n[D],
+                                const double w[D + 2], const Phys<double> &ph, double nb[D])
+{
+  if constexpr (D == 2)
+    conv_face_n_vjp_body<D>(UL, UR, n, w, ph, nb);
+  else
+    conv_face_n_vjp_cold<D>(UL, UR, n, w, ph, nb);
+}
 
 // nb += d (w . phi) / d n for the boundary face function of bnd_face_vjp
 template <int D, bool VISC>
-ZB_HD_COLD void bnd_face_n_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+ZB_HD_INLINE void bnd_face_n_vjp_body(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
                                const double w[D + 2], const Phys<double> &ph, double nb[D])
 {
   constexpr int V = D + 2;
@@ -726,10 +804,25 @@ ZB_HD_COLD void bnd_face_n_vjp(int bc, const double U[D + 2], const double dU[D 
     nb[k] += acc;
   }
 }
+template <int D, bool VISC>
+ZB_HD_COLD void bnd_face_n_vjp_cold(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+                               const double w[D + 2], const Phys<double> &ph, double nb[D])
+{
+  bnd_face_n_vjp_body<D, VISC>(bc, U, dU, n, w, ph, nb);
+}
+template <int D, bool VISC>
+ZB_HD_INLINE void bnd_face_n_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
+                               const double w[D + 2], const Phys<double> &ph, double nb[D])
+{
+  if constexpr (D == 2)
+    bnd_face_n_vjp_body<D, VISC>(bc, U, dU, n, w, ph, nb);
+  else
+    bnd_face_n_vjp_cold<D, VISC>(bc, U, dU, n, w, ph, nb);
+}
 
 // nb += d (w . UB(U, n)) / d n for the LDG boundary common solution
 template <int D>
-ZB_HD_COLD void bnd_ucomm_n_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+ZB_HD_INLINE void bnd_ucomm_n_vjp_body(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
                                 const Phys<double> &ph, double nb[D])
 {
   constexpr int V = D + 2;
@@ -746,6 +839,21 @@ ZB_HD_COLD void bnd_ucomm_n_vjp(int bc, const double U[D + 2], const double n[D]
     for (int v = 0; v < V; v++) acc += w[v] * UB[v].d;
     nb[k] += acc;
   }
+}
+template <int D>
+ZB_HD_COLD void bnd_ucomm_n_vjp_cold(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+                                const Phys<double> &ph, double nb[D])
+{
+  bnd_ucomm_n_vjp_body<D>(bc, U, n, w, ph, nb);
+}
+template <int D>
+ZB_HD_INLINE void bnd_ucomm_n_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
+                                const Phys<double> &ph, double nb[D])
+{
+  if constexpr (D == 2)
+    bnd_ucomm_n_vjp_body<D>(bc, U, n, w, ph, nb);
+  else
+    bnd_ucomm_n_vjp_cold<D>(bc, U, n, w, ph, nb);
 }
 
 // Viscous flux matrix F_visc[var][dim] of one trace (the part flux_visc_add adds)

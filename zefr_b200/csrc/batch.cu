@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__re
 // every order (costliest order first) and runs each with its order's tile
 // body; the group's shared memory fits the largest order present.
 template <typename T, typename A>
-__global__ void __launch_bounds__(256) k_batch_euler_fused(const BatchCase<T, A> *__restrict__ cases,
+__global__ void __launch_bounds__(256, sizeof(A) == 4 ? 3 : 1) k_batch_euler_fused(const BatchCase<T, A> *__restrict__ cases,
                                                            const int2 *__restrict__ items, int begin, int end, int gsz,
                                                            int gstride, int chunk)
 {

@@ -309,7 +309,10 @@ __device__ __forceinline__ void hex_finish(const Args<T, A> &a, int64_t tile, in
   for (int v = 0; v < V; v++)
   {
     const int64_t idx = base + v * TW + l;
-    u_ini[v] = a.save_ini ? (A)a.U[idx] : (A)a.U_ini[idx];
+    // U_ini (after stage 0) and the earlier residual registers are not
+    // written by this kernel: read-only loads, free to move above the stores
+    // of the thread's other points
+    u_ini[v] = a.save_ini ? (A)a.U[idx] : (A)__ldg(a.U_ini + idx);
     comp[v] = (a.rk_mode == 2 && a.Ucomp) ? (A)a.Ucomp[idx] : A(0);
   }
   if (a.rk_mode == 2 && fast)
@@ -319,7 +322,7 @@ __device__ __forceinline__ void hex_finish(const Args<T, A> &a, int64_t tile, in
       if (st < a.nprev)
       {
 #pragma unroll
-        for (int v = 0; v < V; v++) prev[st][v] = (A)a.divF_prev[st][base + v * TW + l];
+        for (int v = 0; v < V; v++) prev[st][v] = (A)__ldg(a.divF_prev[st] + base + v * TW + l);
       }
   }
 #pragma unroll
