@@ -426,6 +426,10 @@ void zb_batch_destroy(zb_batch *batch);
 /* Time every launch shape on `steps` steps from the current states (which are
  * restored afterwards) and keep the fastest; *chosen may be NULL. */
 zb_status zb_batch_autotune(zb_batch *batch, int steps, zb_batch_config *chosen);
+/* As zb_batch_autotune over the shapes of one form only: form 0 keeps one
+ * kernel per order present, form 1 one kernel per stage for all orders, -1
+ * either (zb_batch_autotune).  The chosen shape is installed. */
+zb_status zb_batch_autotune_form(zb_batch *batch, int steps, int form, zb_batch_config *chosen);
 zb_status zb_batch_set_config(zb_batch *batch, const zb_batch_config *cfg);
 /* nsteps RK44 steps of every case; use_graph = 1 replays the captured graph,
  * 0 launches the four stages directly.  Returns once queued. */

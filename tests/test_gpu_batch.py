@@ -82,6 +82,29 @@ def test_autotune_keeps_state_and_picks_a_shape():
         assert _same(s1.get_state(), s2.get_state(), "mixed")
 
 
+@pytest.mark.parametrize("form", [True, False])
+def test_autotune_of_one_form_installs_that_form(form):
+    """Tuning restricted to one form picks a shape of that form, leaves the
+    states untouched, and the installed shape steps as the cases do alone."""
+    cases = zbatch.vortex_cases(8, 7, n_range=(4, 12), precision="mixed")
+    before = [s.get_state() for s in cases]
+    bt = zbatch.Batch(cases)
+    cfg = bt.autotune(steps=1, form=form)
+    assert cfg["fused"] == int(form) and cfg["ms_per_step"] > 0
+    for s, u in zip(cases, before):
+        assert np.array_equal(s.get_state(), u)
+    orders = len({c.info.order for c in cases})
+    n0 = bt.launch_count()
+    bt.step(2)
+    bt.synchronize()
+    assert bt.launch_count() - n0 == 2 * 4 * (1 if form else orders)
+    ref = zbatch.vortex_cases(8, 7, n_range=(4, 12), precision="mixed")
+    for s in ref:
+        s.step(2)
+    for s1, s2 in zip(ref, cases):
+        assert _same(s1.get_state(), s2.get_state(), "mixed")
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("shape", [(256, 64, 0), (128, 128, 1), (256, 256, 8)])
 def test_fused_single_launch_matches_cases_stepped_alone(precision, shape):

@@ -35,7 +35,8 @@ EXPORTED = [
     "zb_synchronize", "zb_launch_count", "zb_profile_enable", "zb_profile_read", "zb_kernel_name",
     "zb_compute_residual_noalloc", "zb_functionals", "zb_vjp", "zb_set_freestream", "zb_wall_force", "zb_vjp_geometry",
     "zb_vjp_geometry_accumulate", "zb_geometry_adjoint_get",
-    "zb_batch_create", "zb_batch_destroy", "zb_batch_autotune", "zb_batch_set_config", "zb_batch_step",
+    "zb_batch_create", "zb_batch_destroy", "zb_batch_autotune", "zb_batch_autotune_form", "zb_batch_set_config",
+    "zb_batch_step",
     "zb_batch_stage", "zb_batch_synchronize", "zb_batch_launch_count",
     "zb_time_scheme_defaults", "zb_set_time_scheme", "zb_time_state", "zb_get_element_dt", "zb_rk_step_vjp",
     "zb_geometry_eval", "zb_geometry_eval_vjp", "zb_set_nodes",
@@ -165,6 +166,7 @@ def lib() -> ctypes.CDLL:
         L.zb_batch_destroy.argtypes = [vp]
         L.zb_batch_destroy.restype = None
         L.zb_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ZbBatchConfig)]
+        L.zb_batch_autotune_form.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ZbBatchConfig)]
         L.zb_batch_set_config.argtypes = [vp, ctypes.POINTER(ZbBatchConfig)]
         L.zb_batch_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.zb_batch_stage.argtypes = [vp, ctypes.c_uint]

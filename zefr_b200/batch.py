@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import ctypes
 import math
-from typing import Dict, List, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -85,9 +85,12 @@ class Batch:
     def synchronize(self) -> None:
         check(lib().zb_batch_synchronize(self.h))
 
-    def autotune(self, steps: int = 3) -> Dict[str, float]:
+    def autotune(self, steps: int = 3, form: Optional[bool] = None) -> Dict[str, float]:
+        """Time every launch shape and install the fastest; form True keeps
+        to one kernel per stage for all orders, False to one kernel per order,
+        None takes either."""
         c = _lib.ZbBatchConfig()
-        check(lib().zb_batch_autotune(self.h, steps, ctypes.byref(c)))
+        check(lib().zb_batch_autotune_form(self.h, steps, -1 if form is None else int(bool(form)), ctypes.byref(c)))
         return {"threads": c.threads, "group": c.group, "chunk": c.chunk, "blocks_per_sm": c.blocks_per_sm,
                 "order": c.order, "ms_per_step": c.ms_per_step, "fused": c.fused}
 

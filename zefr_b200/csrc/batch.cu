@@ -86,9 +86,14 @@ __global__ void __launch_bounds__(256) k_batch_euler(const BatchCase<T, A> *__re
 
 // The single-launch form: one persistent kernel per stage walks the items of
 // every order (costliest order first) and runs each with its order's tile
-// body; the group's shared memory fits the largest order present.
+// body; the group's shared memory fits the largest order present.  In FP32
+// the registers are held to four 256-thread CTAs per SM: the kernel carries
+// every order's body, and left to itself the compiler sizes it for the
+// largest (128 registers, two CTAs per SM: 38 GDOF/s on the 512-case batch
+// against 44 at four CTAs per SM, a few bytes of the largest order's
+// values spilled).
 template <typename T, typename A>
-__global__ void __launch_bounds__(256, sizeof(A) == 4 ? 3 : 1) k_batch_euler_fused(const BatchCase<T, A> *__restrict__ cases,
+__global__ void __launch_bounds__(256, sizeof(A) == 4 ? 4 : 1) k_batch_euler_fused(const BatchCase<T, A> *__restrict__ cases,
                                                            const int2 *__restrict__ items, int begin, int end, int gsz,
                                                            int gstride, int chunk)
 {
@@ -468,7 +473,7 @@ int64_t batch_launches(const Batch *b) { return b->launches; }
 
 // Time each candidate launch shape on a few graph-replayed steps from the
 // current state, restore the state, keep the fastest.
-void batch_autotune(Batch *b, int steps, zb_batch_config *out)
+void batch_autotune(Batch *b, int steps, int form, zb_batch_config *out)
 {
   if (steps < 1) steps = 1;
   prepare(*b, 0);
@@ -497,6 +502,7 @@ void batch_autotune(Batch *b, int steps, zb_batch_config *out)
   for (int fused : {0, 1})
   for (int order : orders)
   {
+    if (form >= 0 && fused != form) continue;
     build_items(*b, order);
     for (const auto &sh : shapes)
       for (int bp : bps)

@@ -484,7 +484,16 @@ zb_status zb_batch_autotune(zb_batch *batch, int steps, zb_batch_config *chosen)
 {
   ZB_GUARD({
     ZB_REQUIRE(batch, "null batch");
-    zb::batch_autotune(batch->impl, steps, chosen);
+    zb::batch_autotune(batch->impl, steps, -1, chosen);
+  })
+}
+
+zb_status zb_batch_autotune_form(zb_batch *batch, int steps, int form, zb_batch_config *chosen)
+{
+  ZB_GUARD({
+    ZB_REQUIRE(batch, "null batch");
+    ZB_REQUIRE(form >= -1 && form <= 1, "form must be -1, 0 or 1");
+    zb::batch_autotune(batch->impl, steps, form, chosen);
   })
 }
 

@@ -71,7 +71,7 @@ void noalloc_residual(const Plan &p, const double *U, double *divF, cudaStream_t
 struct Batch;
 Batch *batch_create(Ctx *const *ctxs, int n);
 void batch_destroy(Batch *b);
-void batch_autotune(Batch *b, int steps, zb_batch_config *out);
+void batch_autotune(Batch *b, int steps, int form, zb_batch_config *out);
 void batch_config(Batch *b, const zb_batch_config *cfg);
 void batch_step(Batch *b, int nsteps, int use_graph);
 void batch_stage(Batch *b, unsigned stage);
