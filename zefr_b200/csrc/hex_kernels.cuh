@@ -535,7 +535,9 @@ __global__ void __launch_bounds__(TW * N * N) k_hex_euler(const __grid_constant_
 // doubling the warps per CTA for the same shared memory; minb is the CTAs per
 // SM the register allocation is held to (0: the compiler's choice).  Chosen by
 // timing P3 on B200: the split pays for the gradient kernel in both
-// precisions and for the face kernel in FP64 only.
+// precisions and for the face kernel in FP64 only.  The FP64 face kernel is
+// held to three CTAs per SM (80 registers; some of the RK update's values
+// spill): 0.43 against 0.47 ms per residual at two CTAs, 0.57 at four.
 // ---------------------------------------------------------------------------
 template <typename A, int N>
 struct HexNsShape
@@ -543,7 +545,7 @@ struct HexNsShape
   static constexpr int grad_zs = (N % 2 == 0) ? 2 : 1;
   static constexpr int grad_minb = grad_zs == 2 ? (sizeof(A) == 4 ? 4 : 2) : 0;
   static constexpr int face_zs = (N % 2 == 0 && sizeof(A) == 8) ? 2 : 1;
-  static constexpr int face_minb = face_zs == 2 ? 2 : 0;
+  static constexpr int face_minb = face_zs == 2 ? 3 : 0;
 };
 
 // ---------------------------------------------------------------------------
