@@ -81,6 +81,21 @@ struct RowOps
   }
 };
 
+// Two variables of a point at once in FP32: the paired FP32 instructions of
+// sm_100 (FFMA2, FMUL2, FADD2) take float2 operands and round each lane as
+// the scalar instruction does.  Variables v and v + 1 of a point lie TW
+// apart in the tile arrays.
+struct F2
+{
+  static __device__ __forceinline__ float2 dup(float x) { return make_float2(x, x); }
+  static __device__ __forceinline__ float2 ld(const float *p) { return make_float2(p[0], p[TW]); }
+  static __device__ __forceinline__ void st(float *p, float2 x)
+  {
+    p[0] = x.x;
+    p[TW] = x.y;
+  }
+};
+
 // own flux point q (0..5): side of the face
 __device__ __forceinline__ bool q_minus(int q) { return (q & 1) == 0; }
 
@@ -726,8 +741,53 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
     A adj[3][3], det;
     load_adj<T, A>(a, tile, S, s, l, adj, det);
     const A inv_det = A(1) / det;
+    if constexpr (sizeof(A) == 4)
+    {
+      // FP32: variables 0-3 in pairs on the paired FP32 instructions, the
+      // fifth in the loop below
 #pragma unroll
-    for (int v = 0; v < V; v++)
+      for (int v = 0; v < V - 1; v += 2)
+      {
+        float2 td[3];
+        {
+          float2 acc = __fmul2_rn(F2::dup(o.Dx[0]), F2::ld(sU + ((N * iy + H::N2 * iz) * V + v) * TW + l));
+#pragma unroll
+          for (int m = 1; m < N; m++)
+            acc = __ffma2_rn(F2::dup(o.Dx[m]), F2::ld(sU + ((m + N * iy + H::N2 * iz) * V + v) * TW + l), acc);
+          const float2 cm = __fmul2_rn(F2::dup(o.dbxm), F2::ld(sUC + (fxm * V + v) * TW + l));
+          td[0] = __fadd2_rn(acc, __ffma2_rn(F2::dup(o.dbxp), F2::ld(sUC + (fxp * V + v) * TW + l), cm));
+        }
+        {
+          float2 acc = __fmul2_rn(F2::dup(o.Dy[0]), F2::ld(sU + ((ix + H::N2 * iz) * V + v) * TW + l));
+#pragma unroll
+          for (int m = 1; m < N; m++)
+            acc = __ffma2_rn(F2::dup(o.Dy[m]), F2::ld(sU + ((ix + N * m + H::N2 * iz) * V + v) * TW + l), acc);
+          const float2 cm = __fmul2_rn(F2::dup(o.dbym), F2::ld(sUC + (fym * V + v) * TW + l));
+          td[1] = __fadd2_rn(acc, __ffma2_rn(F2::dup(o.dbyp), F2::ld(sUC + (fyp * V + v) * TW + l), cm));
+        }
+        {
+          float2 acc = __fmul2_rn(F2::dup(ops.Dm[iz * N]), F2::ld(sU + ((ix + N * iy) * V + v) * TW + l));
+#pragma unroll
+          for (int m = 1; m < N; m++)
+            acc = __ffma2_rn(F2::dup(ops.Dm[iz * N + m]), F2::ld(sU + ((ix + N * iy + H::N2 * m) * V + v) * TW + l),
+                             acc);
+          const float2 cm = __fmul2_rn(F2::dup(ops.Dbm[iz]), F2::ld(sUC + (fzm * V + v) * TW + l));
+          td[2] = __fadd2_rn(acc, __ffma2_rn(F2::dup(ops.Dbp[iz]), F2::ld(sUC + (fzp * V + v) * TW + l), cm));
+        }
+#pragma unroll
+        for (int d1 = 0; d1 < 3; d1++)
+        {
+          float2 g = __fmul2_rn(td[0], F2::dup(adj[0][d1]));
+          g = __ffma2_rn(td[1], F2::dup(adj[1][d1]), g);
+          g = __ffma2_rn(td[2], F2::dup(adj[2][d1]), g);
+          g = __fmul2_rn(g, F2::dup(inv_det));
+          F2::st(sX + xo(d1 * S + s) + v * TW + l, g);
+          if (a.dU_out) F2::st(a.dU_out + (((tile * 3 + d1) * S + s) * V + v) * TW + l, g);
+        }
+      }
+    }
+#pragma unroll
+    for (int v = (sizeof(A) == 4 ? V - 1 : 0); v < V; v++)
     {
       A td[3];
       {
@@ -884,8 +944,28 @@ __global__ void __launch_bounds__(TW * N * N * HexNsShape<A, N>::grad_zs, HexNsS
   {
     const int s = ix + N * iy + H::N2 * iz;
     A *out = a.divF_vol + (tile * S + s) * (int64_t)V * TW + l;
+    if constexpr (sizeof(A) == 4)
+    {
+      // FP32: variables 0-3 in pairs, the fifth in the loop below
 #pragma unroll
-    for (int v = 0; v < V; v++)
+      for (int v = 0; v < V - 1; v += 2)
+      {
+        float2 vol = __fmul2_rn(F2::dup(o.Dx[0]), F2::ld(sX + xo(N * iy + H::N2 * iz) + v * TW + l));
+#pragma unroll
+        for (int m = 1; m < N; m++)
+          vol = __ffma2_rn(F2::dup(o.Dx[m]), F2::ld(sX + xo(m + N * iy + H::N2 * iz) + v * TW + l), vol);
+#pragma unroll
+        for (int m = 0; m < N; m++)
+          vol = __ffma2_rn(F2::dup(o.Dy[m]), F2::ld(sX + xo(S + ix + N * m + H::N2 * iz) + v * TW + l), vol);
+#pragma unroll
+        for (int m = 0; m < N; m++)
+          vol = __ffma2_rn(F2::dup(ops.Dm[iz * N + m]), F2::ld(sX + xo(2 * S + ix + N * iy + H::N2 * m) + v * TW + l),
+                           vol);
+        F2::st(out + v * TW, vol);
+      }
+    }
+#pragma unroll
+    for (int v = (sizeof(A) == 4 ? V - 1 : 0); v < V; v++)
     {
       A vol = A(0);
 #pragma unroll
