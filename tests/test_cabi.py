@@ -119,3 +119,14 @@ def test_adjoint_and_geometry_entry_points_reject_a_null_context():
     for name, call in calls.items():
         assert call() == -1, name
         assert b"null" in L.zb_last_error(), name
+
+
+def test_batch_tuning_entry_points_reject_a_null_batch():
+    """Both autotuners check the batch before touching the GPU."""
+    L = _lib.lib()
+    cfg = _lib.ZbBatchConfig()
+    assert L.zb_batch_autotune(None, 1, ctypes.byref(cfg)) == -1
+    assert b"null" in L.zb_last_error()
+    for form in (-1, 0, 1):
+        assert L.zb_batch_autotune_form(None, 1, form, ctypes.byref(cfg)) == -1
+        assert b"null" in L.zb_last_error()
