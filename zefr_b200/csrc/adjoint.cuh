@@ -537,7 +537,8 @@ ZB_HD void visc_normal_vjp(const double U[D + 2], const double dU[D + 2][D], con
 //   F_visc(UB, ghost_grad(U, dU)) . n + tau (U - UB).
 template <int D, bool VISC>
 ZB_HD_INLINE void bnd_face_vjp_body(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
-                        const double w[D + 2], const Phys<Dual<double>> &pd, double Ub[D + 2], double dUb[D + 2][D])
+                                    const double w[D + 2], const Phys<Dual<double>> &pd,
+                                    double Ub[D + 2], double dUb[D + 2][D])
 {
   constexpr int V = D + 2;
   using DD = Dual<double>;
@@ -571,13 +572,15 @@ ZB_HD_INLINE void bnd_face_vjp_body(int bc, const double U[D + 2], const double 
 }
 template <int D, bool VISC>
 ZB_HD_COLD void bnd_face_vjp_cold(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
-                        const double w[D + 2], const Phys<Dual<double>> &pd, double Ub[D + 2], double dUb[D + 2][D])
+                                  const double w[D + 2], const Phys<Dual<double>> &pd,
+                                  double Ub[D + 2], double dUb[D + 2][D])
 {
   bnd_face_vjp_body<D, VISC>(bc, U, dU, n, w, pd, Ub, dUb);
 }
 template <int D, bool VISC>
 ZB_HD_INLINE void bnd_face_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
-                        const double w[D + 2], const Phys<Dual<double>> &pd, double Ub[D + 2], double dUb[D + 2][D])
+                               const double w[D + 2], const Phys<Dual<double>> &pd,
+                               double Ub[D + 2], double dUb[D + 2][D])
 {
   if constexpr (D == 2)
     bnd_face_vjp_body<D, VISC>(bc, U, dU, n, w, pd, Ub, dUb);
@@ -589,7 +592,7 @@ ZB_HD_INLINE void bnd_face_vjp(int bc, const double U[D + 2], const double dU[D 
 // common solution.
 template <int D>
 ZB_HD_INLINE void bnd_ucomm_vjp_body(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
-                         const Phys<Dual<double>> &pd, double Ub[D + 2])
+                                     const Phys<Dual<double>> &pd, double Ub[D + 2])
 {
   constexpr int V = D + 2;
   using DD = Dual<double>;
@@ -607,13 +610,13 @@ ZB_HD_INLINE void bnd_ucomm_vjp_body(int bc, const double U[D + 2], const double
 }
 template <int D>
 ZB_HD_COLD void bnd_ucomm_vjp_cold(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
-                         const Phys<Dual<double>> &pd, double Ub[D + 2])
+                                   const Phys<Dual<double>> &pd, double Ub[D + 2])
 {
   bnd_ucomm_vjp_body<D>(bc, U, n, w, pd, Ub);
 }
 template <int D>
 ZB_HD_INLINE void bnd_ucomm_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
-                         const Phys<Dual<double>> &pd, double Ub[D + 2])
+                                const Phys<Dual<double>> &pd, double Ub[D + 2])
 {
   if constexpr (D == 2)
     bnd_ucomm_vjp_body<D>(bc, U, n, w, pd, Ub);
@@ -639,7 +642,7 @@ ZB_HD void seed_param(Phys<Dual<double>> &q, int k)
 // bnd_face_vjp.
 template <int D, bool VISC>
 ZB_HD_INLINE void bnd_face_param_vjp_body(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
-                              const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
+                                          const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
 {
   constexpr int V = D + 2;
   using DD = Dual<double>;
@@ -673,13 +676,13 @@ ZB_HD_INLINE void bnd_face_param_vjp_body(int bc, const double U[D + 2], const d
 }
 template <int D, bool VISC>
 ZB_HD_COLD void bnd_face_param_vjp_cold(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
-                              const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
+                                        const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
 {
   bnd_face_param_vjp_body<D, VISC>(bc, U, dU, n, w, pd, pb);
 }
 template <int D, bool VISC>
 ZB_HD_INLINE void bnd_face_param_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
-                              const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
+                                     const double w[D + 2], const Phys<Dual<double>> &pd, double pb[5])
 {
   if constexpr (D == 2)
     bnd_face_param_vjp_body<D, VISC>(bc, U, dU, n, w, pd, pb);
@@ -690,7 +693,7 @@ ZB_HD_INLINE void bnd_face_param_vjp(int bc, const double U[D + 2], const double
 // pb[k] += d (w . UB) / d param_k for the LDG boundary common solution.
 template <int D>
 ZB_HD_INLINE void bnd_ucomm_param_vjp_body(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
-                               const Phys<Dual<double>> &pd, double pb[5])
+                                           const Phys<Dual<double>> &pd, double pb[5])
 {
   constexpr int V = D + 2;
   using DD = Dual<double>;
@@ -712,13 +715,13 @@ ZB_HD_INLINE void bnd_ucomm_param_vjp_body(int bc, const double U[D + 2], const 
 }
 template <int D>
 ZB_HD_COLD void bnd_ucomm_param_vjp_cold(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
-                               const Phys<Dual<double>> &pd, double pb[5])
+                                         const Phys<Dual<double>> &pd, double pb[5])
 {
   bnd_ucomm_param_vjp_body<D>(bc, U, n, w, pd, pb);
 }
 template <int D>
 ZB_HD_INLINE void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
-                               const Phys<Dual<double>> &pd, double pb[5])
+                                      const Phys<Dual<double>> &pd, double pb[5])
 {
   if constexpr (D == 2)
     bnd_ucomm_param_vjp_body<D>(bc, U, n, w, pd, pb);
@@ -735,7 +738,7 @@ ZB_HD_INLINE void bnd_ucomm_param_vjp(int bc, const double U[D + 2], const doubl
 // nb += d (w . Fc(UL, UR, n)) / d n for an interior face (dual-number seeds on n)
 template <int D>
 ZB_HD_INLINE void conv_face_n_vjp_body(const double UL[D + 2], const double UR[D + 2], const double n[D],
-                                const double w[D + 2], const Phys<double> &ph, double nb[D])
+                                       const double w[D + 2], const Phys<double> &ph, double nb[D])
 {
   constexpr int V = D + 2;
   using DD = Dual<double>;
@@ -758,13 +761,13 @@ ZB_HD_INLINE void conv_face_n_vjp_body(const double UL[D + 2], const double UR[D
 }
 template <int D>
 ZB_HD_COLD void conv_face_n_vjp_cold(const double UL[D + 2], const double UR[D + 2], const double n[D],
-                                const double w[D + 2], const Phys<double> &ph, double nb[D])
+                                     const double w[D + 2], const Phys<double> &ph, double nb[D])
 {
   conv_face_n_vjp_body<D>(UL, UR, n, w, ph, nb);
 }
 template <int D>
 ZB_HD_INLINE void conv_face_n_vjp(const double UL[D + 2], const double UR[D + 2], const double n[D],
-                                const double w[D + 2], const Phys<double> &ph, double nb[D])
+                                  const double w[D + 2], const Phys<double> &ph, double nb[D])
 {
   if constexpr (D == 2)
     conv_face_n_vjp_body<D>(UL, UR, n, w, ph, nb);
@@ -775,7 +778,7 @@ ZB_HD_INLINE void conv_face_n_vjp(const double UL[D + 2], const double UR[D + 2]
 // nb += d (w . phi) / d n for the boundary face function of bnd_face_vjp
 template <int D, bool VISC>
 ZB_HD_INLINE void bnd_face_n_vjp_body(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
-                               const double w[D + 2], const Phys<double> &ph, double nb[D])
+                                      const double w[D + 2], const Phys<double> &ph, double nb[D])
 {
   constexpr int V = D + 2;
   using DD = Dual<double>;
@@ -806,13 +809,13 @@ ZB_HD_INLINE void bnd_face_n_vjp_body(int bc, const double U[D + 2], const doubl
 }
 template <int D, bool VISC>
 ZB_HD_COLD void bnd_face_n_vjp_cold(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
-                               const double w[D + 2], const Phys<double> &ph, double nb[D])
+                                    const double w[D + 2], const Phys<double> &ph, double nb[D])
 {
   bnd_face_n_vjp_body<D, VISC>(bc, U, dU, n, w, ph, nb);
 }
 template <int D, bool VISC>
 ZB_HD_INLINE void bnd_face_n_vjp(int bc, const double U[D + 2], const double dU[D + 2][D], const double n[D],
-                               const double w[D + 2], const Phys<double> &ph, double nb[D])
+                                 const double w[D + 2], const Phys<double> &ph, double nb[D])
 {
   if constexpr (D == 2)
     bnd_face_n_vjp_body<D, VISC>(bc, U, dU, n, w, ph, nb);
@@ -823,7 +826,7 @@ ZB_HD_INLINE void bnd_face_n_vjp(int bc, const double U[D + 2], const double dU[
 // nb += d (w . UB(U, n)) / d n for the LDG boundary common solution
 template <int D>
 ZB_HD_INLINE void bnd_ucomm_n_vjp_body(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
-                                const Phys<double> &ph, double nb[D])
+                                       const Phys<double> &ph, double nb[D])
 {
   constexpr int V = D + 2;
   using DD = Dual<double>;
@@ -842,13 +845,13 @@ ZB_HD_INLINE void bnd_ucomm_n_vjp_body(int bc, const double U[D + 2], const doub
 }
 template <int D>
 ZB_HD_COLD void bnd_ucomm_n_vjp_cold(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
-                                const Phys<double> &ph, double nb[D])
+                                     const Phys<double> &ph, double nb[D])
 {
   bnd_ucomm_n_vjp_body<D>(bc, U, n, w, ph, nb);
 }
 template <int D>
 ZB_HD_INLINE void bnd_ucomm_n_vjp(int bc, const double U[D + 2], const double n[D], const double w[D + 2],
-                                const Phys<double> &ph, double nb[D])
+                                  const Phys<double> &ph, double nb[D])
 {
   if constexpr (D == 2)
     bnd_ucomm_n_vjp_body<D>(bc, U, n, w, ph, nb);
